@@ -1,0 +1,77 @@
+"""Generate the golden fixtures in this directory from the reference itself.
+
+Runs oracle/_ref/ref_driver (the reference's own FGMRES sources compiled
+against the MKL stand-in, built by ``make -C oracle``) on small grids and
+stores what the reference computed:
+
+  ref_setup_<tag>.npz   sound2D, deltaL, base 2D CSR matrix (values/ia/ja)
+  ref_fgmres_<tag>.npz  f, x_sol (u = L0^{-1} w), convergence rows
+                        (iteration, Res_phys, RelRes_phys, analytic error)
+
+The reference is compiled in its default configuration (HOMO, nu = 4 Hz,
+c_z = 1280 m/s, LENGTH = 3200 m, REL_RES_EXIT = 1e-4).  Needs the reference
+sources, so it runs in the development container only; the fixtures travel.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+DRIVER = os.path.join(REPO, "oracle", "_ref", "ref_driver")
+
+# (tag, n_nopml, pml, spg, beta, niter, restart)
+CASES = [
+    ("n10p4s3", 10, 4, 3, 0.5, 10, 5),
+    ("n11p4s3", 11, 4, 3, 0.5, 10, 5),     # odd sizes: source at (n-1)/2
+    ("n16p6s4", 16, 6, 4, 0.25, 8, 4),
+]
+
+
+def run(args, cwd):
+    res = subprocess.run([DRIVER] + [str(a) for a in args], cwd=cwd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(res.stdout[-2000:] + res.stderr[-2000:])
+
+
+def main():
+    if not os.path.exists(DRIVER):
+        subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "-j8"], check=True)
+    for tag, n, pml, spg, beta, niter, rest in CASES:
+        nx = n + 2 * pml
+        nz = n + 2 * spg
+        with tempfile.TemporaryDirectory() as d:
+            run(["setup", n, pml, spg, beta, d], d)
+            ia = np.fromfile(os.path.join(d, "csr_ia.bin"), dtype=np.int32)
+            np.savez_compressed(
+                os.path.join(HERE, f"ref_setup_{tag}.npz"),
+                params=np.array([n, pml, spg, beta]),
+                sound2D=np.fromfile(os.path.join(d, "sound2D.bin"), dtype=np.complex128).reshape(nx, nx),
+                deltaL=np.fromfile(os.path.join(d, "deltaL.bin"), dtype=np.complex128).reshape(nz, nx, nx),
+                csr_values=np.fromfile(os.path.join(d, "csr_values.bin"), dtype=np.complex128),
+                csr_ia=ia,
+                csr_ja=np.fromfile(os.path.join(d, "csr_ja.bin"), dtype=np.int32),
+            )
+        with tempfile.TemporaryDirectory() as d:
+            run(["fgmres", n, pml, spg, beta, niter, rest, d], d)
+            conv = np.loadtxt(glob.glob(os.path.join(d, "convergence_*"))[0], ndmin=2)
+            np.savez_compressed(
+                os.path.join(HERE, f"ref_fgmres_{tag}.npz"),
+                params=np.array([n, pml, spg, beta, niter, rest]),
+                f=np.fromfile(os.path.join(d, "f.bin"), dtype=np.complex128).reshape(nz, nx, nx),
+                x_sol=np.fromfile(os.path.join(d, "x_sol.bin"), dtype=np.complex128).reshape(nz, nx, nx),
+                conv=conv,
+            )
+        print("wrote", tag, file=sys.stderr)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,76 @@
+"""The oracle against the reference itself (golden fixtures) and against the
+reference's own test properties.  CPU only."""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import GOLDEN
+from oracle import grid, mode_r
+
+CASES = ["n10p4s3", "n11p4s3", "n16p6s4"]
+
+
+def _load(kind, tag):
+    return np.load(os.path.join(GOLDEN, f"ref_{kind}_{tag}.npz"))
+
+
+@pytest.mark.parametrize("tag", CASES)
+def test_setup_matches_reference(tag):
+    """sound2D (quirk q1), deltaL and the base 5-point PML matrix
+    (Source/FGMRES.cpp:79-151) equal the reference's to rounding."""
+    z = _load("setup", tag)
+    n, pml, spg, beta = z["params"]
+    g = grid.reference_grid(int(n), int(pml), int(spg))
+    st = mode_r.setup(g, beta=float(beta), media="homo", factor=False)
+    assert np.abs(z["sound2D"].real - st.c2d).max() <= 1e-13 * st.c2d.max()
+    assert np.abs(z["sound2D"].imag).max() == 0.0
+    assert np.abs(z["deltaL"] - st.dl).max() <= 1e-12 * np.abs(st.dl).max()
+    n2 = g.size2d
+    A_ref = sp.csr_matrix((z["csr_values"], z["csr_ja"] - 1, z["csr_ia"] - 1), shape=(n2, n2))
+    A = mode_r.assemble_2d(g, np.zeros((g.y.n, g.x.n)))
+    assert abs(A_ref - A).max() <= 1e-14 * abs(A).max()
+
+
+@pytest.mark.parametrize("tag", CASES)
+def test_fgmres_matches_reference(tag):
+    """The reference's FGMRES (q5 Arnoldi, zgels every step, exit at
+    phys. rel. residual 1e-4): same residual history and same solution."""
+    z = _load("fgmres", tag)
+    n, pml, spg, beta, niter, rest = z["params"]
+    g = grid.reference_grid(int(n), int(pml), int(spg))
+    st = mode_r.setup(g, beta=float(beta), media="homo")
+    f = mode_r.point_source_rhs(g)
+    assert np.array_equal(f, z["f"])
+    log = mode_r.fgmres_reference(st, f, m=int(niter), rest=int(rest), arnoldi="reference")
+    conv = z["conv"]
+    assert len(log.rows) == conv.shape[0]
+    for row, ref in zip(log.rows, conv):
+        assert row[1] == pytest.approx(ref[1], rel=1e-5)   # printed with %e (7 digits)
+        assert row[2] == pytest.approx(ref[2], rel=1e-5)
+    err = np.linalg.norm(log.u - z["x_sol"]) / np.linalg.norm(z["x_sol"])
+    assert err < 1e-11
+
+
+def test_pml_symmetry_invariant():
+    """A_2D / (alpha_x alpha_y) is symmetric (Source/Tests.cpp:686-757)."""
+    g = grid.reference_grid(12, 5, 3)
+    A = mode_r.assemble_2d(g, np.zeros((g.y.n, g.x.n))).tocsr()
+    ax = np.array([grid.alpha(g.x, float(i), g.omega) for i in range(g.x.n)])
+    ay = np.array([grid.alpha(g.y, float(j), g.omega) for j in range(g.y.n)])
+    scale = (ay[:, None] * ax[None, :]).ravel()
+    S = sp.diags(1.0 / scale) @ A
+    assert abs(S - S.T).max() <= 1e-12 * abs(S).max()
+
+
+def test_inverse_traversal_identity():
+    """A_R (L0^{-1} g) = g - dL L0^{-1} g, i.e. K = A_R L0^{-1}
+    (Source/Tests.cpp:444-684)."""
+    g = grid.reference_grid(10, 4, 3)
+    st = mode_r.setup(g, beta=0.5, media="homo")
+    rng = np.random.default_rng(1)
+    v = rng.standard_normal(g.shape_zyx) + 1j * rng.standard_normal(g.shape_zyx)
+    lhs = st.apply_a(st.l0_solve(v))
+    rhs = st.apply_k(v)
+    assert np.linalg.norm(lhs - rhs) <= 1e-11 * np.linalg.norm(rhs)
