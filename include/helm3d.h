@@ -1,0 +1,178 @@
+/*
+ * helm3d.h -- C ABI of the B200 3D Helmholtz solver.
+ *
+ * The solve is the reference's: a Krylov outer iteration preconditioned by
+ * an FFT along z that splits the 3D problem into one shifted 2D system per
+ * kz (dklyuchinskiy/Iterative-Helmholtz-solver-with-PARDISO).  The 2D
+ * systems are factorised here by a batched block-tridiagonal block LU over
+ * y-lines instead of PARDISO.  Every call returns a helm3d_status (0 = OK).
+ *
+ * Vectors are complex128, interleaved (re, im), laid out l = i + nx*j +
+ * nx*ny*k (x fastest) as the reference's take_coord3D
+ * (Source/functions.cpp:225-230).  A vector argument may be a device
+ * pointer or a host pointer (pageable or pinned); host data is copied in and
+ * out by the call.  A context owns the factor and all workspace; it is not
+ * shared between threads.  Work is ordered on the context's stream.
+ *
+ * Two operators (helm3d_opts.mode):
+ *   HELM3D_MODE_R  the reference's K w = (I - dL L0^{-1}) w = f, u = L0^{-1} w
+ *                  (Source/FGMRES.cpp:464-684, Source/functions.cpp:5554-5575)
+ *   HELM3D_MODE_N  the 7-point PML-stretched operator A u = f, with the FFT-z
+ *                  operator as a flexible right preconditioner M.
+ */
+#ifndef HELM3D_H
+#define HELM3D_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HELM3D_ABI_VERSION 1
+
+typedef enum helm3d_status {
+    HELM3D_OK = 0,
+    HELM3D_ERR_ARG = 1,            /* bad argument or unsupported size */
+    HELM3D_ERR_OOM = 2,            /* device allocation failed */
+    HELM3D_ERR_CUDA = 3,           /* a CUDA call failed */
+    HELM3D_ERR_SINGULAR = 4,       /* zero pivot in the block LU factor */
+    HELM3D_ERR_NOT_CONVERGED = 5,  /* max_iter reached above tol */
+    HELM3D_ERR_BREAKDOWN = 6,      /* Krylov breakdown (BiCGStab rho/omega = 0) */
+    HELM3D_ERR_NONFINITE = 7,      /* NaN/Inf in the input or a residual */
+    HELM3D_ERR_NO_DEVICE = 8       /* no usable CUDA device */
+} helm3d_status;
+
+typedef enum helm3d_mode { HELM3D_MODE_R = 0, HELM3D_MODE_N = 1 } helm3d_mode;
+
+/* arithmetic and storage type of the preconditioner (FFT planes, factor,
+ * sweep); the outer Krylov loop is always complex128 */
+typedef enum helm3d_precision { HELM3D_PREC_C128 = 0, HELM3D_PREC_C64 = 1 } helm3d_precision;
+
+/* kz^2 of plane k: (4/hz^2) sin^2(pi k/nz) | (2 pi min(k,nz-k)/Lz)^2 |
+ * the reference's table (Source/FGMRES.cpp:182-190) */
+typedef enum helm3d_kz_symbol {
+    HELM3D_KZ_DISCRETE = 0,
+    HELM3D_KZ_CONTINUOUS = 1,
+    HELM3D_KZ_REFERENCE = 2
+} helm3d_kz_symbol;
+
+/* Grid: mirrors size_m (Source/definitions.h:55-68) for three axes. */
+typedef struct helm3d_grid {
+    int nx, ny, nz;          /* points per axis, PML/sponge included */
+    double hx, hy, hz;       /* steps */
+    int pml_x, pml_y, pml_z; /* PML points on each face (alpha != 1 there) */
+    int spg_z;               /* sponge points at each z end (mode R) */
+    double lz;               /* z period of the kz table; 0 -> nz*hz */
+    double omega;            /* angular frequency */
+} helm3d_grid;
+
+typedef struct helm3d_opts {
+    int mode;            /* helm3d_mode */
+    int precision;       /* helm3d_precision */
+    int kz_symbol;       /* helm3d_kz_symbol */
+    double beta_prec;    /* complex shift of the preconditioner; mode R: beta_eq */
+    double beta_phys;    /* mode N: physical damping in A */
+    double s2_l0;        /* mode R: > 0 -> L0 uses this constant s^2 (HOMO, q3) */
+    int quirk_q1;        /* mode R: c0 by the reference's running-sum mean (q1) */
+    int restart;         /* FGMRES cycle length m */
+    int max_iter;        /* total iteration cap */
+    double tol;          /* relative residual target ||f - A u|| / ||f|| */
+    int stop_phys;       /* 1: test the physical-domain residual instead */
+    int device;          /* CUDA device ordinal */
+    int verbose;
+} helm3d_opts;
+
+typedef struct helm3d_stats {
+    int status;
+    int iterations;       /* Krylov iterations over all right-hand sides */
+    int restarts;
+    double relres;        /* true ||f - A u|| / ||f|| over the whole grid */
+    double relres_phys;   /* the same restricted to the physical domain */
+    double ms_factor;     /* set-up + factor time of helm3d_create */
+    double ms_solve;      /* device time of the last solve */
+    double *history;      /* optional caller buffer: residual estimate per iteration */
+    int history_cap;
+    int history_len;
+} helm3d_stats;
+
+typedef struct helm3d_ctx helm3d_ctx;
+
+/* Fill opts with defaults (mode N, C64 preconditioner, discrete kz symbol,
+ * beta_prec 0.25, restart 20, tol 1e-8). */
+int helm3d_default_opts(helm3d_opts *opts);
+
+/* Set up a solve on one device: PML tables, media (s2 = 1/c^2, real,
+ * nx*ny*nz, host or device), the kz table and the block LU factor of every
+ * kz system.  Replaces FGMRES's set-up block (Source/FGMRES.cpp:72-298). */
+int helm3d_create(const helm3d_grid *grid, const double *s2, const helm3d_opts *opts, helm3d_ctx **ctx);
+
+/* New medium on the same grid: recompute dL / shifts and refactor. */
+int helm3d_set_medium(helm3d_ctx *ctx, const double *s2);
+
+/* Solve for nrhs right-hand sides f[r*N .. ] -> u[r*N ..] with FGMRES.
+ * u on entry is the initial guess when stats->status == -1 on entry is not
+ * used; initial guess is zero.  Replaces FGMRES (Source/FGMRES.cpp:6-725,
+ * prototype Source/templates.h:59). */
+int helm3d_solve(helm3d_ctx *ctx, const double *f, double *u, int nrhs, helm3d_stats *stats);
+
+/* The same system by BiCGStab with the reference's shadow residual 2 r0.
+ * Replaces BCGSTAB (Source/BcGSTAB.cpp:6-666, Source/templates.h:60). */
+int helm3d_solve_bicgstab(helm3d_ctx *ctx, const double *f, double *u, helm3d_stats *stats);
+
+/* Adjoint solve A^H lambda = g (mode N), with M^H as the preconditioner. */
+int helm3d_solve_adjoint(helm3d_ctx *ctx, const double *g, double *lambda, helm3d_stats *stats);
+
+/* y = A x (mode N) or y = K x = x - dL L0^{-1} x (mode R,
+ * ApplyCoeffMatrixA_CSR, Source/functions.cpp:5554-5575). */
+int helm3d_apply_op(helm3d_ctx *ctx, const double *x, double *y);
+
+/* y = A^H x (mode N). */
+int helm3d_apply_op_adjoint(helm3d_ctx *ctx, const double *x, double *y);
+
+/* y = M^{-1} x: forward FFT along z, one 2D solve per kz, inverse FFT
+ * (Solve3DSparseUsingFT_CSR, Source/functions.cpp:5837-6061). */
+int helm3d_apply_prec(helm3d_ctx *ctx, const double *x, double *y);
+
+/* Gradient of J = 0.5 sum_s ||P u_s - d_s||^2 with respect to s2, where
+ * A u_s = f_s; P samples u at nrecv grid indices.  f: nsrc vectors, data:
+ * nsrc*nrecv complex, grad: N doubles (host or device), misfit: host. */
+int helm3d_misfit_grad(helm3d_ctx *ctx, const double *f, int nsrc, const long long *recv, int nrecv,
+                       const double *data, double *grad, double *misfit, helm3d_stats *stats);
+
+/* Order the context's work on a caller stream (cudaStream_t; NULL restores
+ * the context's own stream). */
+int helm3d_set_stream(helm3d_ctx *ctx, void *stream);
+
+/* Kernel families timed by the optional profiler. */
+typedef enum helm3d_kernel_kind {
+    HELM3D_K_FACTOR = 0,   /* block LU factor */
+    HELM3D_K_FFT_FWD = 1,  /* forward z-FFT */
+    HELM3D_K_SWEEP = 2,    /* block sweep */
+    HELM3D_K_FFT_INV = 3,  /* inverse z-FFT (+ mode R epilogue) */
+    HELM3D_K_STENCIL = 4,  /* 7-point operator */
+    HELM3D_K_KRYLOV = 5,   /* dots, updates, norms, combine */
+    HELM3D_K_COUNT = 6
+} helm3d_kernel_kind;
+
+/* enable = 1: record CUDA events around every launch on the launching
+ * stream; helm3d_profile_read returns the summed device time (ms) and launch
+ * count per kind, and clears them. */
+int helm3d_profile(helm3d_ctx *ctx, int enable);
+int helm3d_profile_read(helm3d_ctx *ctx, double *ms, long long *launches, int nkinds);
+
+/* Bytes of device memory held by the context. */
+size_t helm3d_device_bytes(const helm3d_ctx *ctx);
+
+/* Kernels launched by this context since creation (all entry points). */
+long long helm3d_kernel_launches(const helm3d_ctx *ctx);
+
+const char *helm3d_status_string(int status);
+const char *helm3d_last_error(const helm3d_ctx *ctx);
+
+int helm3d_destroy(helm3d_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HELM3D_H */

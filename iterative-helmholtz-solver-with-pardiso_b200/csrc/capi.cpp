@@ -1,0 +1,338 @@
+// capi.cpp -- the extern "C" entry points of include/helm3d.h.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "helm3d_internal.h"
+
+using namespace h3d;
+
+namespace {
+
+// message of the last failed helm3d_create on this thread (no context exists then)
+thread_local std::string g_create_error;
+
+bool is_device_ptr(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// A vector argument: device pointers are used in place, host data is staged.
+struct VecArg {
+    helm3d_ctx *c;
+    double2 *dev = nullptr;
+    bool staged = false;
+    int rc = HELM3D_OK;
+    VecArg(helm3d_ctx *ctx, const void *p, size_t count, bool copy_in, double2 **slot) : c(ctx) {
+        if (!p) { rc = set_error(c, HELM3D_ERR_ARG, "null vector argument"); return; }
+        if (is_device_ptr(p)) { dev = (double2 *)p; return; }
+        staged = true;
+        if (!*slot) {
+            rc = cuda_check(c, cudaMalloc((void **)slot, sizeof(double2) * count), "staging buffer");
+            if (rc) return;
+            c->bytes += sizeof(double2) * count;
+        }
+        dev = *slot;
+        if (copy_in)
+            rc = cuda_check(c, cudaMemcpyAsync(dev, p, sizeof(double2) * count, cudaMemcpyHostToDevice, c->stream),
+                            "copy in");
+    }
+    int copy_out(void *p, size_t count) {
+        if (!staged) return HELM3D_OK;
+        int r = cuda_check(c, cudaMemcpyAsync(p, dev, sizeof(double2) * count, cudaMemcpyDeviceToHost, c->stream),
+                           "copy out");
+        if (r) return r;
+        return cuda_check(c, cudaStreamSynchronize(c->stream), "copy out sync");
+    }
+};
+
+int validate(const helm3d_grid *g, const helm3d_opts *o) {
+    if (!g || !o) return HELM3D_ERR_ARG;
+    if (g->nx < 2 || g->ny < 2 || g->nz < 1) return HELM3D_ERR_ARG;
+    if (!(g->hx > 0) || !(g->hy > 0) || !(g->hz > 0) || !(g->omega > 0)) return HELM3D_ERR_ARG;
+    if (g->pml_x < 0 || g->pml_y < 0 || g->pml_z < 0 || g->spg_z < 0) return HELM3D_ERR_ARG;
+    if (2 * g->pml_x >= g->nx || 2 * g->pml_y >= g->ny) return HELM3D_ERR_ARG;
+    if (o->mode == HELM3D_MODE_R && 2 * g->spg_z >= g->nz) return HELM3D_ERR_ARG;
+    if (o->mode != HELM3D_MODE_R && o->mode != HELM3D_MODE_N) return HELM3D_ERR_ARG;
+    if (o->precision != HELM3D_PREC_C64 && o->precision != HELM3D_PREC_C128) return HELM3D_ERR_ARG;
+    if (o->kz_symbol < 0 || o->kz_symbol > 2) return HELM3D_ERR_ARG;
+    if (o->restart < 1 || o->restart > 1000 || o->max_iter < 0 || !(o->tol >= 0)) return HELM3D_ERR_ARG;
+    if (g->nz > 4096) return HELM3D_ERR_ARG;
+    return HELM3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int helm3d_default_opts(helm3d_opts *o) {
+    if (!o) return HELM3D_ERR_ARG;
+    memset(o, 0, sizeof(*o));
+    o->mode = HELM3D_MODE_N;
+    o->precision = HELM3D_PREC_C64;
+    o->kz_symbol = HELM3D_KZ_DISCRETE;
+    o->beta_prec = 0.25;
+    o->beta_phys = 0.0;
+    o->s2_l0 = 0.0;
+    o->quirk_q1 = 1;
+    o->restart = 20;
+    o->max_iter = 2000;
+    o->tol = 1e-8;
+    o->stop_phys = 0;
+    o->device = 0;
+    o->verbose = 0;
+    return HELM3D_OK;
+}
+
+const char *helm3d_status_string(int s) {
+    switch (s) {
+        case HELM3D_OK: return "ok";
+        case HELM3D_ERR_ARG: return "bad argument";
+        case HELM3D_ERR_OOM: return "out of device memory";
+        case HELM3D_ERR_CUDA: return "CUDA error";
+        case HELM3D_ERR_SINGULAR: return "singular block in the factor";
+        case HELM3D_ERR_NOT_CONVERGED: return "not converged";
+        case HELM3D_ERR_BREAKDOWN: return "Krylov breakdown";
+        case HELM3D_ERR_NONFINITE: return "non-finite value";
+        case HELM3D_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+const char *helm3d_last_error(const helm3d_ctx *c) { return c ? c->last_error.c_str() : g_create_error.c_str(); }
+
+size_t helm3d_device_bytes(const helm3d_ctx *c) { return c ? c->bytes : 0; }
+
+int helm3d_set_stream(helm3d_ctx *c, void *stream) {
+    if (!c) return HELM3D_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return HELM3D_OK;
+}
+
+int helm3d_profile(helm3d_ctx *c, int enable) {
+    if (!c) return HELM3D_ERR_ARG;
+    c->prof = enable != 0;
+    return HELM3D_OK;
+}
+
+int helm3d_profile_read(helm3d_ctx *c, double *ms, long long *launches, int nkinds) {
+    if (!c || nkinds < 0) return HELM3D_ERR_ARG;
+    cudaSetDevice(c->device);
+    int rc = cuda_check(c, cudaStreamSynchronize(c->stream), "profile sync");
+    if (rc) return rc;
+    for (auto &e : c->prof_ev) {
+        float t = 0;
+        if (cudaEventElapsedTime(&t, e.a, e.b) == cudaSuccess) c->prof_ms[e.kind] += t;
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    c->prof_ev.clear();
+    for (int k = 0; k < nkinds && k < HELM3D_K_COUNT; k++) {
+        if (ms) ms[k] = c->prof_ms[k];
+        if (launches) launches[k] = c->prof_n[k];
+    }
+    for (int k = 0; k < HELM3D_K_COUNT; k++) {
+        c->prof_ms[k] = 0;
+        c->prof_n[k] = 0;
+    }
+    return HELM3D_OK;
+}
+
+long long helm3d_kernel_launches(const helm3d_ctx *c) { return c ? c->launches : 0; }
+
+int helm3d_create(const helm3d_grid *grid, const double *s2, const helm3d_opts *opts, helm3d_ctx **out) {
+    if (!out) return HELM3D_ERR_ARG;
+    *out = nullptr;
+    int rc = validate(grid, opts);
+    if (rc) return rc;
+    if (!s2) return HELM3D_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return HELM3D_ERR_NO_DEVICE;
+    }
+    if (opts->device < 0 || opts->device >= ndev) return HELM3D_ERR_ARG;
+    helm3d_ctx *c = new (std::nothrow) helm3d_ctx();
+    if (!c) return HELM3D_ERR_OOM;
+    c->grid = *grid;
+    c->opts = *opts;
+    c->device = opts->device;
+    c->c64 = opts->precision == HELM3D_PREC_C64;
+    c->plane = (long)grid->nx * grid->ny;
+    c->N = c->plane * grid->nz;
+    if (cudaSetDevice(c->device) != cudaSuccess) {
+        delete c;
+        return HELM3D_ERR_CUDA;
+    }
+    auto fail = [&](int code) {
+        g_create_error = c->last_error;
+        helm3d_destroy(c);
+        return code;
+    };
+    if ((rc = cuda_check(c, cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking), "stream")) ||
+        (rc = cuda_check(c, cudaEventCreate(&c->ev0), "event")) ||
+        (rc = cuda_check(c, cudaEventCreate(&c->ev1), "event")))
+        return fail(rc);
+    c->stream = c->own_stream;
+    auto t0 = std::chrono::steady_clock::now();
+    // the medium is read on the host for the set-up tables
+    std::vector<double> s2h;
+    const double *s2p = s2;
+    if (is_device_ptr(s2)) {
+        s2h.resize(c->N);
+        if ((rc = cuda_check(c, cudaMemcpy(s2h.data(), s2, sizeof(double) * c->N, cudaMemcpyDeviceToHost), "s2")))
+            return fail(rc);
+        s2p = s2h.data();
+    }
+    for (long q = 0; q < c->N; q++)
+        if (!std::isfinite(s2p[q])) {
+            c->last_error = "medium has NaN/Inf";
+            return fail(HELM3D_ERR_NONFINITE);
+        }
+    if ((rc = ctx_setup_tables(c, s2p)) || (rc = ctx_factor(c))) return fail(rc);
+    c->ms_factor = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    g_create_error.clear();
+    *out = c;
+    return HELM3D_OK;
+}
+
+int helm3d_set_medium(helm3d_ctx *c, const double *s2) {
+    if (!c || !s2) return HELM3D_ERR_ARG;
+    cudaSetDevice(c->device);
+    std::vector<double> s2h;
+    const double *s2p = s2;
+    if (is_device_ptr(s2)) {
+        s2h.resize(c->N);
+        int rc = cuda_check(c, cudaMemcpy(s2h.data(), s2, sizeof(double) * c->N, cudaMemcpyDeviceToHost), "s2");
+        if (rc) return rc;
+        s2p = s2h.data();
+    }
+    for (long q = 0; q < c->N; q++)
+        if (!std::isfinite(s2p[q])) return HELM3D_ERR_NONFINITE;
+    int rc = ctx_setup_tables(c, s2p);
+    if (rc) return rc;
+    return ctx_factor(c);
+}
+
+static int solve_common(helm3d_ctx *c, const double *f, double *u, int nrhs, helm3d_stats *st, int which) {
+    if (!c || !f || !u || nrhs < 1) return HELM3D_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (st) {
+        st->iterations = 0;
+        st->restarts = 0;
+        st->ms_solve = 0;
+        st->relres = 0;
+        st->relres_phys = 0;
+        st->history_len = 0;
+    }
+    const bool fdev = is_device_ptr(f), udev = is_device_ptr(u);
+    int worst = HELM3D_OK;
+    double relres_max = 0, relphys_max = 0;
+    for (int r = 0; r < nrhs; r++) {
+        const double *fr = f + 2 * (size_t)r * c->N;
+        double *ur = u + 2 * (size_t)r * c->N;
+        VecArg fa(c, fr, c->N, true, &c->d_f);
+        if (fa.rc) return fa.rc;
+        VecArg ua(c, ur, c->N, false, &c->d_u);
+        if (ua.rc) return ua.rc;
+        (void)fdev;
+        (void)udev;
+        int rc;
+        if (which == 0) rc = fgmres(c, fa.dev, ua.dev, false, st);
+        else if (which == 1) rc = bicgstab(c, fa.dev, ua.dev, st);
+        else rc = fgmres(c, fa.dev, ua.dev, true, st);
+        if (rc && rc != HELM3D_ERR_NOT_CONVERGED) return rc;
+        if (rc) worst = rc;
+        int rc2 = ua.copy_out(ur, c->N);
+        if (rc2) return rc2;
+        if (st) {
+            relres_max = std::max(relres_max, st->relres);
+            relphys_max = std::max(relphys_max, st->relres_phys);
+        }
+    }
+    if (st) {
+        st->relres = relres_max;
+        st->relres_phys = relphys_max;
+        st->status = worst;
+    }
+    return worst;
+}
+
+int helm3d_solve(helm3d_ctx *c, const double *f, double *u, int nrhs, helm3d_stats *st) {
+    return solve_common(c, f, u, nrhs, st, 0);
+}
+
+int helm3d_solve_bicgstab(helm3d_ctx *c, const double *f, double *u, helm3d_stats *st) {
+    return solve_common(c, f, u, 1, st, 1);
+}
+
+int helm3d_solve_adjoint(helm3d_ctx *c, const double *g, double *lam, helm3d_stats *st) {
+    if (c && c->opts.mode != HELM3D_MODE_N) return set_error(c, HELM3D_ERR_ARG, "adjoint solve is mode N only");
+    return solve_common(c, g, lam, 1, st, 2);
+}
+
+static int apply_common(helm3d_ctx *c, const double *x, double *y, int which) {
+    if (!c || !x || !y) return HELM3D_ERR_ARG;
+    cudaSetDevice(c->device);
+    VecArg xa(c, x, c->N, true, &c->d_f);
+    if (xa.rc) return xa.rc;
+    VecArg ya(c, y, c->N, false, &c->d_u);
+    if (ya.rc) return ya.rc;
+    int rc;
+    if (which == 0) rc = apply_op(c, xa.dev, 1.0, ya.dev);
+    else if (which == 1) rc = apply_op_adjoint(c, xa.dev, 1.0, ya.dev);
+    else rc = apply_prec(c, xa.dev, 1.0, ya.dev);
+    if (rc) return rc;
+    rc = ya.copy_out(y, c->N);
+    if (rc) return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "apply");
+}
+
+int helm3d_apply_op(helm3d_ctx *c, const double *x, double *y) { return apply_common(c, x, y, 0); }
+int helm3d_apply_op_adjoint(helm3d_ctx *c, const double *x, double *y) { return apply_common(c, x, y, 1); }
+int helm3d_apply_prec(helm3d_ctx *c, const double *x, double *y) { return apply_common(c, x, y, 2); }
+
+int helm3d_misfit_grad(helm3d_ctx *c, const double *f, int nsrc, const long long *recv, int nrecv, const double *data,
+                       double *grad, double *misfit, helm3d_stats *st) {
+    (void)f;
+    (void)nsrc;
+    (void)recv;
+    (void)nrecv;
+    (void)data;
+    (void)grad;
+    (void)misfit;
+    (void)st;
+    return set_error(c, HELM3D_ERR_ARG, "misfit gradient not built yet");
+}
+
+int helm3d_destroy(helm3d_ctx *c) {
+    if (!c) return HELM3D_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void *bufs[] = {c->d_Gt, c->d_tw, c->d_cmx, c->d_cpx, c->d_cmy, c->d_cpy, c->d_base2d, c->d_kz2,
+                    c->d_cmx64, c->d_cpx64, c->d_cmy64, c->d_cpy64, c->d_cmz64, c->d_cpz64, c->d_s2, c->d_dl,
+                    c->d_planes, c->d_status, c->d_V, c->d_Z, c->d_vs, c->d_h, c->d_partials, c->d_f, c->d_u,
+                    c->d_r, c->d_t, c->d_t2, c->d_bic};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+    for (auto &e : c->prof_ev) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return HELM3D_OK;
+}
+
+}  // extern "C"

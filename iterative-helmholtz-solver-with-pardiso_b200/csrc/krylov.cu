@@ -1,0 +1,295 @@
+// krylov.cu -- complex128 vector kernels of the outer Krylov loop: the
+// Gram-Schmidt dot products and updates (the reference's zdotc/zaxpy loop,
+// Source/FGMRES.cpp:508-517), norms (dznrm2, :519; the physical-domain norm
+// after reducePML3D, :590-592), the solution update x = x0 + Z y (zgemv,
+// :575) and small helpers.  Reductions are two-level and deterministic:
+// fixed-size per-block partials, then one pass over the blocks.
+#include <cuda_runtime.h>
+
+#include "cplx.cuh"
+#include "helm3d_internal.h"
+
+namespace h3d {
+
+constexpr int kRedThreads = 256;
+constexpr int kDotChunk = 8;
+
+__device__ __forceinline__ double2 warp_sum(double2 v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
+    }
+    return v;
+}
+
+// block sum of CH complex values per thread; result valid in thread 0
+template <int CH> __device__ __forceinline__ void block_sum(double2 (&acc)[CH], double2 *sh /* [8][CH] */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < CH; q++) acc[q] = warp_sum(acc[q]);
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < CH; q++) sh[warp * CH + q] = acc[q];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kRedThreads / 32; w++)
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                acc[q].x += sh[w * CH + q].x;
+                acc[q].y += sh[w * CH + q].y;
+            }
+    }
+    __syncthreads();
+}
+
+// partials[b][i] = sum over this block's l of conj(V_i[l]) w[l] * vs[i]
+__global__ void __launch_bounds__(kRedThreads) dots_kernel(const double2 *__restrict__ V, long ldv,
+                                                           const double *__restrict__ vs, int nv,
+                                                           const double2 *__restrict__ w, long N,
+                                                           double2 *__restrict__ partials, int cap) {
+    __shared__ double2 sh[(kRedThreads / 32) * kDotChunk];
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (int c0 = 0; c0 < nv; c0 += kDotChunk) {
+        double2 acc[kDotChunk];
+#pragma unroll
+        for (int q = 0; q < kDotChunk; q++) acc[q] = make_double2(0, 0);
+        for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
+            const double2 wl = w[l];
+#pragma unroll
+            for (int q = 0; q < kDotChunk; q++)
+                if (c0 + q < nv) acc[q] = cfma(make_double2(V[(c0 + q) * ldv + l].x, -V[(c0 + q) * ldv + l].y), wl, acc[q]);
+        }
+        block_sum<kDotChunk>(acc, sh);
+        if (threadIdx.x == 0)
+            for (int q = 0; q < kDotChunk && c0 + q < nv; q++)
+                partials[(long)blockIdx.x * cap + c0 + q] = cscale(acc[q], vs ? vs[c0 + q] : 1.0);
+    }
+}
+
+// out[i] = sum_b partials[b][i]  (one thread per i, fixed order)
+__global__ void reduce_partials_kernel(const double2 *__restrict__ partials, int nblocks, int cap, int nv,
+                                       double2 *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    double2 s = make_double2(0, 0);
+    for (int b = 0; b < nblocks; b++) {
+        const double2 p = partials[(long)b * cap + i];
+        s.x += p.x;
+        s.y += p.y;
+    }
+    out[i] = s;
+}
+
+// w -= sum_i coef[i] vs[i] V_i ; post: 0 none, 1 ||w_new||^2 partial into partials[b][0]
+__global__ void __launch_bounds__(kRedThreads) update_kernel(const double2 *__restrict__ V, long ldv,
+                                                             const double *__restrict__ vs, int nv,
+                                                             const double2 *__restrict__ coef,
+                                                             double2 *__restrict__ w, long N, int post,
+                                                             double2 *__restrict__ partials, int cap) {
+    extern __shared__ double2 sc[];  // nv coefficients (coef * vs)
+    __shared__ double2 sh[(kRedThreads / 32)];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) sc[i] = cscale(coef[i], vs ? vs[i] : 1.0);
+    __syncthreads();
+    double2 nrm[1] = {make_double2(0, 0)};
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
+        double2 acc = w[l];
+        for (int i = 0; i < nv; i++) acc = cfms(sc[i], V[i * ldv + l], acc);
+        w[l] = acc;
+        nrm[0].x += acc.x * acc.x + acc.y * acc.y;
+    }
+    if (post == 1) {
+        block_sum<1>(nrm, sh);
+        if (threadIdx.x == 0) partials[(long)blockIdx.x * cap] = nrm[0];
+    }
+}
+
+// x += sum_i y[i] zs[i] Z_i
+__global__ void __launch_bounds__(kRedThreads) combine_kernel(const double2 *__restrict__ Z, long ldz,
+                                                              const double *__restrict__ zs, int nzv,
+                                                              const double2 *__restrict__ y, double2 *__restrict__ x,
+                                                              long N) {
+    extern __shared__ double2 sc[];
+    for (int i = threadIdx.x; i < nzv; i += blockDim.x) sc[i] = cscale(y[i], zs ? zs[i] : 1.0);
+    __syncthreads();
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
+        double2 acc = x[l];
+        for (int i = 0; i < nzv; i++) acc = cfma(sc[i], Z[i * ldz + l], acc);
+        x[l] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads) norm2_box_kernel(const double2 *__restrict__ x, int nx, int ny,
+                                                                int x0, int x1, int y0, int y1, int z0, int z1,
+                                                                double2 *__restrict__ partials, int cap) {
+    __shared__ double2 sh[(kRedThreads / 32)];
+    const long bx = x1 - x0, by = y1 - y0, bz = z1 - z0;
+    const long total = bx * by * bz;
+    double2 acc[1] = {make_double2(0, 0)};
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
+        const long i = q % bx, t = q / bx;
+        const long j = t % by, k = t / by;
+        const double2 v = x[((k + z0) * ny + (j + y0)) * (long)nx + (i + x0)];
+        acc[0].x += v.x * v.x + v.y * v.y;
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partials[(long)blockIdx.x * cap] = acc[0];
+}
+
+__global__ void axpby_kernel(double2 a, const double2 *__restrict__ x, double2 b, double2 *__restrict__ y, long N) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
+        const double2 yv = y[l], xv = x[l];
+        y[l] = cadd(cmul(a, xv), cmul(b, yv));
+    }
+}
+
+__global__ void sub_dl_kernel(const double2 *__restrict__ x, const double2 *__restrict__ dl,
+                              const double2 *__restrict__ t, double2 *__restrict__ y, long N) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) y[l] = csub(x[l], cmul(dl[l], t[l]));
+}
+
+__global__ void set_scale_kernel(const double2 *nrm, double *vs, int j) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const double s = sqrt(nrm[0].x);
+        vs[j] = s > 0 ? 1.0 / s : 0.0;
+    }
+}
+
+__global__ void add_vec_kernel(const double2 *a, const double2 *b, double2 *out, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = cadd(a[i], b[i]);
+}
+
+__global__ void grad_accum_kernel(const double2 *__restrict__ lam, const double2 *__restrict__ u, double w2,
+                                  double beta, double *__restrict__ g, long N) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
+        // dA/ds2 = w2 (1 + i beta); contribution Re( conj(lam) * dA/ds2 * u )
+        const double2 du = cmul(make_double2(w2, w2 * beta), u[l]);
+        const double2 lv = lam[l];
+        g[l] += lv.x * du.x + lv.y * du.y;
+    }
+}
+
+__global__ void gather_residual_kernel(const double2 *__restrict__ u, const long long *__restrict__ recv, int nrecv,
+                                       const double2 *__restrict__ d, double2 *__restrict__ res) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < nrecv) res[q] = csub(u[recv[q]], d[q]);
+}
+
+__global__ void scatter_add_kernel(const double2 *__restrict__ vals, const long long *__restrict__ recv, int nrecv,
+                                   double2 *__restrict__ y, double sign) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < nrecv) {
+        const long long l = recv[q];
+        y[l] = make_double2(y[l].x + sign * vals[q].x, y[l].y + sign * vals[q].y);
+    }
+}
+
+static inline bool ok() { return cudaGetLastError() == cudaSuccess; }
+
+static int grid_for(long N) {
+    const long b = (N + kRedThreads - 1) / kRedThreads;
+    const long cap = 4L * device_info().sm_count;
+    return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+int launch_dots(const double2 *V, long ldv, const double *vs, int nv, const double2 *w, long N, const Reduce &red,
+                double2 *out, cudaStream_t s) {
+    if (nv > red.cap) return HELM3D_ERR_ARG;
+    const int nb = red.nblocks;
+    dots_kernel<<<nb, kRedThreads, 0, s>>>(V, ldv, vs, nv, w, N, red.partials, red.cap);
+    reduce_partials_kernel<<<(nv + 127) / 128, 128, 0, s>>>(red.partials, nb, red.cap, nv, out);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_update(const double2 *V, long ldv, const double *vs, int nv, const double2 *coef, double2 *w, long N,
+                  int post, const Reduce &red, double2 *out, cudaStream_t s) {
+    const int nb = post ? red.nblocks : grid_for(N);
+    update_kernel<<<nb, kRedThreads, sizeof(double2) * (nv > 0 ? nv : 1), s>>>(V, ldv, vs, nv, coef, w, N, post,
+                                                                               red.partials, red.cap);
+    if (post == 1) reduce_partials_kernel<<<1, 32, 0, s>>>(red.partials, nb, red.cap, 1, out);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_combine(const double2 *Z, long ldz, const double *zs, int nzv, const double2 *y, double2 *x, long N,
+                   cudaStream_t s) {
+    combine_kernel<<<grid_for(N), kRedThreads, sizeof(double2) * (nzv > 0 ? nzv : 1), s>>>(Z, ldz, zs, nzv, y, x, N);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_norm2_box(const double2 *x, int nx, int ny, int nz, const int box[6], const Reduce &red, double2 *out,
+                     cudaStream_t s) {
+    (void)nz;
+    norm2_box_kernel<<<red.nblocks, kRedThreads, 0, s>>>(x, nx, ny, box[0], box[1], box[2], box[3], box[4], box[5],
+                                                         red.partials, red.cap);
+    reduce_partials_kernel<<<1, 32, 0, s>>>(red.partials, red.nblocks, red.cap, 1, out);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_axpby(double2 a, const double2 *x, double2 b, double2 *y, long N, cudaStream_t s) {
+    axpby_kernel<<<grid_for(N), kRedThreads, 0, s>>>(a, x, b, y, N);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_sub_dl(const double2 *x, const double2 *dl, const double2 *t, double2 *y, long N, cudaStream_t s) {
+    sub_dl_kernel<<<grid_for(N), kRedThreads, 0, s>>>(x, dl, t, y, N);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_set_scale(const double2 *nrm, double *vs, int j, cudaStream_t s) {
+    set_scale_kernel<<<1, 32, 0, s>>>(nrm, vs, j);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_add_vec(const double2 *a, const double2 *b, double2 *out, int n, cudaStream_t s) {
+    add_vec_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, b, out, n);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_zero(void *p, size_t bytes, cudaStream_t s) {
+    return cudaMemsetAsync(p, 0, bytes, s) == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_grad_accum(const double2 *lam, const double2 *u, double w2, double beta, double *g, long N,
+                      cudaStream_t s) {
+    grad_accum_kernel<<<grid_for(N), kRedThreads, 0, s>>>(lam, u, w2, beta, g, N);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_gather_residual(const double2 *u, const long long *recv, int nrecv, const double2 *d, double2 *res,
+                           cudaStream_t s) {
+    if (nrecv <= 0) return HELM3D_OK;
+    gather_residual_kernel<<<(nrecv + 255) / 256, 256, 0, s>>>(u, recv, nrecv, d, res);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_scatter_add(const double2 *vals, const long long *recv, int nrecv, double2 *y, double sign,
+                       cudaStream_t s) {
+    if (nrecv <= 0) return HELM3D_OK;
+    scatter_add_kernel<<<(nrecv + 255) / 256, 256, 0, s>>>(vals, recv, nrecv, y, sign);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+Dev &device_info() {
+    static Dev d;
+    static bool init = false;
+    if (!init) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, dev) == cudaSuccess) {
+            d.sm_count = p.multiProcessorCount;
+            d.smem_optin = p.sharedMemPerBlockOptin;
+        }
+        init = true;
+    }
+    return d;
+}
+
+}  // namespace h3d

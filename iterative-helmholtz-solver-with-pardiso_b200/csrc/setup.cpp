@@ -1,0 +1,284 @@
+// setup.cpp -- host (FP64) set-up of a solve: PML coefficient tables, the
+// z-averaged medium of the preconditioner, dL (mode R), the kz table, the FFT
+// plan, device uploads and the block LU factor.  Replaces the set-up block of
+// FGMRES (Source/FGMRES.cpp:72-298).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "helm3d_internal.h"
+
+namespace h3d {
+
+static const double kPi = 3.141592653589793238462643;
+
+// d(x) = 1000 x^2 (Source/functions.cpp:893-906)
+static double d_pml(double x) { return 1000.0 * x * x; }
+
+// alpha(size_m, double) (Source/functions.cpp:1839-1878): -i w / (d(x) - i w)
+// inside the PML, 1 outside; the left test i < pml includes i = pml - 1/2.
+static zc alpha(int n, int pml, double i, double omega) {
+    if (pml == 0) return zc(1.0, 0.0);
+    const double h = 1.0 / pml;
+    if (i < pml || i >= (n - pml)) {
+        double x;
+        if (i < pml) x = 1.0 - i * h;
+        else x = 1.0 + (i - n + 1) * h;
+        return zc(0.0, -omega) / zc(d_pml(x), -omega);
+    }
+    return zc(1.0, 0.0);
+}
+
+// cm[i] = alpha(i) alpha(i-1/2)/h^2, cp[i] = alpha(i) alpha(i+1/2)/h^2
+// (beta2D_pml cases -1/+1, -2/+2: Source/functions.cpp:2385-2399)
+static void pml_table(int n, int pml, double h, double omega, std::vector<zc> &cm, std::vector<zc> &cp) {
+    cm.resize(n);
+    cp.resize(n);
+    const double h2 = h * h;
+    for (int i = 0; i < n; i++) {
+        const zc a = alpha(n, pml, (double)i, omega);
+        cm[i] = a * alpha(n, pml, i - 0.5, omega) / h2;
+        cp[i] = a * alpha(n, pml, i + 0.5, omega) / h2;
+    }
+}
+
+void build_fft_plan(int n, FftPlan &plan, std::vector<zc> &tables) {
+    plan = FftPlan();
+    plan.n = n;
+    int rem = n;
+    std::vector<int> rad;
+    while (rem % 8 == 0) { rad.push_back(8); rem /= 8; }
+    while (rem % 4 == 0) { rad.push_back(4); rem /= 4; }
+    while (rem % 2 == 0) { rad.push_back(2); rem /= 2; }
+    for (int p : {3, 5, 7}) while (rem % p == 0) { rad.push_back(p); rem /= p; }
+    for (int p = 11; rem > 1; p += 2)
+        while (rem % p == 0) { rad.push_back(p); rem /= p; }
+    if (rad.empty()) rad.push_back(1);
+    plan.npass = (int)rad.size();
+    tables.clear();
+    int span = 1;
+    for (int s = 0; s < plan.npass; s++) {
+        const int r = rad[s];
+        plan.radix[s] = r;
+        plan.span[s] = span;
+        plan.twoff[s] = (int)tables.size();
+        for (int k = 0; k < span; k++)
+            for (int q = 0; q < r; q++) {
+                const long e = (long)q * k;
+                const long mod = (long)span * r;
+                const double ang = -2.0 * kPi * (double)(e % mod) / (double)mod;
+                tables.push_back(zc(std::cos(ang), std::sin(ang)));
+            }
+        plan.dftoff[s] = (int)tables.size();
+        for (int t = 0; t < r; t++) {
+            const double ang = -2.0 * kPi * (double)t / (double)r;
+            tables.push_back(zc(std::cos(ang), std::sin(ang)));
+        }
+        span *= r;
+    }
+    plan.twlen = (int)tables.size();
+}
+
+int set_error(helm3d_ctx *c, int code, const std::string &msg) {
+    if (c) c->last_error = msg;
+    return code;
+}
+
+int cuda_check(helm3d_ctx *c, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return HELM3D_OK;
+    const int code = (e == cudaErrorMemoryAllocation) ? HELM3D_ERR_OOM : HELM3D_ERR_CUDA;
+    return set_error(c, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+static int dalloc(helm3d_ctx *c, void **p, size_t bytes, const char *what) {
+    if (*p) return HELM3D_OK;
+    const int rc = cuda_check(c, cudaMalloc(p, bytes), what);
+    if (rc == HELM3D_OK) c->bytes += bytes;
+    return rc;
+}
+
+// upload a complex table in the preconditioner precision
+static int upload_c(helm3d_ctx *c, void **dst, const std::vector<zc> &v, const char *what) {
+    const size_t esz = c->c64 ? 8 : 16;
+    int rc = dalloc(c, dst, v.size() * esz + 16, what);
+    if (rc) return rc;
+    if (c->c64) {
+        std::vector<float> tmp(2 * v.size());
+        for (size_t i = 0; i < v.size(); i++) {
+            tmp[2 * i] = (float)v[i].real();
+            tmp[2 * i + 1] = (float)v[i].imag();
+        }
+        return cuda_check(c, cudaMemcpy(*dst, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice), what);
+    }
+    return cuda_check(c, cudaMemcpy(*dst, v.data(), v.size() * 16, cudaMemcpyHostToDevice), what);
+}
+
+static int upload_c64(helm3d_ctx *c, double2 **dst, const std::vector<zc> &v, const char *what) {
+    int rc = dalloc(c, (void **)dst, v.size() * 16 + 16, what);
+    if (rc) return rc;
+    return cuda_check(c, cudaMemcpy(*dst, v.data(), v.size() * 16, cudaMemcpyHostToDevice), what);
+}
+
+int ctx_setup_tables(helm3d_ctx *c, const double *s2) {
+    const helm3d_grid &g = c->grid;
+    const helm3d_opts &o = c->opts;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const double w = g.omega, w2 = w * w;
+    pml_table(nx, g.pml_x, g.hx, w, c->cmx, c->cpx);
+    pml_table(ny, g.pml_y, g.hy, w, c->cmy, c->cpy);
+    pml_table(nz, g.pml_z, g.hz, w, c->cmz, c->cpz);
+
+    // kz table
+    const double lz = g.lz > 0 ? g.lz : nz * g.hz;
+    c->kz2.assign(nz, 0.0);
+    for (int k = 0; k < nz; k++) {
+        double v;
+        if (o.kz_symbol == HELM3D_KZ_DISCRETE) {
+            const double s = std::sin(kPi * k / nz);
+            v = 4.0 / (g.hz * g.hz) * s * s;
+        } else if (o.kz_symbol == HELM3D_KZ_CONTINUOUS) {
+            const int kk = std::min(k, nz - k);
+            v = (2.0 * kPi * kk / lz) * (2.0 * kPi * kk / lz);
+        } else {
+            // Source/FGMRES.cpp:182-190: k < nz/2 - 1 -> k, else nz - k
+            const int kk = (k < nz / 2 - 1) ? k : nz - k;
+            v = 4.0 * kPi * kPi * (double)kk * (double)kk / (lz * lz);
+        }
+        c->kz2[k] = v;
+    }
+
+    // z-mean slowness of the preconditioner, per (j, i)
+    c->base2d.assign((size_t)nx * ny, zc(0, 0));
+    std::vector<double> dl_s0(0);
+    if (o.mode == HELM3D_MODE_N) {
+        int zlo = g.pml_z, zhi = nz - g.pml_z;
+        if (zhi <= zlo) { zlo = 0; zhi = nz; }
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) {
+                double s = 0;
+                for (int k = zlo; k < zhi; k++) s += s2[((long)k * ny + j) * nx + i];
+                s /= (zhi - zlo);
+                c->base2d[(size_t)j * nx + i] = w2 * s * zc(1.0, o.beta_prec);
+            }
+    } else {
+        // mode R: SetSoundSpeed2D (Source/functions.cpp:1686-1738) over the
+        // physical x,y range and the non-sponge z range, j outer / i inner;
+        // with q1 the accumulator carries over between columns.  Then the
+        // edge extension into the x,y PML (Source/functions.cpp:2636-2673).
+        const int spg = g.spg_z, nzp = nz - 2 * spg;
+        std::vector<double> s0((size_t)nx * ny, 0.0);
+        double acc = 0.0;
+        for (int j = g.pml_y; j < ny - g.pml_y; j++)
+            for (int i = g.pml_x; i < nx - g.pml_x; i++) {
+                double col = 0.0;
+                for (int k = spg; k < nz - spg; k++) col += s2[((long)k * ny + j) * nx + i];
+                acc = o.quirk_q1 ? (acc + col) / nzp : col / nzp;
+                const double c0 = std::sqrt(1.0 / acc);
+                s0[(size_t)j * nx + i] = 1.0 / (c0 * c0);
+            }
+        for (int j = 0; j < ny; j++) {
+            for (int i = 0; i < g.pml_x; i++) s0[(size_t)j * nx + i] = s0[(size_t)j * nx + g.pml_x];
+            for (int i = nx - g.pml_x; i < nx; i++) s0[(size_t)j * nx + i] = s0[(size_t)j * nx + nx - g.pml_x - 1];
+        }
+        for (int i = 0; i < nx; i++) {
+            for (int j = 0; j < g.pml_y; j++) s0[(size_t)j * nx + i] = s0[(size_t)g.pml_y * nx + i];
+            for (int j = ny - g.pml_y; j < ny; j++) s0[(size_t)j * nx + i] = s0[(size_t)(ny - g.pml_y - 1) * nx + i];
+        }
+        for (size_t q = 0; q < s0.size(); q++)
+            c->base2d[q] = w2 * (o.s2_l0 > 0 ? o.s2_l0 : s0[q]) * zc(1.0, o.beta_prec);   // q3
+        // dL (Source/functions.cpp:1740-1824)
+        std::vector<zc> dl((size_t)c->N, zc(0, 0));
+        const long pl = c->plane;
+        for (int k = spg; k <= nz - spg && k < nz; k++)
+            for (long q = 0; q < pl; q++)
+                dl[(size_t)k * pl + q] = w2 * (zc(1.0, o.beta_prec) * s0[q] - s2[(size_t)k * pl + q]);
+        const double sigma = 0.3, lzz = g.lz > 0 ? g.lz : nz * g.hz;
+        const double z0 = spg * g.hz, zN = (nz - spg) * g.hz, L0 = z0, Ln = lzz - zN;
+        for (int k = 0; k < spg; k++) {
+            const double zp = k * g.hz;
+            const double e = std::exp(-(zp - z0) * (zp - z0) / (L0 * L0) / (sigma * sigma));
+            for (long q = 0; q < pl; q++) dl[(size_t)k * pl + q] = dl[(size_t)spg * pl + q] * e;
+        }
+        for (int k = nz - spg + 1; k < nz; k++) {
+            const double zp = k * g.hz;
+            const double e = std::exp(-(zp - zN) * (zp - zN) / (Ln * Ln) / (sigma * sigma));
+            for (long q = 0; q < pl; q++) dl[(size_t)k * pl + q] = dl[(size_t)(nz - spg) * pl + q] * e;
+        }
+        int rc = upload_c64(c, &c->d_dl, dl, "dL");
+        if (rc) return rc;
+    }
+
+    // device tables
+    int rc;
+    if ((rc = upload_c(c, &c->d_cmx, c->cmx, "cmx")) || (rc = upload_c(c, &c->d_cpx, c->cpx, "cpx")) ||
+        (rc = upload_c(c, &c->d_cmy, c->cmy, "cmy")) || (rc = upload_c(c, &c->d_cpy, c->cpy, "cpy")) ||
+        (rc = upload_c(c, &c->d_base2d, c->base2d, "base2d")))
+        return rc;
+    if ((rc = upload_c64(c, &c->d_cmx64, c->cmx, "cmx64")) || (rc = upload_c64(c, &c->d_cpx64, c->cpx, "cpx64")) ||
+        (rc = upload_c64(c, &c->d_cmy64, c->cmy, "cmy64")) || (rc = upload_c64(c, &c->d_cpy64, c->cpy, "cpy64")) ||
+        (rc = upload_c64(c, &c->d_cmz64, c->cmz, "cmz64")) || (rc = upload_c64(c, &c->d_cpz64, c->cpz, "cpz64")))
+        return rc;
+    {
+        const size_t esz = c->c64 ? 4 : 8;
+        if ((rc = dalloc(c, &c->d_kz2, nz * esz + 16, "kz2"))) return rc;
+        if (c->c64) {
+            std::vector<float> t(c->kz2.begin(), c->kz2.end());
+            rc = cuda_check(c, cudaMemcpy(c->d_kz2, t.data(), nz * 4, cudaMemcpyHostToDevice), "kz2");
+        } else {
+            rc = cuda_check(c, cudaMemcpy(c->d_kz2, c->kz2.data(), nz * 8, cudaMemcpyHostToDevice), "kz2");
+        }
+        if (rc) return rc;
+    }
+    if (o.mode == HELM3D_MODE_N) {
+        if ((rc = dalloc(c, (void **)&c->d_s2, sizeof(double) * c->N, "s2"))) return rc;
+        if ((rc = cuda_check(c, cudaMemcpy(c->d_s2, s2, sizeof(double) * c->N, cudaMemcpyHostToDevice), "s2")))
+            return rc;
+    }
+    // FFT tables
+    std::vector<zc> tw;
+    build_fft_plan(nz, c->plan, tw);
+    if ((rc = upload_c(c, &c->d_tw, tw, "fft tables"))) return rc;
+    // planes, status, factor storage
+    const size_t esz = c->c64 ? 8 : 16;
+    if ((rc = dalloc(c, &c->d_planes, esz * c->N + 256, "planes"))) return rc;
+    if ((rc = dalloc(c, (void **)&c->d_status, 64, "status"))) return rc;
+    c->ldg = (nx + 3) & ~3;
+    c->Gt_bytes = esz * (size_t)nz * ny * nx * c->ldg;
+    if ((rc = dalloc(c, &c->d_Gt, c->Gt_bytes, "block LU factor"))) return rc;
+    return HELM3D_OK;
+}
+
+int ctx_factor(helm3d_ctx *c) {
+    if (!factor_supported(c->c64, c->grid.nx))
+        return set_error(c, HELM3D_ERR_ARG, "nx beyond the supported block size of the factor");
+    int rc = cuda_check(c, cudaMemsetAsync(c->d_status, 0, 64, c->stream), "status reset");
+    if (rc) return rc;
+    FactorArgs a;
+    a.n = c->grid.nx;
+    a.ny = c->grid.ny;
+    a.nz = c->grid.nz;
+    a.ldg = c->ldg;
+    a.Gt = c->d_Gt;
+    a.cmx = c->d_cmx;
+    a.cpx = c->d_cpx;
+    a.cmy = c->d_cmy;
+    a.cpy = c->d_cpy;
+    a.base2d = c->d_base2d;
+    a.kz2 = c->d_kz2;
+    a.status = c->d_status;
+    rc = timed(c, HELM3D_K_FACTOR, 1, [&] { return launch_factor(c->c64, a, c->stream); });
+    if (rc) return set_error(c, rc, std::string("factor launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+    int st = 0;
+    rc = cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");
+    if (rc) return rc;
+    rc = cuda_check(c, cudaStreamSynchronize(c->stream), "factor");
+    if (rc) return rc;
+    if (st & 1) return set_error(c, HELM3D_ERR_SINGULAR, "zero pivot in the block LU factor");
+    if (st & 2) return set_error(c, HELM3D_ERR_CUDA, "factor: a bounded wait expired");
+    if (st & 8) return set_error(c, HELM3D_ERR_CUDA, "factor: an index check failed");
+    return HELM3D_OK;
+}
+
+}  // namespace h3d

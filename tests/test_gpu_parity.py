@@ -1,0 +1,120 @@
+"""CUDA path against the oracle on the same seeded inputs (needs a B200).
+
+Tolerances: complex128 kernels (stencil, FFT + block LU + sweep in c128)
+agree with the FP64 oracle to 1e-10 relative; the complex64 preconditioner
+to 2e-5; full solves reach the requested relative residual and a solution
+relative error <= 1e-6 against the FP64 oracle solution.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from helpers import mode_n_solver, mode_r_case, mode_r_solver, rand_c, rel, small_problem
+from oracle import grid as ogrid
+from oracle import media, mode_n, mode_r
+
+pytestmark = pytest.mark.gpu
+
+
+# ----------------------------------------------------------------- mode R
+@pytest.mark.parametrize("case", [(10, 4, 3), (11, 4, 3), (16, 6, 4)])
+def test_mode_r_l0_inverse_and_k(case):
+    g, st = mode_r_case(*case)
+    s = mode_r_solver(g, st)
+    v = rand_c(g.shape_zyx, seed=3)
+    assert rel(s.apply_prec(v), st.l0_solve(v)) < 1e-10          # Solve3DSparseUsingFT_CSR
+    assert rel(s.apply_op(v), st.apply_k(v)) < 1e-10             # ApplyCoeffMatrixA_CSR
+
+
+@pytest.mark.parametrize("tag", ["n10p4s3", "n11p4s3", "n16p6s4"])
+def test_mode_r_solve_matches_oracle_and_reference(tag):
+    z = np.load(os.path.join(GOLDEN, f"ref_fgmres_{tag}.npz"))
+    n, pml, spg, beta, niter, rest = z["params"]
+    g, st = mode_r_case(int(n), int(pml), int(spg), beta=float(beta))
+    s = mode_r_solver(g, st, beta=float(beta), tol=1e-11, max_iter=3000)
+    f = z["f"]
+    u = s.solve(f)
+    assert s.last_stats.relres < 1e-10
+    # FP64 oracle solution of A_R u = f: GMRES on K to 1e-12, then u = L0^{-1} w
+    w = mode_n.fgmres(st.apply_k, lambda v: v, f, tol=1e-12, m=30, max_iter=3000).x
+    assert rel(u, st.l0_solve(w)) < 1e-6
+    # where the reference reached its own exit (physical residual < 1e-4,
+    # Source/FGMRES.cpp:650) its solution agrees to that level; the n16p6s4
+    # run ended its 32 iterations at 4.6e-2 and is compared to the oracle only
+    if z["conv"][-1][2] < 1e-4:
+        assert rel(u, z["x_sol"]) < 5e-3
+
+
+# ----------------------------------------------------------------- mode N
+def test_mode_n_stencil_and_adjoint():
+    p = small_problem(20, 18, 16, pml=4)
+    on = mode_n.setup(p, factor=False)
+    s = mode_n_solver(p, precision=0)
+    x = rand_c(p.shape, seed=1)
+    y = rand_c(p.shape, seed=2)
+    assert rel(s.apply_op(x), on.apply_a(x)) < 1e-13
+    assert rel(s.apply_op_adjoint(x), on.apply_a_adjoint(x)) < 1e-13
+    # <A x, y> = <x, A^H y>
+    lhs = np.vdot(y, s.apply_op(x))
+    rhs = np.vdot(s.apply_op_adjoint(y), x)
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+@pytest.mark.parametrize("nz", [16, 17, 24, 30, 48, 49, 64])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_mode_n_preconditioner(nz, prec):
+    """FFT along z (power-of-two, mixed radix, prime lengths) + block LU + sweep."""
+    p = small_problem(20, 18, nz, pml=4, seed=nz)
+    on = mode_n.setup(p, beta_prec=0.25)
+    s = mode_n_solver(p, precision=prec, beta_prec=0.25)
+    v = rand_c(p.shape, seed=nz)
+    tol = 1e-10 if prec == 0 else 2e-5
+    assert rel(s.apply_prec(v), on.apply_prec(v)) < tol
+
+
+@pytest.mark.parametrize("nx", [32, 40, 64, 65, 96, 128])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_mode_n_block_sizes(nx, prec):
+    """Block LU at every padded block size / cluster shape the factor uses."""
+    p = small_problem(nx, 12, 8, pml=3, seed=nx)
+    on = mode_n.setup(p, beta_prec=0.25)
+    s = mode_n_solver(p, precision=prec, beta_prec=0.25)
+    v = rand_c(p.shape, seed=1)
+    tol = 1e-9 if prec == 0 else 5e-5
+    assert rel(s.apply_prec(v), on.apply_prec(v)) < tol
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_mode_n_fgmres_solution(prec):
+    p = media.config_small(24, 4, seed=5)
+    f = p.rhs(0)
+    on = mode_n.setup(p, beta_prec=0.25)
+    ref = mode_n.fgmres(on.apply_a, on.apply_prec, f, tol=1e-12, m=40, max_iter=3000)
+    s = mode_n_solver(p, precision=prec, tol=1e-10)
+    u = s.solve(f)
+    st = s.last_stats
+    assert st.relres < 1e-10
+    assert rel(u, ref.x) < 1e-6
+    # true residual recomputed by the oracle
+    assert np.linalg.norm(on.apply_a(u) - f) / np.linalg.norm(f) < 2e-10
+
+
+def test_mode_n_bicgstab():
+    p = media.config_small(20, 4, seed=9)
+    f = p.rhs(0)
+    on = mode_n.setup(p, factor=False)
+    s = mode_n_solver(p, precision=0, tol=1e-9)
+    u = s.solve_bicgstab(f)
+    assert np.linalg.norm(on.apply_a(u) - f) / np.linalg.norm(f) < 1e-8
+
+
+def test_multiple_right_hand_sides():
+    p = media.config_small(20, 4, seed=4, n_sources=3)
+    F = np.stack([p.rhs(i) for i in range(3)])
+    s = mode_n_solver(p, precision=1, tol=1e-9)
+    U = s.solve(F, nrhs=3)
+    on = mode_n.setup(p, factor=False)
+    for i in range(3):
+        assert np.linalg.norm(on.apply_a(U[i]) - F[i]) / np.linalg.norm(F[i]) < 2e-9
