@@ -15,15 +15,6 @@ namespace {
 // message of the last failed helm3d_create on this thread (no context exists then)
 thread_local std::string g_create_error;
 
-bool is_device_ptr(const void *p) {
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
 // A vector argument: device pointers are used in place, host data is staged.
 struct VecArg {
     helm3d_ctx *c;

@@ -221,6 +221,7 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, bool adjoint, helm3d_sta
 int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st);
 int ensure_krylov(helm3d_ctx *c, int m);
 int set_error(helm3d_ctx *c, int code, const std::string &msg);
+bool is_device_ptr(const void *p);   // device or managed memory
 int cuda_check(helm3d_ctx *c, cudaError_t e, const char *what);
 void build_fft_plan(int n, FftPlan &plan, std::vector<zc> &tables);
 }  // namespace h3d

@@ -81,6 +81,15 @@ void build_fft_plan(int n, FftPlan &plan, std::vector<zc> &tables) {
     plan.twlen = (int)tables.size();
 }
 
+bool is_device_ptr(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 int set_error(helm3d_ctx *c, int code, const std::string &msg) {
     if (c) c->last_error = msg;
     return code;
