@@ -1,0 +1,90 @@
+// noalloc.cu -- helm3d_apply_prec_noalloc: the preconditioner apply
+// (forward z-FFT, per-kz block sweep, inverse z-FFT) with its scratch, the
+// spectral planes, in a fixed device array of this library instead of memory
+// the call allocates.
+//
+// Some callers cannot call cudaMalloc where they apply the preconditioner:
+// code that runs inside a device-memory allocator or pool callback (it must
+// not re-enter the allocator), processes whose free device memory is already
+// reserved by a framework's caching allocator, and latency-bound loops that
+// must stay off the driver's allocation path (cudaMalloc can synchronize the
+// device).  This entry point allocates nothing: the caller passes device
+// input and output vectors, the factor and tables were allocated when the
+// context was created, and the planes live in kScratchBytes (8 MiB) of static
+// device memory that every GPU which loads the library holds until the
+// process exits.  Grids whose planes need more (nx*ny*nz*8 bytes for the
+// complex64 preconditioner, *16 for complex128) are rejected.
+//
+// The array name is only a host-side stand-in for the device symbol: the
+// device address is looked up once per device with cudaGetSymbolAddress (on
+// the first call on that device, with the device current), cached, and
+// passed to the kernels.  That first call should therefore come before any
+// stream capture.  All calls share the array and it keeps the last call's
+// contents; every call overwrites all planes it reads, so nothing needs
+// clearing.  Calls whose work overlaps on the GPU (different streams or
+// contexts at the same time) race on the array.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "helm3d_internal.h"
+
+namespace {
+
+constexpr size_t kScratchBytes = size_t(8) << 20;
+constexpr int kMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_plane_scratch[kScratchBytes];
+
+std::mutex g_mu;
+void *g_scratch_addr[kMaxDevices] = {};
+
+}  // namespace
+
+extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double *y) {
+    using namespace h3d;
+    if (!c || !x || !y) return HELM3D_ERR_ARG;
+    if (c->device < 0 || c->device >= kMaxDevices) return set_error(c, HELM3D_ERR_ARG, "device ordinal too large");
+    int rc = cuda_check(c, cudaSetDevice(c->device), "set device");
+    if (rc) return rc;
+    const size_t need = (size_t)c->N * (c->c64 ? 8 : 16);
+    if (need > kScratchBytes)
+        return set_error(c, HELM3D_ERR_ARG,
+                         "apply_prec_noalloc: nx*ny*nz*" + std::to_string(c->c64 ? 8 : 16) + " = " +
+                             std::to_string(need) + " bytes of planes exceed the 8 MiB static scratch");
+    if (!is_device_ptr(x) || !is_device_ptr(y))
+        return set_error(c, HELM3D_ERR_ARG, "apply_prec_noalloc takes device pointers only");
+    void *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (!g_scratch_addr[c->device]) {
+            void *p = nullptr;
+            rc = cuda_check(c, cudaGetSymbolAddress(&p, g_plane_scratch), "cudaGetSymbolAddress(scratch)");
+            if (rc) return rc;
+            g_scratch_addr[c->device] = p;
+        }
+        scratch = g_scratch_addr[c->device];
+    }
+    rc = launch_fft_forward(c->c64, (const double2 *)x, 1.0, scratch, c->grid.nz, c->plane, c->plan, c->d_tw,
+                            c->stream);
+    if (rc) return set_error(c, rc, "apply_prec_noalloc: forward FFT launch");
+    SweepArgs s;
+    s.n = c->grid.nx;
+    s.ny = c->grid.ny;
+    s.nz = c->grid.nz;
+    s.ldg = c->ldg;
+    s.Gt = c->d_Gt;
+    s.cmy = c->d_cmy;
+    s.cpy = c->d_cpy;
+    s.planes = scratch;
+    s.nrhs = 1;
+    s.rhs_stride = 0;
+    s.status = c->d_status;
+    rc = launch_sweep(c->c64, s, c->stream);
+    if (rc) return set_error(c, rc, "apply_prec_noalloc: sweep launch");
+    rc = launch_fft_inverse(c->c64, scratch, (double2 *)y, c->grid.nz, c->plane, c->plan, c->d_tw, 0, nullptr, 0.0,
+                            nullptr, c->stream);
+    if (rc) return set_error(c, rc, "apply_prec_noalloc: inverse FFT launch");
+    c->launches += 3;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "apply_prec_noalloc");
+}
