@@ -100,9 +100,10 @@ struct Reduce {
     int nblocks;
     int cap;
 };
-// out[i] = sum_l conj(vs[i] V_i[l]) w[l]   (i < nv)
+// out[i] = sum_l conj(vs[i] V_i[l]) w[l]   (i < nv); with wnorm also
+// out[nv].x = ||w||^2 from the same pass
 int launch_dots(const double2 *V, long ldv, const double *vs, int nv, const double2 *w, long N,
-                const Reduce &red, double2 *out, cudaStream_t s);
+                const Reduce &red, double2 *out, cudaStream_t s, bool wnorm = false);
 // w -= sum_i coef[i] vs[i] V_i; then if redot: out[i] = <vs_i V_i, w_new>;
 // if norm: out[0].x = ||w_new||^2.  (out may be null)
 int launch_update(const double2 *V, long ldv, const double *vs, int nv, const double2 *coef, double2 *w,
@@ -146,6 +147,7 @@ struct helm3d_ctx {
     std::string last_error;
     long long launches = 0;
     double ms_factor = 0;      // wall time of set-up + factor in helm3d_create
+    long long reorth = 0;      // Gram-Schmidt second passes taken
     cudaStream_t own_stream = nullptr;
 
     // optional per-kernel-family profiler (helm3d_profile)

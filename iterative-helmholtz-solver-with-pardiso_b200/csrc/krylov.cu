@@ -44,41 +44,58 @@ template <int CH> __device__ __forceinline__ void block_sum(double2 (&acc)[CH], 
 }
 
 // partials[b][i] = sum over this block's l of conj(V_i[l]) w[l] * vs[i]
+// (i < nv); with wnorm, partials[b][nv].x = sum |w[l]|^2 as well
 __global__ void __launch_bounds__(kRedThreads) dots_kernel(const double2 *__restrict__ V, long ldv,
                                                            const double *__restrict__ vs, int nv,
-                                                           const double2 *__restrict__ w, long N,
+                                                           const double2 *__restrict__ w, long N, int wnorm,
                                                            double2 *__restrict__ partials, int cap) {
-    __shared__ double2 sh[(kRedThreads / 32) * kDotChunk];
+    __shared__ double2 sh[(kRedThreads / 32) * (kDotChunk + 1)];
     const long stride = (long)gridDim.x * blockDim.x;
-    for (int c0 = 0; c0 < nv; c0 += kDotChunk) {
-        double2 acc[kDotChunk];
+    for (int c0 = 0; c0 < nv || (c0 == 0 && wnorm); c0 += kDotChunk) {
+        double2 acc[kDotChunk + 1];
 #pragma unroll
-        for (int q = 0; q < kDotChunk; q++) acc[q] = make_double2(0, 0);
+        for (int q = 0; q <= kDotChunk; q++) acc[q] = make_double2(0, 0);
+        const bool with_norm = wnorm && c0 == 0;
         for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
             const double2 wl = w[l];
 #pragma unroll
             for (int q = 0; q < kDotChunk; q++)
                 if (c0 + q < nv) acc[q] = cfma(make_double2(V[(c0 + q) * ldv + l].x, -V[(c0 + q) * ldv + l].y), wl, acc[q]);
+            if (with_norm) acc[kDotChunk].x += wl.x * wl.x + wl.y * wl.y;
         }
-        block_sum<kDotChunk>(acc, sh);
-        if (threadIdx.x == 0)
+        block_sum<kDotChunk + 1>(acc, sh);
+        if (threadIdx.x == 0) {
             for (int q = 0; q < kDotChunk && c0 + q < nv; q++)
                 partials[(long)blockIdx.x * cap + c0 + q] = cscale(acc[q], vs ? vs[c0 + q] : 1.0);
+            if (with_norm) partials[(long)blockIdx.x * cap + nv] = acc[kDotChunk];
+        }
     }
 }
 
-// out[i] = sum_b partials[b][i]  (one thread per i, fixed order)
-__global__ void reduce_partials_kernel(const double2 *__restrict__ partials, int nblocks, int cap, int nv,
-                                       double2 *__restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// out[i] = sum_b partials[b][i]: one block of kFinalThreads per output i,
+// threads stride over the block partials, then a fixed shuffle tree
+// (deterministic: the order depends only on nblocks)
+constexpr int kFinalThreads = 128;
+__global__ void __launch_bounds__(kFinalThreads) reduce_partials_kernel(const double2 *__restrict__ partials,
+                                                                        int nblocks, int cap, int nv,
+                                                                        double2 *__restrict__ out) {
+    __shared__ double2 sh[kFinalThreads / 32];
+    const int i = blockIdx.x;
     if (i >= nv) return;
     double2 s = make_double2(0, 0);
-    for (int b = 0; b < nblocks; b++) {
+    for (int b = threadIdx.x; b < nblocks; b += kFinalThreads) {
         const double2 p = partials[(long)b * cap + i];
         s.x += p.x;
         s.y += p.y;
     }
-    out[i] = s;
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 t = sh[0];
+        for (int w = 1; w < kFinalThreads / 32; w++) t = cadd(t, sh[w]);
+        out[i] = t;
+    }
 }
 
 // w -= sum_i coef[i] vs[i] V_i ; post: 0 none, 1 ||w_new||^2 partial into partials[b][0]
@@ -200,11 +217,12 @@ static int grid_for(long N) {
 }
 
 int launch_dots(const double2 *V, long ldv, const double *vs, int nv, const double2 *w, long N, const Reduce &red,
-                double2 *out, cudaStream_t s) {
-    if (nv > red.cap) return HELM3D_ERR_ARG;
+                double2 *out, cudaStream_t s, bool wnorm) {
+    if (nv + (wnorm ? 1 : 0) > red.cap) return HELM3D_ERR_ARG;
     const int nb = red.nblocks;
-    dots_kernel<<<nb, kRedThreads, 0, s>>>(V, ldv, vs, nv, w, N, red.partials, red.cap);
-    reduce_partials_kernel<<<(nv + 127) / 128, 128, 0, s>>>(red.partials, nb, red.cap, nv, out);
+    dots_kernel<<<nb, kRedThreads, 0, s>>>(V, ldv, vs, nv, w, N, wnorm ? 1 : 0, red.partials, red.cap);
+    reduce_partials_kernel<<<nv + (wnorm ? 1 : 0), kFinalThreads, 0, s>>>(red.partials, nb, red.cap,
+                                                                         nv + (wnorm ? 1 : 0), out);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
@@ -213,7 +231,7 @@ int launch_update(const double2 *V, long ldv, const double *vs, int nv, const do
     const int nb = post ? red.nblocks : grid_for(N);
     update_kernel<<<nb, kRedThreads, sizeof(double2) * (nv > 0 ? nv : 1), s>>>(V, ldv, vs, nv, coef, w, N, post,
                                                                                red.partials, red.cap);
-    if (post == 1) reduce_partials_kernel<<<1, 32, 0, s>>>(red.partials, nb, red.cap, 1, out);
+    if (post == 1) reduce_partials_kernel<<<1, kFinalThreads, 0, s>>>(red.partials, nb, red.cap, 1, out);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
@@ -228,7 +246,7 @@ int launch_norm2_box(const double2 *x, int nx, int ny, int nz, const int box[6],
     (void)nz;
     norm2_box_kernel<<<red.nblocks, kRedThreads, 0, s>>>(x, nx, ny, box[0], box[1], box[2], box[3], box[4], box[5],
                                                          red.partials, red.cap);
-    reduce_partials_kernel<<<1, 32, 0, s>>>(red.partials, red.nblocks, red.cap, 1, out);
+    reduce_partials_kernel<<<1, kFinalThreads, 0, s>>>(red.partials, red.nblocks, red.cap, 1, out);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 

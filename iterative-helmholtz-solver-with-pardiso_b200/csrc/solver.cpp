@@ -270,24 +270,34 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, bool adjoint, helm3d_sta
             } else {
                 RC(apply_op(c, V + (size_t)j * N, vs_h[j], w));
             }
-            // CGS2: h1 = V^H w, w -= V h1, h2 = V^H w, w -= V h2, ||w||^2
+            // Classical Gram-Schmidt, repeated only when needed ("twice is
+            // enough"): h1 = V^H w with ||w||^2 from the same pass, w -= V h1
+            // with ||w||^2 after; a second pass runs when the norm dropped
+            // below 1/sqrt(2) of its value.
             const Reduce red = reducer(c);
             RC(timed(c, HELM3D_K_KRYLOV, 2,
-                     [&] { return launch_dots(V, N, c->d_vs, j + 1, w, N, red, d_h1, c->stream); }));
-            RC(timed(c, HELM3D_K_KRYLOV, 1, [&] {
-                return launch_update(V, N, c->d_vs, j + 1, d_h1, w, N, 0, red, nullptr, c->stream);
-            }));
-            RC(timed(c, HELM3D_K_KRYLOV, 2,
-                     [&] { return launch_dots(V, N, c->d_vs, j + 1, w, N, red, d_h2, c->stream); }));
+                     [&] { return launch_dots(V, N, c->d_vs, j + 1, w, N, red, d_h1, c->stream, true); }));
             RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
-                return launch_update(V, N, c->d_vs, j + 1, d_h2, w, N, 1, red, d_nrm, c->stream);
+                return launch_update(V, N, c->d_vs, j + 1, d_h1, w, N, 1, red, d_nrm, c->stream);
             }));
             RC(cuda_check(c, cudaMemcpyAsync(hb.h, d_h1, sizeof(double2) * 3 * (m + 2), cudaMemcpyDeviceToHost,
                                              c->stream),
                           "h"));
             RC(cuda_check(c, cudaStreamSynchronize(c->stream), "h sync"));
-            for (int i = 0; i <= j; i++)
-                H[(size_t)i * m + j] = zc(hb.h[i].x + hb.h[(m + 2) + i].x, hb.h[i].y + hb.h[(m + 2) + i].y);
+            for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = zc(hb.h[i].x, hb.h[i].y);
+            if (hb.h[2 * (m + 2)].x < 0.5 * hb.h[j + 1].x) {
+                RC(timed(c, HELM3D_K_KRYLOV, 2,
+                         [&] { return launch_dots(V, N, c->d_vs, j + 1, w, N, red, d_h2, c->stream); }));
+                RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+                    return launch_update(V, N, c->d_vs, j + 1, d_h2, w, N, 1, red, d_nrm, c->stream);
+                }));
+                RC(cuda_check(c, cudaMemcpyAsync(hb.h + (m + 2), d_h2, sizeof(double2) * 2 * (m + 2),
+                                                 cudaMemcpyDeviceToHost, c->stream),
+                              "h2"));
+                RC(cuda_check(c, cudaStreamSynchronize(c->stream), "h2 sync"));
+                for (int i = 0; i <= j; i++) H[(size_t)i * m + j] += zc(hb.h[(m + 2) + i].x, hb.h[(m + 2) + i].y);
+                c->reorth++;
+            }
             const double hn = std::sqrt(std::max(0.0, hb.h[2 * (m + 2)].x));
             if (!std::isfinite(hn)) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
             H[(size_t)(j + 1) * m + j] = hn;

@@ -7,13 +7,18 @@
 //   backward  x_{ny-1} = y_{ny-1},   x_j = y_j - cpy[j] G_j x_{j+1}
 // in place on the plane of each kz.  One CTA per (kz, right-hand side).
 //
-// The block product y = G v reads G^T row by row (G^T[m][:] = column m of
-// G, contiguous): warp w accumulates v[m] * G^T[m][:] for m = w, w + NW, ...
-// with lane l owning rows l, l + 32, ...; the NW partial vectors are summed
-// through shared memory.  G^T streams from HBM through a ring of shared
-// memory stages filled by 1D bulk copies (cp.async.bulk) issued by one
-// thread; the copies run ahead of the dependence chain y_{j-1} -> y_j, so
-// the stream is limited by bandwidth rather than by the per-line latency.
+// G_j^T (row m = column m of G, contiguous) streams from HBM through a ring
+// of shared-memory stages filled by 1D bulk copies (cp.async.bulk with
+// mbarrier completion) that a dedicated producer warp issues as far ahead as
+// the ring allows, independently of the y_{j-1} -> y_j dependence chain.
+// Each of the 8 consumer warps owns RW = 32/G rows of y: lane (il, g) owns
+// row i = w*RW + il and accumulates G^T[m][i] v[m] over the rows m = g, g+G,
+// ... of every stage; the G partial sums of a row meet by warp shuffles, so a
+// y-line ends with one named barrier among the consumer warps and no
+// shared-memory reduction.  v[m] is formed on the fly from the previous
+// line's result and the current line's right-hand side, both double-buffered
+// in shared memory; the next line's right-hand side is prefetched into
+// registers while the current line streams.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -37,88 +42,93 @@ template <typename R> struct SweepK {
 };
 
 constexpr uint32_t kSweepWaitLimit = 1u << 20;
+constexpr int kSweepConsumerWarps = 8;
+constexpr int kSweepMaxN = 256;
 
-// stage s of the global sequence: fwd lines 0..ny-1 then bwd lines ny-2..0,
-// each line split in chunks of rows_per_stage rows of G^T
+__device__ __forceinline__ void consumer_barrier() {
+    asm volatile("bar.sync 1, %0;" ::"n"(kSweepConsumerWarps * 32) : "memory");
+}
+
+// G^T source of stage `seq`: forward lines 0..ny-1, then backward lines
+// ny-2..0, each line split in chunks of rows_per_stage rows
 template <typename R>
-__device__ __forceinline__ const cplx<R> *stage_src(const SweepK<R> &a, int kz, long seq, int chunks_per_line,
-                                                    int *rows) {
-    const long line_seq = seq / chunks_per_line;
-    const int chunk = (int)(seq % chunks_per_line);
+__device__ __forceinline__ const cplx<R> *stage_src(const SweepK<R> &a, int kz, long seq, int cpl, int *rows) {
+    const long line_seq = seq / cpl;
+    const int chunk = (int)(seq % cpl);
     const int line = line_seq < a.ny ? (int)line_seq : (int)(2 * a.ny - 2 - line_seq);
     const int r0 = chunk * a.rows_per_stage;
     *rows = min(a.rows_per_stage, a.n - r0);
     return a.Gt + (((long)kz * a.ny + line) * a.n + r0) * (long)a.ldg;
 }
 
-template <typename R, int NW, int RB>
-__global__ void __launch_bounds__(NW * 32, 1) sweep_kernel(SweepK<R> a) {
+template <typename R, int G>
+__global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kernel(SweepK<R> a) {
     typedef cplx<R> Cx;
+    constexpr int RW = 32 / G;  // rows of y per warp
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int n = a.n, ny = a.ny, ldg = a.ldg;
     const int kz = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    Cx *ring = reinterpret_cast<Cx *>(smem_raw);                                    // nstage * stage
-    Cx *vec = reinterpret_cast<Cx *>(smem_raw + (size_t)a.nstage * a.stage_bytes);  // [32*RB] current v
-    Cx *prev = vec + 32 * RB;                                                        // [32*RB] y_{j-1} / x_{j+1}
-    Cx *red = prev + 32 * RB;                                                        // [NW][32*RB]
-    uint64_t *full = reinterpret_cast<uint64_t *>(red + NW * 32 * RB);
+    Cx *ring = reinterpret_cast<Cx *>(smem_raw);
+    Cx *ybuf = reinterpret_cast<Cx *>(smem_raw + (size_t)a.nstage * a.stage_bytes);  // [2][kSweepMaxN]
+    Cx *fbuf = ybuf + 2 * kSweepMaxN;                                                 // [2][kSweepMaxN]
+    uint64_t *full = reinterpret_cast<uint64_t *>(fbuf + 2 * kSweepMaxN);
     uint64_t *empty = full + a.nstage;
     Cx *P = a.planes + (long)blockIdx.y * a.rhs_stride + (long)kz * ny * n;
-
-    const int cpl = (n + a.rows_per_stage - 1) / a.rows_per_stage;  // chunks per line
+    const int cpl = (n + a.rows_per_stage - 1) / a.rows_per_stage;
     const long nseq = (long)(2 * ny - 1) * cpl;
-    bool dead = false;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < a.nstage; s++) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], NW);
+            mbar_init(&empty[s], kSweepConsumerWarps);
         }
         fence_mbar_init_cluster();
     }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) fbuf[i] = P[i];  // f_0
     __syncthreads();
 
-    // producer: thread 0 keeps up to nstage copies in flight
-    long issued = 0;
-    auto produce = [&](long upto) {
-        while (issued < upto && issued < nseq) {
-            const int s = (int)(issued % a.nstage);
-            const uint32_t ph = (uint32_t)((issued / a.nstage) & 1);
-            if (!dead && !mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, kSweepWaitLimit)) {
-                dead = true;
-                atomicOr(a.status, 4);
+    if (warp == kSweepConsumerWarps) {
+        // producer warp: one lane streams every stage of the chain
+        if (lane == 0) {
+            bool dead = false;
+            for (long seq = 0; seq < nseq; seq++) {
+                const int s = (int)(seq % a.nstage);
+                const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
+                if (!dead && !mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, kSweepWaitLimit)) {
+                    dead = true;
+                    atomicOr(a.status, 4);
+                }
+                int rows;
+                const Cx *src = stage_src(a, kz, seq, cpl, &rows);
+                const uint32_t bytes = (uint32_t)rows * ldg * (uint32_t)sizeof(Cx);
+                mbar_expect_tx(&full[s], bytes);
+                bulk_g2s(ring + (size_t)s * (a.stage_bytes / sizeof(Cx)), src, bytes, &full[s]);
             }
-            int rows;
-            const Cx *src = stage_src(a, kz, issued, cpl, &rows);
-            const uint32_t bytes = (uint32_t)rows * ldg * sizeof(Cx);
-            mbar_expect_tx(&full[s], bytes);
-            bulk_g2s(ring + (size_t)s * (a.stage_bytes / sizeof(Cx)), src, bytes, &full[s]);
-            issued++;
         }
-    };
-    if (threadIdx.x == 0) produce(a.nstage);
+        return;
+    }
 
+    const int il = lane % RW, g = lane / RW;
+    const int i = warp * RW + il;
+    const bool own = i < n;
+    bool dead = false;
     long seq = 0;
     for (int step = 0; step < 2 * ny - 1; step++) {
         const bool fwd = step < ny;
         const int line = fwd ? step : 2 * ny - 2 - step;
-        // v for this line
-        for (int i = threadIdx.x; i < n; i += NW * 32) {
-            Cx v;
-            if (fwd) {
-                v = P[(long)line * n + i];
-                if (line > 0) v = cfms(a.cmy[line], prev[i], v);
-            } else {
-                v = prev[i];  // x_{line+1}
-            }
-            vec[i] = v;
+        const Cx *yprev = ybuf + ((step + 1) & 1) * kSweepMaxN;  // y_{line-1} (fwd) / x_{line+1} (bwd)
+        Cx *ycur = ybuf + (step & 1) * kSweepMaxN;
+        const Cx *fcur = fbuf + (step & 1) * kSweepMaxN;
+        const Cx c = fwd ? (line > 0 ? a.cmy[line] : mkc<R>(0, 0)) : mkc<R>(0, 0);
+        // prefetch: next line's right-hand side (forward) or this line's y (backward)
+        Cx pre = mkc<R>(0, 0);
+        if (own && g == 0) {
+            if (fwd && line + 1 < ny) pre = P[(long)(line + 1) * n + i];
+            else if (!fwd) pre = P[(long)line * n + i];
         }
-        __syncthreads();
-        Cx acc[RB];
-#pragma unroll
-        for (int ra = 0; ra < RB; ra++) acc[ra] = mkc<R>(0, 0);
-        for (int c = 0; c < cpl; c++, seq++) {
+        Cx acc = mkc<R>(0, 0);
+        for (int ch = 0; ch < cpl; ch++, seq++) {
             const int s = (int)(seq % a.nstage);
             const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
             if (!dead && !mbar_wait_bounded_cta(smem_u32(&full[s]), ph, kSweepWaitLimit)) {
@@ -126,41 +136,42 @@ __global__ void __launch_bounds__(NW * 32, 1) sweep_kernel(SweepK<R> a) {
                 atomicOr(a.status, 4);
             }
             const Cx *st = ring + (size_t)s * (a.stage_bytes / sizeof(Cx));
-            const int r0 = c * a.rows_per_stage;
+            const int r0 = ch * a.rows_per_stage;
             const int rows = min(a.rows_per_stage, n - r0);
-            for (int m = warp; m < rows; m += NW) {
-                const Cx vm = vec[r0 + m];
-                const Cx *g = st + (long)m * ldg;
-#pragma unroll
-                for (int ra = 0; ra < RB; ra++) {
-                    const int i = lane + 32 * ra;
-                    if (i < n) acc[ra] = cfma(g[i], vm, acc[ra]);
+            if (own) {
+#pragma unroll 4
+                for (int ml = g; ml < rows; ml += G) {
+                    const int m = r0 + ml;
+                    Cx v;
+                    if (fwd) v = (line > 0) ? cfms(c, yprev[m], fcur[m]) : fcur[m];
+                    else v = yprev[m];
+                    acc = cfma(st[(long)ml * ldg + i], v, acc);
                 }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive_local(&empty[s]);
-            if (threadIdx.x == 0) produce(seq + 1 + a.nstage);
         }
 #pragma unroll
-        for (int ra = 0; ra < RB; ra++) red[warp * 32 * RB + lane + 32 * ra] = acc[ra];
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += NW * 32) {
-            Cx y = red[i];
-            for (int w = 1; w < NW; w++) y = cadd(y, red[w * 32 * RB + i]);
-            if (fwd) {
-                prev[i] = y;
-                P[(long)line * n + i] = y;
-            } else {
-                const Cx x = cfms(a.cpy[line], y, P[(long)line * n + i]);
-                prev[i] = x;
-                P[(long)line * n + i] = x;
-            }
+        for (int off = RW; off < 32; off <<= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
         }
-        __syncthreads();
+        if (own && g == 0) {
+            Cx out;
+            if (fwd) {
+                out = acc;
+                if (line + 1 < ny) fbuf[((step + 1) & 1) * kSweepMaxN + i] = pre;
+            } else {
+                out = cfms(a.cpy[line], acc, pre);
+            }
+            ycur[i] = out;
+            P[(long)line * n + i] = out;
+        }
+        consumer_barrier();
     }
 }
 
-template <typename R, int NW, int RB> static int sweep_impl(const SweepArgs &sa, cudaStream_t st) {
+template <typename R, int G> static int sweep_impl(const SweepArgs &sa, cudaStream_t st) {
     typedef cplx<R> Cx;
     SweepK<R> k;
     k.n = sa.n;
@@ -172,47 +183,36 @@ template <typename R, int NW, int RB> static int sweep_impl(const SweepArgs &sa,
     k.planes = (Cx *)sa.planes;
     k.rhs_stride = sa.rhs_stride;
     k.status = sa.status;
-    // ring: ~24 KB stages, as many as fit in ~160 KB
+    // ~16 KB stages, as many as fit in ~200 KB
     const size_t row_bytes = (size_t)sa.ldg * sizeof(Cx);
-    int rows = (int)((24 * 1024) / row_bytes);
+    int rows = (int)((16 * 1024) / row_bytes);
     if (rows < 1) rows = 1;
     if (rows > sa.n) rows = sa.n;
     k.rows_per_stage = rows;
     k.stage_bytes = (uint32_t)(((size_t)rows * row_bytes + 127) & ~(size_t)127);
-    int nst = (int)((160 * 1024) / k.stage_bytes);
-    if (nst > 8) nst = 8;
+    int nst = (int)((200 * 1024) / k.stage_bytes);
+    if (nst > 32) nst = 32;
     if (nst < 2) nst = 2;
     k.nstage = nst;
-    const size_t smem = (size_t)nst * k.stage_bytes + sizeof(Cx) * (2 + NW) * 32 * RB + 2 * nst * sizeof(uint64_t) + 16;
-    auto kern = sweep_kernel<R, NW, RB>;
+    const size_t smem = (size_t)nst * k.stage_bytes + sizeof(Cx) * 4 * kSweepMaxN + 2 * nst * sizeof(uint64_t);
+    auto kern = sweep_kernel<R, G>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return HELM3D_ERR_CUDA;
-    kern<<<dim3((unsigned)sa.nz, (unsigned)sa.nrhs), NW * 32, smem, st>>>(k);
+    kern<<<dim3((unsigned)sa.nz, (unsigned)sa.nrhs), (kSweepConsumerWarps + 1) * 32, smem, st>>>(k);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
 int launch_sweep(bool c64, const SweepArgs &sa, cudaStream_t s) {
-    const int rb = (sa.n + 31) / 32;
+    if (sa.n < 1 || sa.n > kSweepMaxN) return HELM3D_ERR_ARG;
+    const int g = sa.n <= 64 ? 4 : (sa.n <= 128 ? 2 : 1);
     if (c64) {
-        switch (rb) {
-            case 1: return sweep_impl<float, 8, 1>(sa, s);
-            case 2: return sweep_impl<float, 8, 2>(sa, s);
-            case 3: return sweep_impl<float, 8, 3>(sa, s);
-            case 4: return sweep_impl<float, 8, 4>(sa, s);
-            case 5: case 6: return sweep_impl<float, 8, 6>(sa, s);
-            case 7: case 8: return sweep_impl<float, 8, 8>(sa, s);
-        }
-    } else {
-        switch (rb) {
-            case 1: return sweep_impl<double, 8, 1>(sa, s);
-            case 2: return sweep_impl<double, 8, 2>(sa, s);
-            case 3: return sweep_impl<double, 8, 3>(sa, s);
-            case 4: return sweep_impl<double, 8, 4>(sa, s);
-            case 5: case 6: return sweep_impl<double, 8, 6>(sa, s);
-            case 7: case 8: return sweep_impl<double, 8, 8>(sa, s);
-        }
+        if (g == 4) return sweep_impl<float, 4>(sa, s);
+        if (g == 2) return sweep_impl<float, 2>(sa, s);
+        return sweep_impl<float, 1>(sa, s);
     }
-    return HELM3D_ERR_ARG;
+    if (g == 4) return sweep_impl<double, 4>(sa, s);
+    if (g == 2) return sweep_impl<double, 2>(sa, s);
+    return sweep_impl<double, 1>(sa, s);
 }
 
 }  // namespace h3d
