@@ -141,9 +141,9 @@ def run_ours(args, rank, world, dist):
     s2_dev = torch.from_numpy(s2_host).to(dev)
     u_dev = torch.empty_like(f_dev)
 
-    def make(prec):
+    def make(prec, zt=0):
         o = helm3d.default_opts(precision=prec, restart=RESTART, tol=TOL, beta_prec=BETA_PREC, max_iter=20000,
-                                device=dev.index)
+                                device=dev.index, z_transform=zt)
         s = helm3d.Solver(grid, s2_dev, o)
         s.set_stream(stream)
         return s
@@ -223,6 +223,22 @@ def run_ours(args, rank, world, dist):
     relres64 = s64.last_stats.relres
     s64.close()
 
+    # the same solve with the PML-eigenbasis z-transform (c64 and c128)
+    zeig = {}
+    for prec, key in ((helm3d.PREC_C64, "c64"), (helm3d.PREC_C128, "c128")):
+        sz = make(prec, helm3d.ZT_PML_EIGEN)
+        msz, itsz, _, _ = timed_solves(sz, args.steps, 1)
+        sz.profile(True)
+        sz.set_medium(s2_dev)
+        sz.solve(f_dev, u=u_dev, allow_not_converged=True)
+        pz = sz.profile_read()
+        uz = u_dev.clone()
+        zeig[key] = {"value": msz / 1e3 / world, "unit": "s", "iterations": itsz[-1] if itsz else None,
+                     "relres": sz.last_stats.relres,
+                     "relerr_vs_fft_fp64_path": float(torch.linalg.vector_norm(uz - u64) / torch.linalg.vector_norm(u64)),
+                     "kernel_ms_per_solve": {k: round(v[0], 3) for k, v in pz.items()}}
+        sz.close()
+
     if rank != 0:
         return None
 
@@ -261,6 +277,7 @@ def run_ours(args, rank, world, dist):
         "fp64_plain": {"value": ms64 / 1e3 / world, "unit": "s", "iterations": its64[-1] if its64 else None,
                        "relres": relres64},
         "speedup_vs_fp64_plain": (ms64 / ms32) if ms32 > 0 else None,
+        "zpml_eigen": zeig,
         "e2e": {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": N * 8 + N * 16,
                 "d2h_bytes_per_step": N * 16},
         "gpu_launches": int(launches32 / max(1, args.steps)) * args.steps,

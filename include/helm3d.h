@@ -57,6 +57,17 @@ typedef enum helm3d_kz_symbol {
     HELM3D_KZ_REFERENCE = 2
 } helm3d_kz_symbol;
 
+/* How the preconditioner separates z (mode N):
+ *   HELM3D_ZT_FFT        the reference's FFT along z with the periodic kz^2
+ *                        symbol (Source/functions.cpp:5858-5881);
+ *   HELM3D_ZT_PML_EIGEN  the eigenvectors of the 1D z operator with its PML
+ *                        (D_z = W diag(lambda) W^{-1}), applied as dense
+ *                        z-transforms; the per-mode shift is lambda_k.  The
+ *                        split into one shifted 2D system per z-mode and the
+ *                        block LU are unchanged; M equals A when the medium
+ *                        is z-invariant and beta_prec = 0. */
+typedef enum helm3d_z_transform { HELM3D_ZT_FFT = 0, HELM3D_ZT_PML_EIGEN = 1 } helm3d_z_transform;
+
 /* Grid: mirrors size_m (Source/definitions.h:55-68) for three axes. */
 typedef struct helm3d_grid {
     int nx, ny, nz;          /* points per axis, PML/sponge included */
@@ -81,6 +92,7 @@ typedef struct helm3d_opts {
     int stop_phys;       /* 1: test the physical-domain residual instead */
     int device;          /* CUDA device ordinal */
     int verbose;
+    int z_transform;     /* helm3d_z_transform (mode N; mode R always uses the FFT) */
 } helm3d_opts;
 
 typedef struct helm3d_stats {

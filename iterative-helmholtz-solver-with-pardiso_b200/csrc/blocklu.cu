@@ -51,7 +51,7 @@ template <typename R> struct FactorK {
     int n, ny, nz, ldg;
     cplx<R> *Gt;
     const cplx<R> *cmx, *cpx, *cmy, *cpy, *base2d;
-    const R *kz2;
+    const cplx<R> *kz2;  // complex shift of mode kz
     int *status;
 };
 
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(NW * 32, 1) factor_kernel(FactorK<R> a) {
     if (C > 1) cluster_sync_all();
     else __syncthreads();
 
-    const R kzv = a.kz2[kz];
+    const Cx kzv = a.kz2[kz];
     Cx S[RB][CB];
     long t = 0;  // global pivot step counter (line * n + k)
 
@@ -167,8 +167,8 @@ __global__ void __launch_bounds__(NW * 32, 1) factor_kernel(FactorK<R> a) {
                             v = mkc<R>(-(cc.x * gij.x - cc.y * gij.y), -(cc.x * gij.y + cc.y * gij.x));
                         }
                         if (i == j) {
-                            Cx d = cadd(cyd, a.base2d[(long)line * n + i]);
-                            d.x -= kzv + a.cmx[i].x + a.cpx[i].x;
+                            Cx d = cadd(cadd(cyd, a.base2d[(long)line * n + i]), kzv);
+                            d.x -= a.cmx[i].x + a.cpx[i].x;
                             d.y -= a.cmx[i].y + a.cpx[i].y;
                             v = cadd(v, d);
                         } else if (j == i + 1) {
@@ -355,7 +355,7 @@ static int launch_cfg(const FactorArgs &fa, cudaStream_t st) {
     k.cmy = (const cplx<R> *)fa.cmy;
     k.cpy = (const cplx<R> *)fa.cpy;
     k.base2d = (const cplx<R> *)fa.base2d;
-    k.kz2 = (const R *)fa.kz2;
+    k.kz2 = (const cplx<R> *)fa.kz2;
     k.status = fa.status;
     constexpr size_t smem = factor_smem_bytes<R, NP, NP / C>();
     auto kern = factor_kernel<R, NP, NW, CB, C>;

@@ -54,6 +54,7 @@ int validate(const helm3d_grid *g, const helm3d_opts *o) {
     if (o->mode != HELM3D_MODE_R && o->mode != HELM3D_MODE_N) return HELM3D_ERR_ARG;
     if (o->precision != HELM3D_PREC_C64 && o->precision != HELM3D_PREC_C128) return HELM3D_ERR_ARG;
     if (o->kz_symbol < 0 || o->kz_symbol > 2) return HELM3D_ERR_ARG;
+    if (o->z_transform != HELM3D_ZT_FFT && o->z_transform != HELM3D_ZT_PML_EIGEN) return HELM3D_ERR_ARG;
     if (o->restart < 1 || o->restart > 1000 || o->max_iter < 0 || !(o->tol >= 0)) return HELM3D_ERR_ARG;
     if (g->nz > 4096) return HELM3D_ERR_ARG;
     return HELM3D_OK;
@@ -309,7 +310,7 @@ int helm3d_destroy(helm3d_ctx *c) {
     if (!c) return HELM3D_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void *bufs[] = {c->d_Gt, c->d_tw, c->d_cmx, c->d_cpx, c->d_cmy, c->d_cpy, c->d_base2d, c->d_kz2,
+    void *bufs[] = {c->d_Gt, c->d_tw, c->d_cmx, c->d_cpx, c->d_cmy, c->d_cpy, c->d_base2d, c->d_kz2, c->d_zW, c->d_zWi, c->d_zW64, c->d_zWi64,
                     c->d_cmx64, c->d_cpx64, c->d_cmy64, c->d_cpy64, c->d_cmz64, c->d_cpz64, c->d_s2, c->d_dl,
                     c->d_planes, c->d_status, c->d_V, c->d_Z, c->d_vs, c->d_h, c->d_partials, c->d_f, c->d_u,
                     c->d_r, c->d_t, c->d_t2, c->d_bic};

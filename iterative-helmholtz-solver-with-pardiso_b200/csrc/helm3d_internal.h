@@ -51,6 +51,13 @@ int launch_fft_inverse(bool c64, const void *planes, double2 *y, int nz, long pl
                        const void *tw, int mode, const double2 *w, double scale, const double2 *dl,
                        cudaStream_t s);
 
+// Dense z-transforms with the eigenvectors of the z operator (FP64 matrices
+// W, Wi row-major nz x nz): planes = Wi (scale x); y = W planes.
+int launch_ztrans_forward(bool c64, const double2 *x, double scale, void *planes, int nz, long plane,
+                          const double2 *Wi, cudaStream_t s);
+int launch_ztrans_inverse(bool c64, const void *planes, double2 *y, int nz, long plane, const double2 *W,
+                          cudaStream_t s);
+
 // Block-tridiagonal factor of all nz systems: G^T of every (kz, y-line).
 struct FactorArgs {
     int n, ny, nz, ldg;
@@ -58,7 +65,7 @@ struct FactorArgs {
     const void *cmx, *cpx;    // cplx<P>[n]
     const void *cmy, *cpy;    // cplx<P>[ny]
     const void *base2d;       // cplx<P>[ny][n]: omega^2 s0^2 (1 + i beta)
-    const void *kz2;          // P[nz]
+    const void *kz2;          // cplx<P>[nz]: complex shift of mode k (-kz^2 or lambda_k)
     int *status;              // device flag: bit 0 = zero pivot
 };
 int launch_factor(bool c64, const FactorArgs &a, cudaStream_t s);
@@ -164,6 +171,9 @@ struct helm3d_ctx {
     std::vector<h3d::zc> cmx, cpx, cmy, cpy, cmz, cpz;
     std::vector<double> kz2;
     std::vector<h3d::zc> base2d;   // [ny][nx]
+    bool zeig = false;             // PML eigenbasis z-transform instead of the FFT
+    std::vector<h3d::zc> zshift;   // per-mode diagonal shift: -kz^2 or lambda_k
+    std::vector<h3d::zc> zW, zWi;  // z eigenvectors (row-major nz x nz) and inverse
     h3d::FftPlan plan;
 
     // device buffers
@@ -171,7 +181,9 @@ struct helm3d_ctx {
     size_t Gt_bytes = 0;
     void *d_tw = nullptr;          // FFT tables (precision P)
     void *d_cmx = nullptr, *d_cpx = nullptr, *d_cmy = nullptr, *d_cpy = nullptr;   // P precision
-    void *d_base2d = nullptr, *d_kz2 = nullptr;                                    // P precision
+    void *d_base2d = nullptr, *d_kz2 = nullptr;                                    // P precision (kz2: complex mode shifts)
+    void *d_zW = nullptr, *d_zWi = nullptr;                                        // P precision
+    double2 *d_zW64 = nullptr, *d_zWi64 = nullptr;
     double2 *d_cmx64 = nullptr, *d_cpx64 = nullptr, *d_cmy64 = nullptr, *d_cpy64 = nullptr;
     double2 *d_cmz64 = nullptr, *d_cpz64 = nullptr;
     double *d_s2 = nullptr;        // squared slowness (mode N operator)

@@ -65,8 +65,10 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
         }
         scratch = g_scratch_addr[c->device];
     }
-    rc = launch_fft_forward(c->c64, (const double2 *)x, 1.0, scratch, c->grid.nz, c->plane, c->plan, c->d_tw,
-                            c->stream);
+    rc = c->zeig ? launch_ztrans_forward(c->c64, (const double2 *)x, 1.0, scratch, c->grid.nz, c->plane, c->d_zWi64,
+                                         c->stream)
+                 : launch_fft_forward(c->c64, (const double2 *)x, 1.0, scratch, c->grid.nz, c->plane, c->plan, c->d_tw,
+                                      c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: forward FFT launch");
     SweepArgs s;
     s.n = c->grid.nx;
@@ -82,8 +84,9 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
     s.status = c->d_status;
     rc = launch_sweep(c->c64, s, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: sweep launch");
-    rc = launch_fft_inverse(c->c64, scratch, (double2 *)y, c->grid.nz, c->plane, c->plan, c->d_tw, 0, nullptr, 0.0,
-                            nullptr, c->stream);
+    rc = c->zeig ? launch_ztrans_inverse(c->c64, scratch, (double2 *)y, c->grid.nz, c->plane, c->d_zW64, c->stream)
+                 : launch_fft_inverse(c->c64, scratch, (double2 *)y, c->grid.nz, c->plane, c->plan, c->d_tw, 0,
+                                      nullptr, 0.0, nullptr, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: inverse FFT launch");
     c->launches += 3;
     return cuda_check(c, cudaStreamSynchronize(c->stream), "apply_prec_noalloc");

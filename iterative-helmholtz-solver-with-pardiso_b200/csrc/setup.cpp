@@ -44,6 +44,171 @@ static void pml_table(int n, int pml, double h, double omega, std::vector<zc> &c
     }
 }
 
+// ------------------------------------------------------------------------
+// Eigen-decomposition D = W diag(lam) W^{-1} of the z operator with its PML
+// (tridiagonal: sub cm[i+1], diagonal -(cm+cp)[i], super cp[i]).  D is
+// upper Hessenberg; its complex Schur form D = Z T Z^H is computed by the
+// single-shift QR algorithm with Wilkinson shifts, deflation and bulge
+// chasing by complex Givens rotations (Golub & Van Loan, Matrix
+// Computations, sec. 7.5); eigenvectors of T by back substitution, W = Z Y;
+// W^{-1} by Gaussian elimination with partial pivoting.
+static bool schur_hessenberg(int n, std::vector<zc> &H, std::vector<zc> &Z) {
+    auto h = [&](int i, int j) -> zc & { return H[(size_t)i * n + j]; };
+    auto z = [&](int i, int j) -> zc & { return Z[(size_t)i * n + j]; };
+    Z.assign((size_t)n * n, zc(0, 0));
+    for (int i = 0; i < n; i++) z(i, i) = 1.0;
+    double anorm = 0;
+    for (auto &v : H) anorm = std::max(anorm, std::abs(v));
+    const double eps = 2.220446049250313e-16;
+    int hi = n - 1, iter = 0, total = 0;
+    while (hi > 0) {
+        int lo = hi;
+        while (lo > 0) {
+            double sc = std::abs(h(lo - 1, lo - 1)) + std::abs(h(lo, lo));
+            if (sc == 0.0) sc = anorm;
+            if (std::abs(h(lo, lo - 1)) <= eps * sc) {
+                h(lo, lo - 1) = 0.0;
+                break;
+            }
+            lo--;
+        }
+        if (lo == hi) {
+            hi--;
+            iter = 0;
+            continue;
+        }
+        if (++total > 100 * n) return false;
+        iter++;
+        const zc a = h(hi - 1, hi - 1), b = h(hi - 1, hi), c = h(hi, hi - 1), d = h(hi, hi);
+        const zc half = (a - d) * 0.5;
+        const zc disc = std::sqrt(half * half + b * c);
+        const zc m1 = (a + d) * 0.5 + disc, m2 = (a + d) * 0.5 - disc;
+        zc mu = std::abs(m1 - d) < std::abs(m2 - d) ? m1 : m2;
+        if (iter % 11 == 10) mu = d + 0.75 * std::abs(h(hi, hi - 1));  // exceptional shift
+        zc x = h(lo, lo) - mu, y = h(lo + 1, lo);
+        for (int k = lo; k < hi; k++) {
+            const double ax = std::abs(x), nrm = std::hypot(ax, std::abs(y));
+            double cs;
+            zc sn;
+            if (nrm == 0.0) {
+                cs = 1.0;
+                sn = 0.0;
+            } else if (ax == 0.0) {
+                cs = 0.0;
+                sn = 1.0;
+            } else {
+                cs = ax / nrm;
+                sn = (x / ax) * std::conj(y) / nrm;
+            }
+            for (int j = std::max(lo, k - 1); j < n; j++) {
+                const zc t1 = h(k, j), t2 = h(k + 1, j);
+                h(k, j) = cs * t1 + sn * t2;
+                h(k + 1, j) = -std::conj(sn) * t1 + cs * t2;
+            }
+            for (int i = 0; i <= std::min(k + 2, hi); i++) {
+                const zc t1 = h(i, k), t2 = h(i, k + 1);
+                h(i, k) = cs * t1 + std::conj(sn) * t2;
+                h(i, k + 1) = -sn * t1 + cs * t2;
+            }
+            for (int i = 0; i < n; i++) {
+                const zc t1 = z(i, k), t2 = z(i, k + 1);
+                z(i, k) = cs * t1 + std::conj(sn) * t2;
+                z(i, k + 1) = -sn * t1 + cs * t2;
+            }
+            if (k < hi - 1) {
+                x = h(k + 1, k);
+                y = h(k + 2, k);
+            }
+        }
+    }
+    return true;
+}
+
+static bool invert(int n, std::vector<zc> A, std::vector<zc> &Ainv) {
+    Ainv.assign((size_t)n * n, zc(0, 0));
+    for (int i = 0; i < n; i++) Ainv[(size_t)i * n + i] = 1.0;
+    for (int k = 0; k < n; k++) {
+        int p = k;
+        for (int i = k + 1; i < n; i++)
+            if (std::abs(A[(size_t)i * n + k]) > std::abs(A[(size_t)p * n + k])) p = i;
+        if (std::abs(A[(size_t)p * n + k]) == 0.0) return false;
+        if (p != k)
+            for (int j = 0; j < n; j++) {
+                std::swap(A[(size_t)k * n + j], A[(size_t)p * n + j]);
+                std::swap(Ainv[(size_t)k * n + j], Ainv[(size_t)p * n + j]);
+            }
+        const zc inv = 1.0 / A[(size_t)k * n + k];
+        for (int j = 0; j < n; j++) {
+            A[(size_t)k * n + j] *= inv;
+            Ainv[(size_t)k * n + j] *= inv;
+        }
+        for (int i = 0; i < n; i++) {
+            if (i == k) continue;
+            const zc f = A[(size_t)i * n + k];
+            if (f == zc(0, 0)) continue;
+            for (int j = 0; j < n; j++) {
+                A[(size_t)i * n + j] -= f * A[(size_t)k * n + j];
+                Ainv[(size_t)i * n + j] -= f * Ainv[(size_t)k * n + j];
+            }
+        }
+    }
+    return true;
+}
+
+static bool zpml_eigen(const std::vector<zc> &cm, const std::vector<zc> &cp, std::vector<zc> &lam,
+                       std::vector<zc> &W, std::vector<zc> &Wi, double *resid) {
+    const int n = (int)cm.size();
+    std::vector<zc> D((size_t)n * n, zc(0, 0));
+    for (int i = 0; i < n; i++) {
+        D[(size_t)i * n + i] = -(cm[i] + cp[i]);
+        if (i + 1 < n) {
+            D[(size_t)i * n + i + 1] = cp[i];
+            D[(size_t)(i + 1) * n + i] = cm[i + 1];
+        }
+    }
+    std::vector<zc> T = D, Z;
+    if (!schur_hessenberg(n, T, Z)) return false;
+    lam.resize(n);
+    for (int k = 0; k < n; k++) lam[k] = T[(size_t)k * n + k];
+    double tnorm = 0;
+    for (auto &v : T) tnorm = std::max(tnorm, std::abs(v));
+    const double small = 1e-14 * std::max(tnorm, 1e-300);
+    W.assign((size_t)n * n, zc(0, 0));
+    std::vector<zc> y(n);
+    for (int k = 0; k < n; k++) {
+        std::fill(y.begin(), y.end(), zc(0, 0));
+        y[k] = 1.0;
+        for (int j = k - 1; j >= 0; j--) {
+            zc sum = 0.0;
+            for (int l = j + 1; l <= k; l++) sum += T[(size_t)j * n + l] * y[l];
+            zc den = T[(size_t)j * n + j] - lam[k];
+            if (std::abs(den) < small) den = small;
+            y[j] = -sum / den;
+        }
+        double nrm = 0;
+        for (int i = 0; i < n; i++) {
+            zc v = 0.0;
+            for (int l = 0; l <= k; l++) v += Z[(size_t)i * n + l] * y[l];
+            W[(size_t)i * n + k] = v;
+            nrm += std::norm(v);
+        }
+        nrm = std::sqrt(nrm);
+        for (int i = 0; i < n; i++) W[(size_t)i * n + k] /= nrm;
+    }
+    if (!invert(n, W, Wi)) return false;
+    // residual max_k ||D w_k - lam_k w_k|| / ||D||
+    double r = 0, dn = 0;
+    for (auto &v : D) dn = std::max(dn, std::abs(v));
+    for (int k = 0; k < n; k++)
+        for (int i = 0; i < n; i++) {
+            zc v = -lam[k] * W[(size_t)i * n + k];
+            for (int j = std::max(0, i - 1); j <= std::min(n - 1, i + 1); j++) v += D[(size_t)i * n + j] * W[(size_t)j * n + k];
+            r = std::max(r, std::abs(v) / dn);
+        }
+    *resid = r;
+    return r < 1e-8;
+}
+
 void build_fft_plan(int n, FftPlan &plan, std::vector<zc> &tables) {
     plan = FftPlan();
     plan.n = n;
@@ -229,17 +394,22 @@ int ctx_setup_tables(helm3d_ctx *c, const double *s2) {
         (rc = upload_c64(c, &c->d_cmy64, c->cmy, "cmy64")) || (rc = upload_c64(c, &c->d_cpy64, c->cpy, "cpy64")) ||
         (rc = upload_c64(c, &c->d_cmz64, c->cmz, "cmz64")) || (rc = upload_c64(c, &c->d_cpz64, c->cpz, "cpz64")))
         return rc;
-    {
-        const size_t esz = c->c64 ? 4 : 8;
-        if ((rc = dalloc(c, &c->d_kz2, nz * esz + 16, "kz2"))) return rc;
-        if (c->c64) {
-            std::vector<float> t(c->kz2.begin(), c->kz2.end());
-            rc = cuda_check(c, cudaMemcpy(c->d_kz2, t.data(), nz * 4, cudaMemcpyHostToDevice), "kz2");
-        } else {
-            rc = cuda_check(c, cudaMemcpy(c->d_kz2, c->kz2.data(), nz * 8, cudaMemcpyHostToDevice), "kz2");
-        }
-        if (rc) return rc;
+    // per-mode complex shift added to the 2D diagonal: -kz^2 (FFT) or the
+    // eigenvalue lambda_k of the z operator (PML eigenbasis)
+    c->zeig = (o.mode == HELM3D_MODE_N && o.z_transform == HELM3D_ZT_PML_EIGEN);
+    c->zshift.assign(nz, zc(0, 0));
+    if (c->zeig) {
+        double resid = 0;
+        if (!zpml_eigen(c->cmz, c->cpz, c->zshift, c->zW, c->zWi, &resid))
+            return set_error(c, HELM3D_ERR_ARG, "eigen-decomposition of the z operator failed (residual " +
+                                                    std::to_string(resid) + ")");
+        if ((rc = upload_c64(c, &c->d_zW64, c->zW, "z eigenvectors c128")) ||
+            (rc = upload_c64(c, &c->d_zWi64, c->zWi, "z eigenvectors inverse c128")))
+            return rc;
+    } else {
+        for (int k = 0; k < nz; k++) c->zshift[k] = -c->kz2[k];
     }
+    if ((rc = upload_c(c, &c->d_kz2, c->zshift, "mode shifts"))) return rc;
     if (o.mode == HELM3D_MODE_N) {
         if ((rc = dalloc(c, (void **)&c->d_s2, sizeof(double) * c->N, "s2"))) return rc;
         if ((rc = cuda_check(c, cudaMemcpy(c->d_s2, s2, sizeof(double) * c->N, cudaMemcpyHostToDevice), "s2")))

@@ -90,6 +90,8 @@ static SweepArgs sweep_args(helm3d_ctx *c) {
 // planes = FFT_z(xscale * x); per-kz block sweep in place
 static int prec_to_planes(helm3d_ctx *c, const double2 *x, double xscale) {
     RC(timed(c, HELM3D_K_FFT_FWD, 1, [&] {
+        if (c->zeig)
+            return launch_ztrans_forward(c->c64, x, xscale, c->d_planes, c->grid.nz, c->plane, c->d_zWi64, c->stream);
         return launch_fft_forward(c->c64, x, xscale, c->d_planes, c->grid.nz, c->plane, c->plan, c->d_tw, c->stream);
     }));
     const SweepArgs s = sweep_args(c);
@@ -99,6 +101,7 @@ static int prec_to_planes(helm3d_ctx *c, const double2 *x, double xscale) {
 int apply_prec(helm3d_ctx *c, const double2 *x, double xscale, double2 *y) {
     RC(prec_to_planes(c, x, xscale));
     return timed(c, HELM3D_K_FFT_INV, 1, [&] {
+        if (c->zeig) return launch_ztrans_inverse(c->c64, c->d_planes, y, c->grid.nz, c->plane, c->d_zW64, c->stream);
         return launch_fft_inverse(c->c64, c->d_planes, y, c->grid.nz, c->plane, c->plan, c->d_tw, 0, nullptr, 0.0,
                                   nullptr, c->stream);
     });

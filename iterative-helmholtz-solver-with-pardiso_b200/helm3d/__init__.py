@@ -26,6 +26,7 @@ lib = ctypes.CDLL(LIB_PATH)
 MODE_R, MODE_N = 0, 1
 PREC_C128, PREC_C64 = 0, 1
 KZ_DISCRETE, KZ_CONTINUOUS, KZ_REFERENCE = 0, 1, 2
+ZT_FFT, ZT_PML_EIGEN = 0, 1
 
 OK = 0
 ERR_ARG, ERR_OOM, ERR_CUDA, ERR_SINGULAR, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_NONFINITE, ERR_NO_DEVICE = range(1, 9)
@@ -43,7 +44,7 @@ class Opts(ctypes.Structure):
                 ("beta_prec", ctypes.c_double), ("beta_phys", ctypes.c_double), ("s2_l0", ctypes.c_double),
                 ("quirk_q1", ctypes.c_int), ("restart", ctypes.c_int), ("max_iter", ctypes.c_int),
                 ("tol", ctypes.c_double), ("stop_phys", ctypes.c_int), ("device", ctypes.c_int),
-                ("verbose", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("z_transform", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):

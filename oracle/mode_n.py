@@ -22,6 +22,11 @@ applied as forward FFT along z (unscaled), one 2D solve per kz, inverse FFT
 (4/hz^2) sin^2(pi k / nz) ("discrete", the default), the continuous
 (2 pi min(k, nz-k) / Lz)^2 ("continuous"), or the reference's table q2.
 
+With z_transform="eigen" the FFT is replaced by the eigenvectors of the 1D
+z operator including its PML, D_z = W diag(lam) W^{-1}: the 2D system of
+mode k gets the shift lam_k instead of -kz^2, and M^{-1} = W diag(M_k^{-1})
+W^{-1} (exact when the medium is z-invariant and beta_prec = 0).
+
 FGMRES here is flexible (Z_j = M^{-1} V_j kept), right preconditioned, with
 Givens rotations and classical Gram-Schmidt applied twice (CGS2).
 """
@@ -69,6 +74,8 @@ class ModeN:
     kz2: np.ndarray
     shifts: np.ndarray
     lus: list
+    zW: np.ndarray | None = None
+    zWi: np.ndarray | None = None
 
     @property
     def shape(self):
@@ -124,10 +131,15 @@ class ModeN:
 
     # ------------------------------------------------------------------ M
     def apply_prec(self, v: np.ndarray) -> np.ndarray:
-        vh = np.fft.fft(v.reshape(self.shape), axis=0)
+        if self.zW is not None:
+            vh = np.tensordot(self.zWi, v.reshape(self.shape), axes=(1, 0))
+        else:
+            vh = np.fft.fft(v.reshape(self.shape), axis=0)
         out = np.empty_like(vh)
         for k in range(self.shape[0]):
             out[k] = self.lus[k].solve(vh[k].ravel()).reshape(vh[k].shape)
+        if self.zW is not None:
+            return np.tensordot(self.zW, out, axes=(1, 0))
         return np.fft.ifft(out, axis=0)
 
     def apply_prec_adjoint(self, v: np.ndarray) -> np.ndarray:
@@ -139,7 +151,15 @@ class ModeN:
         return np.fft.ifft(out, axis=0)
 
 
-def setup(prob: Problem, beta_prec: float = 0.5, kz_symbol: str = "discrete", factor: bool = True) -> ModeN:
+def zpml_eigen(cm: np.ndarray, cp: np.ndarray):
+    """Eigen-decomposition of the tridiagonal z operator with its PML."""
+    D = np.diag(-(cm + cp)) + np.diag(cp[:-1], 1) + np.diag(cm[1:], -1)
+    lam, W = np.linalg.eig(D)
+    return lam, W, np.linalg.inv(W)
+
+
+def setup(prob: Problem, beta_prec: float = 0.5, kz_symbol: str = "discrete", factor: bool = True,
+          z_transform: str = "fft") -> ModeN:
     ax = Axis(n=prob.nx, h=prob.h, pml_pts=prob.pml)
     ay = Axis(n=prob.ny, h=prob.h, pml_pts=prob.pml)
     az = Axis(n=prob.nz, h=prob.h, pml_pts=prob.pml)
@@ -148,12 +168,17 @@ def setup(prob: Problem, beta_prec: float = 0.5, kz_symbol: str = "discrete", fa
     kz2 = kz2_table(prob.nz, prob.h, kz_symbol)
     s0 = s0_squared(prob.s2, prob.pml)
     base = (prob.omega ** 2) * s0 * complex(1.0, beta_prec)
-    shifts = base[None, :, :] - kz2[:, None, None]
+    zW = zWi = None
+    if z_transform == "eigen":
+        lam, zW, zWi = zpml_eigen(*coef["z"])
+        shifts = base[None, :, :] + lam[:, None, None]
+    else:
+        shifts = base[None, :, :] - kz2[:, None, None]
     lus = []
     if factor:
         for k in range(prob.nz):
             lus.append(spla.splu(assemble_2d(g, shifts[k])))
-    return ModeN(prob, g, beta_prec, coef, kz2, shifts, lus)
+    return ModeN(prob, g, beta_prec, coef, kz2, shifts, lus, zW, zWi)
 
 
 @dataclass
