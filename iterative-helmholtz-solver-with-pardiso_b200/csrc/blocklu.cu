@@ -57,6 +57,13 @@ template <typename R> struct FactorK {
 
 template <typename R> __device__ __forceinline__ R cabs1(cplx<R> a) { return fabs(a.x) + fabs(a.y); }
 
+// bounded wait on a local mbarrier; cluster-scope acquire only when other
+// CTAs of the cluster arrive on it
+template <int C> __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+    if constexpr (C == 1) return mbar_wait_bounded_cta(addr, parity, kWaitLimit);
+    else return mbar_wait_bounded_cluster(addr, parity, kWaitLimit);
+}
+
 // Predicated selects in inline PTX.  Written as plain `if (a == q) x = S[q]`
 // chains, the compiler folds the unrolled selects back into one dynamically
 // indexed load, which moves the whole register tile to local memory.
@@ -182,74 +189,84 @@ __global__ void __launch_bounds__(NW * 32, 1) factor_kernel(FactorK<R> a) {
             }
         }
 
-        // ---- Gauss-Jordan with partial pivoting
+        // ---- Gauss-Jordan with partial pivoting, pivot search one step ahead:
+        // the warp owning column k+1 updates that column first, searches and
+        // publishes pivot k+1, then updates its other columns.
         uint32_t used = 0;
+        const long t0 = t;
+        auto publish = [&](int k) {
+            // owner warp of column k: pick the pivot among unused rows and
+            // write column k, the row index and the value into ring slot s
+            const long tk = t0 + k;
+            const int s = (int)(tk % kRing);
+            const uint32_t ph = (uint32_t)((tk / kRing) & 1);
+            const int ob = (k % NPC) % CB;
+            if (!dead && !mbar_wait<C>(smem_u32(&sm.empty[s]), ph ^ 1u)) {
+                dead = true;
+                atomicOr(a.status, 2);
+            }
+            R best = (R)-1;
+            int bi = NP;
+#pragma unroll
+            for (int ra = 0; ra < RB; ra++) {
+                const int i = lane + 32 * ra;
+                const R v = cabs1<R>(sel_col<CB>(S[ra], ob));
+                if (i < n && !((used >> ra) & 1u) && v > best) {
+                    best = v;
+                    bi = i;
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const R ov = __shfl_xor_sync(0xffffffffu, best, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                if (ov > best || (ov == best && oi < bi)) {
+                    best = ov;
+                    bi = oi;
+                }
+            }
+            const int r = bi < n ? bi : k;  // no candidate only if the block is broken
+            Cx pvs = mkc<R>(0, 0);
+#pragma unroll
+            for (int ra = 0; ra < RB; ra++) pvs = csel((r >> 5) == ra, sel_col<CB>(S[ra], ob), pvs);
+            const Cx pv = shfl_c(pvs, r & 31);
+            if constexpr (C == 1) {
+#pragma unroll
+                for (int ra = 0; ra < RB; ra++) sm.ringcol[s * NP + lane + 32 * ra] = sel_col<CB>(S[ra], ob);
+                if (lane == 0) {
+                    sm.ringpv[s] = pv;
+                    sm.ringr[s] = r;
+                    sm.perm[k] = r;
+                }
+                mbar_arrive_local(&sm.full[s]);
+            } else {
+                const uint32_t a_col = smem_u32(&sm.ringcol[s * NP]);
+                const uint32_t a_pv = smem_u32(&sm.ringpv[s]);
+                const uint32_t a_r = smem_u32(&sm.ringr[s]);
+                const uint32_t a_perm = smem_u32(&sm.perm[k]);
+                const uint32_t a_full = smem_u32(&sm.full[s]);
+#pragma unroll
+                for (int q = 0; q < C; q++) {
+#pragma unroll
+                    for (int ra = 0; ra < RB; ra++)
+                        st_cluster_c(mapa_u32(a_col + (lane + 32 * ra) * (uint32_t)sizeof(Cx), q),
+                                     sel_col<CB>(S[ra], ob));
+                    if (lane == 0) {
+                        st_cluster_c(mapa_u32(a_pv, q), pv);
+                        st_cluster_u32(mapa_u32(a_r, q), (uint32_t)r);
+                        st_cluster_u32(mapa_u32(a_perm, q), (uint32_t)r);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < C; q++) mbar_arrive_cluster(mapa_u32(a_full, q));
+            }
+        };
+        auto owns = [&](int k) { return (int)rank == k / NPC && warp == (k % NPC) / CB; };
+        if (owns(0)) publish(0);
         for (int k = 0; k < n; k++, t++) {
             const int s = (int)(t % kRing);
             const uint32_t ph = (uint32_t)((t / kRing) & 1);
-            const int oc = k / NPC, kl = k % NPC, ow = kl / CB, ob = kl % CB;
-            if ((int)rank == oc && warp == ow) {
-                if (!dead && !mbar_wait_bounded_cluster(smem_u32(&sm.empty[s]), ph ^ 1u, kWaitLimit)) {
-                    dead = true;
-                    atomicOr(a.status, 2);
-                }
-                R best = (R)-1;
-                int bi = NP;
-#pragma unroll
-                for (int ra = 0; ra < RB; ra++) {
-                    const int i = lane + 32 * ra;
-                    const R v = cabs1<R>(sel_col<CB>(S[ra], ob));
-                    if (i < n && !((used >> ra) & 1u) && v > best) {
-                        best = v;
-                        bi = i;
-                    }
-                }
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    const R ov = __shfl_xor_sync(0xffffffffu, best, off);
-                    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                    if (ov > best || (ov == best && oi < bi)) {
-                        best = ov;
-                        bi = oi;
-                    }
-                }
-                const int r = bi < n ? bi : k;  // no candidate only if the block is broken
-                Cx pvs = mkc<R>(0, 0);
-#pragma unroll
-                for (int ra = 0; ra < RB; ra++) pvs = csel((r >> 5) == ra, sel_col<CB>(S[ra], ob), pvs);
-                const Cx pv = shfl_c(pvs, r & 31);
-                if constexpr (C == 1) {
-#pragma unroll
-                    for (int ra = 0; ra < RB; ra++) sm.ringcol[s * NP + lane + 32 * ra] = sel_col<CB>(S[ra], ob);
-                    if (lane == 0) {
-                        sm.ringpv[s] = pv;
-                        sm.ringr[s] = r;
-                        sm.perm[k] = r;
-                    }
-                    mbar_arrive_cluster(smem_u32(&sm.full[s]));
-                } else {
-                    const uint32_t a_col = smem_u32(&sm.ringcol[s * NP]);
-                    const uint32_t a_pv = smem_u32(&sm.ringpv[s]);
-                    const uint32_t a_r = smem_u32(&sm.ringr[s]);
-                    const uint32_t a_perm = smem_u32(&sm.perm[k]);
-                    const uint32_t a_full = smem_u32(&sm.full[s]);
-#pragma unroll
-                    for (int q = 0; q < C; q++) {
-#pragma unroll
-                        for (int ra = 0; ra < RB; ra++)
-                            st_cluster_c(mapa_u32(a_col + (lane + 32 * ra) * (uint32_t)sizeof(Cx), q),
-                                         sel_col<CB>(S[ra], ob));
-                        if (lane == 0) {
-                            st_cluster_c(mapa_u32(a_pv, q), pv);
-                            st_cluster_u32(mapa_u32(a_r, q), (uint32_t)r);
-                            st_cluster_u32(mapa_u32(a_perm, q), (uint32_t)r);
-                        }
-                    }
-#pragma unroll
-                    for (int q = 0; q < C; q++) mbar_arrive_cluster(mapa_u32(a_full, q));
-                }
-            }
-            if (!dead && !mbar_wait_bounded_cluster(smem_u32(&sm.full[s]), ph, kWaitLimit)) {
+            if (!dead && !mbar_wait<C>(smem_u32(&sm.full[s]), ph)) {
                 dead = true;
                 atomicOr(a.status, 2);
             }
@@ -270,12 +287,12 @@ __global__ void __launch_bounds__(NW * 32, 1) factor_kernel(FactorK<R> a) {
             Cx prow[CB];
 #pragma unroll
             for (int b = 0; b < CB; b++) prow[b] = cmul(shfl_c(sel_row<RB, CB>(S, ar, b), rl), pinv);
+            // element update of column slot b for step k
+            auto update_col = [&](int b) {
+                const bool isk = (col0 + b) == k;
 #pragma unroll
-            for (int ra = 0; ra < RB; ra++) {
-                const bool isr = (lane + 32 * ra) == r;
-#pragma unroll
-                for (int b = 0; b < CB; b++) {
-                    const bool isk = (col0 + b) == k;
+                for (int ra = 0; ra < RB; ra++) {
+                    const bool isr = (lane + 32 * ra) == r;
                     Cx v;
                     if (isr) v = isk ? pinv : prow[b];
                     else if (isk) v = mkc<R>(-(colk[ra].x * pinv.x - colk[ra].y * pinv.y),
@@ -283,8 +300,19 @@ __global__ void __launch_bounds__(NW * 32, 1) factor_kernel(FactorK<R> a) {
                     else v = cfms(colk[ra], prow[b], S[ra][b]);
                     S[ra][b] = v;
                 }
-            }
+            };
             if (lane == rl) used |= 1u << ar;
+            const bool ahead = (k + 1 < n) && owns(k + 1);
+            const int obn = ((k + 1) % NPC) % CB;
+            if (ahead) {
+#pragma unroll
+                for (int b = 0; b < CB; b++)
+                    if (b == obn) update_col(b);
+                publish(k + 1);
+            }
+#pragma unroll
+            for (int b = 0; b < CB; b++)
+                if (!ahead || b != obn) update_col(b);
             __syncwarp();
             // Release slot s on the `empty` barrier of every CTA: whichever CTA
             // produces the next step that uses slot s, its barrier has then
@@ -292,7 +320,7 @@ __global__ void __launch_bounds__(NW * 32, 1) factor_kernel(FactorK<R> a) {
             // can wait on the parity of the global step count.
             if (lane == 0 && (t + kRing) / n < ny) {
                 if constexpr (C == 1) {
-                    mbar_arrive_cluster(smem_u32(&sm.empty[s]));
+                    mbar_arrive_local(&sm.empty[s]);
                 } else {
                     const uint32_t a_empty = smem_u32(&sm.empty[s]);
 #pragma unroll

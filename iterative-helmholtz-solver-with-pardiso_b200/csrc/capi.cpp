@@ -176,21 +176,8 @@ int helm3d_create(const helm3d_grid *grid, const double *s2, const helm3d_opts *
         return fail(rc);
     c->stream = c->own_stream;
     auto t0 = std::chrono::steady_clock::now();
-    // the medium is read on the host for the set-up tables
-    std::vector<double> s2h;
-    const double *s2p = s2;
-    if (is_device_ptr(s2)) {
-        s2h.resize(c->N);
-        if ((rc = cuda_check(c, cudaMemcpy(s2h.data(), s2, sizeof(double) * c->N, cudaMemcpyDeviceToHost), "s2")))
-            return fail(rc);
-        s2p = s2h.data();
-    }
-    for (long q = 0; q < c->N; q++)
-        if (!std::isfinite(s2p[q])) {
-            c->last_error = "medium has NaN/Inf";
-            return fail(HELM3D_ERR_NONFINITE);
-        }
-    if ((rc = ctx_setup_tables(c, s2p)) || (rc = ctx_factor(c))) return fail(rc);
+    if ((rc = ctx_setup_grid(c)) || (rc = ctx_setup_medium(c, s2, is_device_ptr(s2))) || (rc = ctx_factor(c)))
+        return fail(rc);
     c->ms_factor = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     g_create_error.clear();
     *out = c;
@@ -200,17 +187,7 @@ int helm3d_create(const helm3d_grid *grid, const double *s2, const helm3d_opts *
 int helm3d_set_medium(helm3d_ctx *c, const double *s2) {
     if (!c || !s2) return HELM3D_ERR_ARG;
     cudaSetDevice(c->device);
-    std::vector<double> s2h;
-    const double *s2p = s2;
-    if (is_device_ptr(s2)) {
-        s2h.resize(c->N);
-        int rc = cuda_check(c, cudaMemcpy(s2h.data(), s2, sizeof(double) * c->N, cudaMemcpyDeviceToHost), "s2");
-        if (rc) return rc;
-        s2p = s2h.data();
-    }
-    for (long q = 0; q < c->N; q++)
-        if (!std::isfinite(s2p[q])) return HELM3D_ERR_NONFINITE;
-    int rc = ctx_setup_tables(c, s2p);
+    int rc = ctx_setup_medium(c, s2, is_device_ptr(s2));
     if (rc) return rc;
     return ctx_factor(c);
 }

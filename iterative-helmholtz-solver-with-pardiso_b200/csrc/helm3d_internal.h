@@ -129,6 +129,10 @@ int launch_sub_dl(const double2 *x, const double2 *dl, const double2 *t, double2
 int launch_set_scale(const double2 *nrm, double *vs, int j, cudaStream_t s);
 int launch_add_vec(const double2 *a, const double2 *b, double2 *out, int n, cudaStream_t s);
 int launch_zero(void *p, size_t bytes, cudaStream_t s);
+// base2d[q] = w2 (1 + i beta) mean_{zlo <= k < zhi} s2[k][q]  (P precision);
+// sets bit 4 of *status when s2 holds NaN/Inf
+int launch_base2d(bool c64, const double *s2, int nz, long plane, int zlo, int zhi, double w2, double beta,
+                  void *base2d, int *status, cudaStream_t s);
 // gradient accumulation g += Re(conj(lam) * w2 * u)  (d A / d s2 = w2 (1 + i beta))
 int launch_grad_accum(const double2 *lam, const double2 *u, double w2, double beta, double *g, long N,
                       cudaStream_t s);
@@ -225,7 +229,8 @@ template <class F> int timed(helm3d_ctx *c, int kind, int kernels, F &&f) {
     return rc;
 }
 
-int ctx_setup_tables(helm3d_ctx *c, const double *s2_host);   // host FP64 tables + upload + factor
+int ctx_setup_grid(helm3d_ctx *c);                                   // grid/option tables, allocations
+int ctx_setup_medium(helm3d_ctx *c, const double *s2, bool s2_on_device);  // medium tables
 int ctx_factor(helm3d_ctx *c);
 int apply_prec(helm3d_ctx *c, const double2 *x, double xscale, double2 *y);
 int apply_op(helm3d_ctx *c, const double2 *x, double xscale, double2 *y);

@@ -208,6 +208,23 @@ __global__ void scatter_add_kernel(const double2 *__restrict__ vals, const long 
     }
 }
 
+template <typename R>
+__global__ void base2d_kernel(const double *__restrict__ s2, int nz, long plane, int zlo, int zhi, double w2,
+                              double beta, cplx<R> *__restrict__ out, int *status) {
+    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= plane) return;
+    double s = 0.0;
+    bool bad = false;
+    for (int k = 0; k < nz; k++) {
+        const double v = s2[(long)k * plane + q];
+        bad |= !isfinite(v);
+        if (k >= zlo && k < zhi) s += v;
+    }
+    s *= w2 / (double)(zhi - zlo);
+    out[q] = cvt<cplx<R>, double2>(make_double2(s, s * beta));
+    if (bad) atomicOr(status, 16);
+}
+
 static inline bool ok() { return cudaGetLastError() == cudaSuccess; }
 
 static int grid_for(long N) {
@@ -267,6 +284,14 @@ int launch_set_scale(const double2 *nrm, double *vs, int j, cudaStream_t s) {
 
 int launch_add_vec(const double2 *a, const double2 *b, double2 *out, int n, cudaStream_t s) {
     add_vec_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, b, out, n);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_base2d(bool c64, const double *s2, int nz, long plane, int zlo, int zhi, double w2, double beta,
+                  void *base2d, int *status, cudaStream_t s) {
+    const unsigned grid = (unsigned)((plane + 255) / 256);
+    if (c64) base2d_kernel<float><<<grid, 256, 0, s>>>(s2, nz, plane, zlo, zhi, w2, beta, (float2 *)base2d, status);
+    else base2d_kernel<double><<<grid, 256, 0, s>>>(s2, nz, plane, zlo, zhi, w2, beta, (double2 *)base2d, status);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 

@@ -295,11 +295,13 @@ static int upload_c64(helm3d_ctx *c, double2 **dst, const std::vector<zc> &v, co
     return cuda_check(c, cudaMemcpy(*dst, v.data(), v.size() * 16, cudaMemcpyHostToDevice), what);
 }
 
-int ctx_setup_tables(helm3d_ctx *c, const double *s2) {
+// Everything that depends on the grid and options only: PML tables, the kz
+// table or the z eigenbasis, the FFT plan, uploads and allocations.
+int ctx_setup_grid(helm3d_ctx *c) {
     const helm3d_grid &g = c->grid;
     const helm3d_opts &o = c->opts;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const double w = g.omega, w2 = w * w;
+    const double w = g.omega;
     pml_table(nx, g.pml_x, g.hx, w, c->cmx, c->cpx);
     pml_table(ny, g.pml_y, g.hy, w, c->cmy, c->cpy);
     pml_table(nz, g.pml_z, g.hz, w, c->cmz, c->cpz);
@@ -310,8 +312,8 @@ int ctx_setup_tables(helm3d_ctx *c, const double *s2) {
     for (int k = 0; k < nz; k++) {
         double v;
         if (o.kz_symbol == HELM3D_KZ_DISCRETE) {
-            const double s = std::sin(kPi * k / nz);
-            v = 4.0 / (g.hz * g.hz) * s * s;
+            const double sn = std::sin(kPi * k / nz);
+            v = 4.0 / (g.hz * g.hz) * sn * sn;
         } else if (o.kz_symbol == HELM3D_KZ_CONTINUOUS) {
             const int kk = std::min(k, nz - k);
             v = (2.0 * kPi * kk / lz) * (2.0 * kPi * kk / lz);
@@ -322,73 +324,9 @@ int ctx_setup_tables(helm3d_ctx *c, const double *s2) {
         }
         c->kz2[k] = v;
     }
-
-    // z-mean slowness of the preconditioner, per (j, i)
-    c->base2d.assign((size_t)nx * ny, zc(0, 0));
-    std::vector<double> dl_s0(0);
-    if (o.mode == HELM3D_MODE_N) {
-        int zlo = g.pml_z, zhi = nz - g.pml_z;
-        if (zhi <= zlo) { zlo = 0; zhi = nz; }
-        for (int j = 0; j < ny; j++)
-            for (int i = 0; i < nx; i++) {
-                double s = 0;
-                for (int k = zlo; k < zhi; k++) s += s2[((long)k * ny + j) * nx + i];
-                s /= (zhi - zlo);
-                c->base2d[(size_t)j * nx + i] = w2 * s * zc(1.0, o.beta_prec);
-            }
-    } else {
-        // mode R: SetSoundSpeed2D (Source/functions.cpp:1686-1738) over the
-        // physical x,y range and the non-sponge z range, j outer / i inner;
-        // with q1 the accumulator carries over between columns.  Then the
-        // edge extension into the x,y PML (Source/functions.cpp:2636-2673).
-        const int spg = g.spg_z, nzp = nz - 2 * spg;
-        std::vector<double> s0((size_t)nx * ny, 0.0);
-        double acc = 0.0;
-        for (int j = g.pml_y; j < ny - g.pml_y; j++)
-            for (int i = g.pml_x; i < nx - g.pml_x; i++) {
-                double col = 0.0;
-                for (int k = spg; k < nz - spg; k++) col += s2[((long)k * ny + j) * nx + i];
-                acc = o.quirk_q1 ? (acc + col) / nzp : col / nzp;
-                const double c0 = std::sqrt(1.0 / acc);
-                s0[(size_t)j * nx + i] = 1.0 / (c0 * c0);
-            }
-        for (int j = 0; j < ny; j++) {
-            for (int i = 0; i < g.pml_x; i++) s0[(size_t)j * nx + i] = s0[(size_t)j * nx + g.pml_x];
-            for (int i = nx - g.pml_x; i < nx; i++) s0[(size_t)j * nx + i] = s0[(size_t)j * nx + nx - g.pml_x - 1];
-        }
-        for (int i = 0; i < nx; i++) {
-            for (int j = 0; j < g.pml_y; j++) s0[(size_t)j * nx + i] = s0[(size_t)g.pml_y * nx + i];
-            for (int j = ny - g.pml_y; j < ny; j++) s0[(size_t)j * nx + i] = s0[(size_t)(ny - g.pml_y - 1) * nx + i];
-        }
-        for (size_t q = 0; q < s0.size(); q++)
-            c->base2d[q] = w2 * (o.s2_l0 > 0 ? o.s2_l0 : s0[q]) * zc(1.0, o.beta_prec);   // q3
-        // dL (Source/functions.cpp:1740-1824)
-        std::vector<zc> dl((size_t)c->N, zc(0, 0));
-        const long pl = c->plane;
-        for (int k = spg; k <= nz - spg && k < nz; k++)
-            for (long q = 0; q < pl; q++)
-                dl[(size_t)k * pl + q] = w2 * (zc(1.0, o.beta_prec) * s0[q] - s2[(size_t)k * pl + q]);
-        const double sigma = 0.3, lzz = g.lz > 0 ? g.lz : nz * g.hz;
-        const double z0 = spg * g.hz, zN = (nz - spg) * g.hz, L0 = z0, Ln = lzz - zN;
-        for (int k = 0; k < spg; k++) {
-            const double zp = k * g.hz;
-            const double e = std::exp(-(zp - z0) * (zp - z0) / (L0 * L0) / (sigma * sigma));
-            for (long q = 0; q < pl; q++) dl[(size_t)k * pl + q] = dl[(size_t)spg * pl + q] * e;
-        }
-        for (int k = nz - spg + 1; k < nz; k++) {
-            const double zp = k * g.hz;
-            const double e = std::exp(-(zp - zN) * (zp - zN) / (Ln * Ln) / (sigma * sigma));
-            for (long q = 0; q < pl; q++) dl[(size_t)k * pl + q] = dl[(size_t)(nz - spg) * pl + q] * e;
-        }
-        int rc = upload_c64(c, &c->d_dl, dl, "dL");
-        if (rc) return rc;
-    }
-
-    // device tables
     int rc;
     if ((rc = upload_c(c, &c->d_cmx, c->cmx, "cmx")) || (rc = upload_c(c, &c->d_cpx, c->cpx, "cpx")) ||
-        (rc = upload_c(c, &c->d_cmy, c->cmy, "cmy")) || (rc = upload_c(c, &c->d_cpy, c->cpy, "cpy")) ||
-        (rc = upload_c(c, &c->d_base2d, c->base2d, "base2d")))
+        (rc = upload_c(c, &c->d_cmy, c->cmy, "cmy")) || (rc = upload_c(c, &c->d_cpy, c->cpy, "cpy")))
         return rc;
     if ((rc = upload_c64(c, &c->d_cmx64, c->cmx, "cmx64")) || (rc = upload_c64(c, &c->d_cpx64, c->cpx, "cpx64")) ||
         (rc = upload_c64(c, &c->d_cmy64, c->cmy, "cmy64")) || (rc = upload_c64(c, &c->d_cpy64, c->cpy, "cpy64")) ||
@@ -410,17 +348,15 @@ int ctx_setup_tables(helm3d_ctx *c, const double *s2) {
         for (int k = 0; k < nz; k++) c->zshift[k] = -c->kz2[k];
     }
     if ((rc = upload_c(c, &c->d_kz2, c->zshift, "mode shifts"))) return rc;
-    if (o.mode == HELM3D_MODE_N) {
-        if ((rc = dalloc(c, (void **)&c->d_s2, sizeof(double) * c->N, "s2"))) return rc;
-        if ((rc = cuda_check(c, cudaMemcpy(c->d_s2, s2, sizeof(double) * c->N, cudaMemcpyHostToDevice), "s2")))
-            return rc;
-    }
     // FFT tables
     std::vector<zc> tw;
     build_fft_plan(nz, c->plan, tw);
     if ((rc = upload_c(c, &c->d_tw, tw, "fft tables"))) return rc;
-    // planes, status, factor storage
+    // medium tables, planes, status, factor storage
     const size_t esz = c->c64 ? 8 : 16;
+    if ((rc = dalloc(c, &c->d_base2d, esz * c->plane + 16, "base2d"))) return rc;
+    if (o.mode == HELM3D_MODE_N && (rc = dalloc(c, (void **)&c->d_s2, sizeof(double) * c->N, "s2"))) return rc;
+    if (o.mode == HELM3D_MODE_R && (rc = dalloc(c, (void **)&c->d_dl, sizeof(double2) * c->N, "dL"))) return rc;
     if ((rc = dalloc(c, &c->d_planes, esz * c->N + 256, "planes"))) return rc;
     if ((rc = dalloc(c, (void **)&c->d_status, 64, "status"))) return rc;
     c->ldg = (nx + 3) & ~3;
@@ -429,11 +365,94 @@ int ctx_setup_tables(helm3d_ctx *c, const double *s2) {
     return HELM3D_OK;
 }
 
+// The medium-dependent tables.  Mode N: s2 is copied to the device and the
+// z-mean of s2 (base2d = omega^2 s0^2 (1 + i beta_prec)) is formed by a kernel,
+// which also flags non-finite values (status bit 4).  Mode R: the reference's
+// c0 (q1 running mean) and dL are formed on the host in FP64.
+int ctx_setup_medium(helm3d_ctx *c, const double *s2, bool s2_on_device) {
+    const helm3d_grid &g = c->grid;
+    const helm3d_opts &o = c->opts;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const double w2 = g.omega * g.omega;
+    int rc = cuda_check(c, cudaMemsetAsync(c->d_status, 0, 64, c->stream), "status reset");
+    if (rc) return rc;
+    if (o.mode == HELM3D_MODE_N) {
+        rc = cuda_check(c, cudaMemcpyAsync(c->d_s2, s2, sizeof(double) * c->N,
+                                           s2_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream),
+                        "s2");
+        if (rc) return rc;
+        int zlo = g.pml_z, zhi = nz - g.pml_z;
+        if (zhi <= zlo) {
+            zlo = 0;
+            zhi = nz;
+        }
+        return timed(c, HELM3D_K_KRYLOV, 1, [&] {
+            return launch_base2d(c->c64, c->d_s2, nz, c->plane, zlo, zhi, w2, o.beta_prec, c->d_base2d, c->d_status,
+                                 c->stream);
+        });
+    }
+    // mode R (host)
+    std::vector<double> s2h;
+    if (s2_on_device) {
+        s2h.resize(c->N);
+        rc = cuda_check(c, cudaMemcpy(s2h.data(), s2, sizeof(double) * c->N, cudaMemcpyDeviceToHost), "s2");
+        if (rc) return rc;
+        s2 = s2h.data();
+    }
+    for (long q = 0; q < c->N; q++)
+        if (!std::isfinite(s2[q])) return set_error(c, HELM3D_ERR_NONFINITE, "medium has NaN/Inf");
+    c->base2d.assign((size_t)nx * ny, zc(0, 0));
+    // SetSoundSpeed2D (Source/functions.cpp:1686-1738) over the physical x,y
+    // range and the non-sponge z range, j outer / i inner; with q1 the
+    // accumulator carries over between columns.  Then the edge extension
+    // into the x,y PML (Source/functions.cpp:2636-2673).
+    const int spg = g.spg_z, nzp = nz - 2 * spg;
+    std::vector<double> s0((size_t)nx * ny, 0.0);
+    double acc = 0.0;
+    for (int j = g.pml_y; j < ny - g.pml_y; j++)
+        for (int i = g.pml_x; i < nx - g.pml_x; i++) {
+            double col = 0.0;
+            for (int k = spg; k < nz - spg; k++) col += s2[((long)k * ny + j) * nx + i];
+            acc = o.quirk_q1 ? (acc + col) / nzp : col / nzp;
+            const double c0 = std::sqrt(1.0 / acc);
+            s0[(size_t)j * nx + i] = 1.0 / (c0 * c0);
+        }
+    for (int j = 0; j < ny; j++) {
+        for (int i = 0; i < g.pml_x; i++) s0[(size_t)j * nx + i] = s0[(size_t)j * nx + g.pml_x];
+        for (int i = nx - g.pml_x; i < nx; i++) s0[(size_t)j * nx + i] = s0[(size_t)j * nx + nx - g.pml_x - 1];
+    }
+    for (int i = 0; i < nx; i++) {
+        for (int j = 0; j < g.pml_y; j++) s0[(size_t)j * nx + i] = s0[(size_t)g.pml_y * nx + i];
+        for (int j = ny - g.pml_y; j < ny; j++) s0[(size_t)j * nx + i] = s0[(size_t)(ny - g.pml_y - 1) * nx + i];
+    }
+    for (size_t q = 0; q < s0.size(); q++)
+        c->base2d[q] = w2 * (o.s2_l0 > 0 ? o.s2_l0 : s0[q]) * zc(1.0, o.beta_prec);   // q3
+    // dL (Source/functions.cpp:1740-1824)
+    std::vector<zc> dl((size_t)c->N, zc(0, 0));
+    const long pl = c->plane;
+    for (int k = spg; k <= nz - spg && k < nz; k++)
+        for (long q = 0; q < pl; q++)
+            dl[(size_t)k * pl + q] = w2 * (zc(1.0, o.beta_prec) * s0[q] - s2[(size_t)k * pl + q]);
+    const double sigma = 0.3, lzz = g.lz > 0 ? g.lz : nz * g.hz;
+    const double z0 = spg * g.hz, zN = (nz - spg) * g.hz, L0 = z0, Ln = lzz - zN;
+    for (int k = 0; k < spg; k++) {
+        const double zp = k * g.hz;
+        const double e = std::exp(-(zp - z0) * (zp - z0) / (L0 * L0) / (sigma * sigma));
+        for (long q = 0; q < pl; q++) dl[(size_t)k * pl + q] = dl[(size_t)spg * pl + q] * e;
+    }
+    for (int k = nz - spg + 1; k < nz; k++) {
+        const double zp = k * g.hz;
+        const double e = std::exp(-(zp - zN) * (zp - zN) / (Ln * Ln) / (sigma * sigma));
+        for (long q = 0; q < pl; q++) dl[(size_t)k * pl + q] = dl[(size_t)(nz - spg) * pl + q] * e;
+    }
+    if ((rc = upload_c64(c, &c->d_dl, dl, "dL"))) return rc;
+    return upload_c(c, &c->d_base2d, c->base2d, "base2d");
+}
+
 int ctx_factor(helm3d_ctx *c) {
     if (!factor_supported(c->c64, c->grid.nx))
         return set_error(c, HELM3D_ERR_ARG, "nx beyond the supported block size of the factor");
-    int rc = cuda_check(c, cudaMemsetAsync(c->d_status, 0, 64, c->stream), "status reset");
-    if (rc) return rc;
+    int rc;
     FactorArgs a;
     a.n = c->grid.nx;
     a.ny = c->grid.ny;
@@ -454,6 +473,7 @@ int ctx_factor(helm3d_ctx *c) {
     if (rc) return rc;
     rc = cuda_check(c, cudaStreamSynchronize(c->stream), "factor");
     if (rc) return rc;
+    if (st & 16) return set_error(c, HELM3D_ERR_NONFINITE, "medium has NaN/Inf");
     if (st & 1) return set_error(c, HELM3D_ERR_SINGULAR, "zero pivot in the block LU factor");
     if (st & 2) return set_error(c, HELM3D_ERR_CUDA, "factor: a bounded wait expired");
     if (st & 8) return set_error(c, HELM3D_ERR_CUDA, "factor: an index check failed");
