@@ -4,6 +4,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <algorithm>
 #include <new>
 
 #include "helm3d_internal.h"
@@ -15,20 +16,30 @@ namespace {
 // message of the last failed helm3d_create on this thread (no context exists then)
 thread_local std::string g_create_error;
 
-// A vector argument: device pointers are used in place, host data is staged.
+// A vector argument of `count` complex values: device pointers are used in
+// place, host data is staged through *slot (capacity *cap values).
 struct VecArg {
     helm3d_ctx *c;
     double2 *dev = nullptr;
     bool staged = false;
     int rc = HELM3D_OK;
-    VecArg(helm3d_ctx *ctx, const void *p, size_t count, bool copy_in, double2 **slot) : c(ctx) {
+    VecArg(helm3d_ctx *ctx, const void *p, size_t count, bool copy_in, double2 **slot, size_t *cap) : c(ctx) {
         if (!p) { rc = set_error(c, HELM3D_ERR_ARG, "null vector argument"); return; }
         if (is_device_ptr(p)) { dev = (double2 *)p; return; }
         staged = true;
+        if (*slot && *cap < count) {
+            rc = cuda_check(c, cudaStreamSynchronize(c->stream), "staging sync");
+            if (rc) return;
+            cudaFree(*slot);
+            c->bytes -= sizeof(double2) * *cap;
+            *slot = nullptr;
+            *cap = 0;
+        }
         if (!*slot) {
             rc = cuda_check(c, cudaMalloc((void **)slot, sizeof(double2) * count), "staging buffer");
             if (rc) return;
             c->bytes += sizeof(double2) * count;
+            *cap = count;
         }
         dev = *slot;
         if (copy_in)
@@ -43,6 +54,25 @@ struct VecArg {
         return cuda_check(c, cudaStreamSynchronize(c->stream), "copy out sync");
     }
 };
+
+// Right-hand sides per lockstep batch: at most kMaxBatch, and as many as the
+// Krylov bases (V, Z), packed iterates, planes and staging of each fit in
+// 85% of the free device memory (plus what the context's Krylov workspace
+// already holds).
+int batch_size(helm3d_ctx *c, int nrhs, bool staged) {
+    const int m = std::max(1, c->opts.restart);
+    const size_t vb = sizeof(double2) * (size_t)c->N;
+    const size_t per = vb * ((size_t)(m + 1) + (c->opts.mode == HELM3D_MODE_N ? m : 0) + 2 + (staged ? 2 : 0)) +
+                       (c->c64 ? 8 : 16) * (size_t)c->N;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    const size_t avail = (size_t)(0.85 * (double)(fr + c->kry_bytes));
+    int R = (int)std::min<size_t>(avail / std::max<size_t>(per, 1), (size_t)kMaxBatch);
+    return std::max(1, std::min(R, nrhs));
+}
 
 int validate(const helm3d_grid *g, const helm3d_opts *o) {
     if (!g || !o) return HELM3D_ERR_ARG;
@@ -203,36 +233,28 @@ static int solve_common(helm3d_ctx *c, const double *f, double *u, int nrhs, hel
         st->relres_phys = 0;
         st->history_len = 0;
     }
-    const bool fdev = is_device_ptr(f), udev = is_device_ptr(u);
+    const bool staged = !is_device_ptr(f) || !is_device_ptr(u);
+    const int B = which == 1 ? 1 : batch_size(c, nrhs, staged);
     int worst = HELM3D_OK;
-    double relres_max = 0, relphys_max = 0;
-    for (int r = 0; r < nrhs; r++) {
-        const double *fr = f + 2 * (size_t)r * c->N;
-        double *ur = u + 2 * (size_t)r * c->N;
-        VecArg fa(c, fr, c->N, true, &c->d_f);
+    for (int r0 = 0; r0 < nrhs; r0 += B) {
+        const int R = std::min(B, nrhs - r0);
+        const size_t count = (size_t)R * c->N;
+        const double *fr = f + 2 * (size_t)r0 * c->N;
+        double *ur = u + 2 * (size_t)r0 * c->N;
+        VecArg fa(c, fr, count, true, &c->d_f, &c->f_cap);
         if (fa.rc) return fa.rc;
-        VecArg ua(c, ur, c->N, false, &c->d_u);
+        VecArg ua(c, ur, count, false, &c->d_u, &c->u_cap);
         if (ua.rc) return ua.rc;
-        (void)fdev;
-        (void)udev;
         int rc;
-        if (which == 0) rc = fgmres(c, fa.dev, ua.dev, false, st);
+        if (which == 0) rc = fgmres(c, fa.dev, ua.dev, R, false, st);
         else if (which == 1) rc = bicgstab(c, fa.dev, ua.dev, st);
-        else rc = fgmres(c, fa.dev, ua.dev, true, st);
+        else rc = fgmres(c, fa.dev, ua.dev, R, true, st);
         if (rc && rc != HELM3D_ERR_NOT_CONVERGED) return rc;
         if (rc) worst = rc;
-        int rc2 = ua.copy_out(ur, c->N);
+        int rc2 = ua.copy_out(ur, count);
         if (rc2) return rc2;
-        if (st) {
-            relres_max = std::max(relres_max, st->relres);
-            relphys_max = std::max(relphys_max, st->relres_phys);
-        }
     }
-    if (st) {
-        st->relres = relres_max;
-        st->relres_phys = relphys_max;
-        st->status = worst;
-    }
+    if (st) st->status = worst;
     return worst;
 }
 
@@ -252,14 +274,16 @@ int helm3d_solve_adjoint(helm3d_ctx *c, const double *g, double *lam, helm3d_sta
 static int apply_common(helm3d_ctx *c, const double *x, double *y, int which) {
     if (!c || !x || !y) return HELM3D_ERR_ARG;
     cudaSetDevice(c->device);
-    VecArg xa(c, x, c->N, true, &c->d_f);
+    VecArg xa(c, x, c->N, true, &c->d_f, &c->f_cap);
     if (xa.rc) return xa.rc;
-    VecArg ya(c, y, c->N, false, &c->d_u);
+    VecArg ya(c, y, c->N, false, &c->d_u, &c->u_cap);
     if (ya.rc) return ya.rc;
+    const VecBatch xb{xa.dev, 0}, yb{ya.dev, 0};
+    const ScaleBatch one{nullptr, 0};
     int rc;
-    if (which == 0) rc = apply_op(c, xa.dev, 1.0, ya.dev);
-    else if (which == 1) rc = apply_op_adjoint(c, xa.dev, 1.0, ya.dev);
-    else rc = apply_prec(c, xa.dev, 1.0, ya.dev);
+    if (which == 0) rc = apply_op(c, xb, 1.0, one, yb, 1);
+    else if (which == 1) rc = apply_op_adjoint(c, xb, 1.0, one, yb, 1);
+    else rc = apply_prec(c, xb, 1.0, one, yb, 1);
     if (rc) return rc;
     rc = ya.copy_out(y, c->N);
     if (rc) return rc;
@@ -290,7 +314,7 @@ int helm3d_destroy(helm3d_ctx *c) {
     void *bufs[] = {c->d_Gt, c->d_tw, c->d_cmx, c->d_cpx, c->d_cmy, c->d_cpy, c->d_base2d, c->d_kz2, c->d_zW, c->d_zWi, c->d_zW64, c->d_zWi64,
                     c->d_cmx64, c->d_cpx64, c->d_cmy64, c->d_cpy64, c->d_cmz64, c->d_cpz64, c->d_s2, c->d_dl,
                     c->d_planes, c->d_status, c->d_V, c->d_Z, c->d_vs, c->d_h, c->d_partials, c->d_f, c->d_u,
-                    c->d_r, c->d_t, c->d_t2, c->d_bic};
+                    c->d_r, c->d_t, c->d_t2, c->d_bic, c->d_Fw, c->d_Uw};
     for (void *p : bufs)
         if (p) cudaFree(p);
     for (auto &e : c->prof_ev) {

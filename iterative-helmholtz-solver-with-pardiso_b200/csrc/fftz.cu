@@ -116,54 +116,69 @@ __device__ cplx<R> *fft_passes(cplx<R> *A, cplx<R> *B, const FftK &fp, const cpl
 
 constexpr int kFftThreads = 256;
 
+// plane index of (row k, column w = i + nx*j) for right-hand side r
+__device__ __forceinline__ long plane_index(const PlaneLayout &L, int r, int k, long w) {
+    const long j = w / L.nx, i = w - j * L.nx;
+    return (long)k * L.plane * L.R + (j * L.R + r) * L.nx + i;
+}
+
 template <typename R, int TW>
-__global__ void __launch_bounds__(kFftThreads) fftz_forward_kernel(FftK fp, const double2 *__restrict__ x,
-                                                                   double scale, cplx<R> *__restrict__ out,
-                                                                   long plane, const cplx<R> *__restrict__ tw) {
+__global__ void __launch_bounds__(kFftThreads) fftz_forward_kernel(FftK fp, VecBatch x, double scale, ScaleBatch sc,
+                                                                   cplx<R> *__restrict__ out, PlaneLayout L,
+                                                                   const cplx<R> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R> *A = reinterpret_cast<cplx<R> *>(smem_raw);
     cplx<R> *B = A + (size_t)fp.n * TW;
     const int col = threadIdx.x % TW, grp = threadIdx.x / TW, ngrp = kFftThreads / TW;
+    const int r = blockIdx.y;
+    const long plane = L.plane;
+    const double2 *xr = x.p + r * x.stride;
+    const double s = scale * (sc.p ? sc.p[r * sc.stride] : 1.0);
     const long w = (long)blockIdx.x * TW + col;
     const bool valid = w < plane;
     for (int row = grp; row < fp.n; row += ngrp) {
-        double2 v = valid ? x[(long)row * plane + w] : make_double2(0.0, 0.0);
-        A[row * TW + col] = cvt<cplx<R>, double2>(make_double2(v.x * scale, v.y * scale));
+        double2 v = valid ? xr[(long)row * plane + w] : make_double2(0.0, 0.0);
+        A[row * TW + col] = cvt<cplx<R>, double2>(make_double2(v.x * s, v.y * s));
     }
     __syncthreads();
     cplx<R> *res = fft_passes<R, false, TW>(A, B, fp, tw, col, grp, ngrp);
     if (valid)
-        for (int row = grp; row < fp.n; row += ngrp) out[(long)row * plane + w] = res[row * TW + col];
+        for (int row = grp; row < fp.n; row += ngrp) out[plane_index(L, r, row, w)] = res[row * TW + col];
 }
 
 template <typename R, int TW>
 __global__ void __launch_bounds__(kFftThreads) fftz_inverse_kernel(FftK fp, const cplx<R> *__restrict__ in,
-                                                                   double2 *__restrict__ y, long plane,
+                                                                   PlaneLayout L, VecBatch y,
                                                                    const cplx<R> *__restrict__ tw, int mode,
-                                                                   const double2 *__restrict__ wv, double scale,
+                                                                   VecBatch wv, double scale, ScaleBatch sc,
                                                                    const double2 *__restrict__ dl) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R> *A = reinterpret_cast<cplx<R> *>(smem_raw);
     cplx<R> *B = A + (size_t)fp.n * TW;
     const int col = threadIdx.x % TW, grp = threadIdx.x / TW, ngrp = kFftThreads / TW;
+    const int r = blockIdx.y;
+    const long plane = L.plane;
     const long w = (long)blockIdx.x * TW + col;
     const bool valid = w < plane;
     for (int row = grp; row < fp.n; row += ngrp)
-        A[row * TW + col] = valid ? in[(long)row * plane + w] : mkc<R>(0, 0);
+        A[row * TW + col] = valid ? in[plane_index(L, r, row, w)] : mkc<R>(0, 0);
     __syncthreads();
     cplx<R> *res = fft_passes<R, true, TW>(A, B, fp, tw, col, grp, ngrp);
     if (!valid) return;
     const double inv_n = 1.0 / (double)fp.n;
+    double2 *yr = y.p + r * y.stride;
+    const double2 *wr = mode == 1 ? wv.p + r * wv.stride : nullptr;
+    const double s = scale * (sc.p ? sc.p[r * sc.stride] : 1.0);
     for (int row = grp; row < fp.n; row += ngrp) {
         const long idx = (long)row * plane + w;
         double2 t = cvt<double2, cplx<R>>(res[row * TW + col]);
         t.x *= inv_n;
         t.y *= inv_n;
         if (mode == 1) {
-            double2 a = wv[idx], d = dl[idx];
-            t = make_double2(scale * a.x - (d.x * t.x - d.y * t.y), scale * a.y - (d.x * t.y + d.y * t.x));
+            const double2 a = wr[idx], d = dl[idx];
+            t = make_double2(s * a.x - (d.x * t.x - d.y * t.y), s * a.y - (d.x * t.y + d.y * t.x));
         }
-        y[idx] = t;
+        yr[idx] = t;
     }
 }
 
@@ -189,57 +204,56 @@ template <typename R> static int pick_tw(int n) {
 }
 
 template <typename R, int TW>
-static int fwd_impl(const double2 *x, double scale, void *planes, long plane, const FftPlan &plan, const void *tw,
-                    cudaStream_t s) {
+static int fwd_impl(const VecBatch &x, double scale, const ScaleBatch &sc, void *planes, const PlaneLayout &L,
+                    const FftPlan &plan, const void *tw, cudaStream_t s) {
     size_t smem = (size_t)2 * plan.n * TW * sizeof(cplx<R>);
     auto kern = fftz_forward_kernel<R, TW>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return HELM3D_ERR_CUDA;
-    dim3 grid((unsigned)((plane + TW - 1) / TW));
-    kern<<<grid, kFftThreads, smem, s>>>(to_k(plan), x, scale, (cplx<R> *)planes, plane, (const cplx<R> *)tw);
+    dim3 grid((unsigned)((L.plane + TW - 1) / TW), (unsigned)L.R);
+    kern<<<grid, kFftThreads, smem, s>>>(to_k(plan), x, scale, sc, (cplx<R> *)planes, L, (const cplx<R> *)tw);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
 template <typename R, int TW>
-static int inv_impl(const void *planes, double2 *y, long plane, const FftPlan &plan, const void *tw, int mode,
-                    const double2 *w, double scale, const double2 *dl, cudaStream_t s) {
+static int inv_impl(const void *planes, const PlaneLayout &L, const VecBatch &y, const FftPlan &plan, const void *tw,
+                    int mode, const VecBatch &w, double scale, const ScaleBatch &sc, const double2 *dl,
+                    cudaStream_t s) {
     size_t smem = (size_t)2 * plan.n * TW * sizeof(cplx<R>);
     auto kern = fftz_inverse_kernel<R, TW>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return HELM3D_ERR_CUDA;
-    dim3 grid((unsigned)((plane + TW - 1) / TW));
-    kern<<<grid, kFftThreads, smem, s>>>(to_k(plan), (const cplx<R> *)planes, y, plane, (const cplx<R> *)tw, mode,
-                                         w, scale, dl);
+    dim3 grid((unsigned)((L.plane + TW - 1) / TW), (unsigned)L.R);
+    kern<<<grid, kFftThreads, smem, s>>>(to_k(plan), (const cplx<R> *)planes, L, y, (const cplx<R> *)tw, mode, w,
+                                         scale, sc, dl);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
-int launch_fft_forward(bool c64, const double2 *x, double scale, void *planes, int nz, long plane,
-                       const FftPlan &plan, const void *tw, cudaStream_t s) {
-    (void)nz;
+int launch_fft_forward(bool c64, const VecBatch &x, double scale, const ScaleBatch &sc, void *planes,
+                       const PlaneLayout &L, const FftPlan &plan, const void *tw, cudaStream_t s) {
     if (c64) {
         int tw_ = pick_tw<float>(plan.n);
-        if (tw_ == 32) return fwd_impl<float, 32>(x, scale, planes, plane, plan, tw, s);
-        if (tw_ == 16) return fwd_impl<float, 16>(x, scale, planes, plane, plan, tw, s);
+        if (tw_ == 32) return fwd_impl<float, 32>(x, scale, sc, planes, L, plan, tw, s);
+        if (tw_ == 16) return fwd_impl<float, 16>(x, scale, sc, planes, L, plan, tw, s);
     } else {
         int tw_ = pick_tw<double>(plan.n);
-        if (tw_ == 32) return fwd_impl<double, 32>(x, scale, planes, plane, plan, tw, s);
-        if (tw_ == 16) return fwd_impl<double, 16>(x, scale, planes, plane, plan, tw, s);
+        if (tw_ == 32) return fwd_impl<double, 32>(x, scale, sc, planes, L, plan, tw, s);
+        if (tw_ == 16) return fwd_impl<double, 16>(x, scale, sc, planes, L, plan, tw, s);
     }
     return HELM3D_ERR_ARG;
 }
 
-int launch_fft_inverse(bool c64, const void *planes, double2 *y, int nz, long plane, const FftPlan &plan,
-                       const void *tw, int mode, const double2 *w, double scale, const double2 *dl,
-                       cudaStream_t s) {
-    (void)nz;
+int launch_fft_inverse(bool c64, const void *planes, const PlaneLayout &L, const VecBatch &y, const FftPlan &plan,
+                       const void *tw, int mode, const VecBatch &w, double scale, const ScaleBatch &sc,
+                       const double2 *dl, cudaStream_t s) {
     if (c64) {
         int tw_ = pick_tw<float>(plan.n);
-        if (tw_ == 32) return inv_impl<float, 32>(planes, y, plane, plan, tw, mode, w, scale, dl, s);
-        if (tw_ == 16) return inv_impl<float, 16>(planes, y, plane, plan, tw, mode, w, scale, dl, s);
+        if (tw_ == 32) return inv_impl<float, 32>(planes, L, y, plan, tw, mode, w, scale, sc, dl, s);
+        if (tw_ == 16) return inv_impl<float, 16>(planes, L, y, plan, tw, mode, w, scale, sc, dl, s);
     } else {
         int tw_ = pick_tw<double>(plan.n);
-        if (tw_ == 32) return inv_impl<double, 32>(planes, y, plane, plan, tw, mode, w, scale, dl, s);
-        if (tw_ == 16) return inv_impl<double, 16>(planes, y, plane, plan, tw, mode, w, scale, dl, s);
+        if (tw_ == 32) return inv_impl<double, 32>(planes, L, y, plan, tw, mode, w, scale, sc, dl, s);
+        if (tw_ == 16) return inv_impl<double, 16>(planes, L, y, plan, tw, mode, w, scale, sc, dl, s);
     }
     return HELM3D_ERR_ARG;
 }

@@ -39,23 +39,39 @@ struct Dev {
     size_t smem_optin = 227 * 1024;
 };
 
-// FFT along z for a batch of columns [0, ncols) of nz-long columns with
-// stride `plane` (= nx*ny).
-//   forward: in = complex128 vector (times `scale`), out = planes of type P
-//   inverse: in = planes of type P, out = complex128 vector scaled 1/nz,
-//            then epilogue: mode 0 y = t; mode 1 y = scale*w - dl*t (mode R's
-//            K x with x = scale*w).
-int launch_fft_forward(bool c64, const double2 *x, double scale, void *planes, int nz, long plane,
-                       const FftPlan &plan, const void *tw, cudaStream_t s);
-int launch_fft_inverse(bool c64, const void *planes, double2 *y, int nz, long plane, const FftPlan &plan,
-                       const void *tw, int mode, const double2 *w, double scale, const double2 *dl,
-                       cudaStream_t s);
+// A batch of R complex128 vectors: vector r at p + r * stride.
+struct VecBatch {
+    double2 *p;
+    long stride;
+};
+// Per-vector real scales: scale of vector r at p[r * stride] (p may be null: 1).
+struct ScaleBatch {
+    const double *p;
+    long stride;
+};
+
+// Spectral planes of R right-hand sides: plane k, y-line j holds the R
+// vectors of length nx contiguously: index ((k*ny + j)*R + r)*nx + i.
+struct PlaneLayout {
+    int nx, ny, nz, R;
+    long plane;               // nx*ny
+};
+
+// FFT along z (stride nx*ny) of every z-column, for R right-hand sides.
+//   forward: planes = FFT(scale * sc_r * x_r)        (complex128 in, P out)
+//   inverse: y_r = IFFT(planes_r) / nz, then epilogue mode 0: y_r = t;
+//            mode 1: y_r = scale * sc_r * w_r - dl * t (mode R's K x).
+int launch_fft_forward(bool c64, const VecBatch &x, double scale, const ScaleBatch &sc, void *planes,
+                       const PlaneLayout &L, const FftPlan &plan, const void *tw, cudaStream_t s);
+int launch_fft_inverse(bool c64, const void *planes, const PlaneLayout &L, const VecBatch &y, const FftPlan &plan,
+                       const void *tw, int mode, const VecBatch &w, double scale, const ScaleBatch &sc,
+                       const double2 *dl, cudaStream_t s);
 
 // Dense z-transforms with the eigenvectors of the z operator (FP64 matrices
-// W, Wi row-major nz x nz): planes = Wi (scale x); y = W planes.
-int launch_ztrans_forward(bool c64, const double2 *x, double scale, void *planes, int nz, long plane,
-                          const double2 *Wi, cudaStream_t s);
-int launch_ztrans_inverse(bool c64, const void *planes, double2 *y, int nz, long plane, const double2 *W,
+// W, Wi row-major nz x nz): planes = Wi (scale sc_r x_r); y_r = W planes_r.
+int launch_ztrans_forward(bool c64, const VecBatch &x, double scale, const ScaleBatch &sc, void *planes,
+                          const PlaneLayout &L, const double2 *Wi, cudaStream_t s);
+int launch_ztrans_inverse(bool c64, const void *planes, const PlaneLayout &L, const VecBatch &y, const double2 *W,
                           cudaStream_t s);
 
 // Block-tridiagonal factor of all nz systems: G^T of every (kz, y-line).
@@ -71,69 +87,69 @@ struct FactorArgs {
 int launch_factor(bool c64, const FactorArgs &a, cudaStream_t s);
 bool factor_supported(bool c64, int n);
 
-// Forward/backward block sweep over y-lines for every kz, in place on the
-// planes (cplx<P> [nz][ny][n]).
+// Forward/backward block sweep over y-lines for every kz and all R
+// right-hand sides of the planes, in place.
 struct SweepArgs {
     int n, ny, nz, ldg;
     const void *Gt;
     const void *cmy, *cpy;
-    void *planes;
-    int nrhs;
-    long rhs_stride;          // elements between right-hand sides' planes
+    void *planes;             // PlaneLayout with R right-hand sides
+    int R;
     int *status;              // device flag: bit 2 = a bounded wait expired
 };
 int launch_sweep(bool c64, const SweepArgs &a, cudaStream_t s);
+constexpr int kMaxBatch = 16;  // right-hand sides per preconditioner launch
 
-// 7-point PML operator y = A x (adjoint: y = A^H x), complex128.
+// 7-point PML operator y_r = A (xscale sc_r x_r) (adjoint: A^H), complex128.
 struct StencilArgs {
     int nx, ny, nz;
     const double2 *cmx, *cpx, *cmy, *cpy, *cmz, *cpz;
     const double *s2;
     double w2;                // omega^2
     double beta_phys;
-    const double2 *x;
+    VecBatch x;
     double xscale;
-    double2 *y;
-    const double2 *f;         // if non-null: y = f - A x
+    ScaleBatch sc;
+    VecBatch y;
+    VecBatch f;               // if f.p: y = f - A x
+    int R;
 };
 int launch_stencil(const StencilArgs &a, bool adjoint, cudaStream_t s);
 
 // ------------------------------------------------------ Krylov kernels
-// All vectors complex128 of length N; V is a basis of nv vectors with
-// leading dimension ldv and per-vector real scale vs[i] (the basis vector is
-// vs[i] * V_i).
+// All vectors complex128 of length N; a basis V_r of nv vectors (leading
+// dimension ldv) per right-hand side r, with real scales vs (basis vector i
+// of r is vs[r][i] V_r[i]).
 struct Reduce {
-    double2 *partials;        // [nblocks][cap] scratch
+    double2 *partials;        // [rmax][nblocks][cap] scratch
     int nblocks;
     int cap;
+    int rmax;
 };
-// out[i] = sum_l conj(vs[i] V_i[l]) w[l]   (i < nv); with wnorm also
-// out[nv].x = ||w||^2 from the same pass
-int launch_dots(const double2 *V, long ldv, const double *vs, int nv, const double2 *w, long N,
-                const Reduce &red, double2 *out, cudaStream_t s, bool wnorm = false);
-// w -= sum_i coef[i] vs[i] V_i; then if redot: out[i] = <vs_i V_i, w_new>;
-// if norm: out[0].x = ||w_new||^2.  (out may be null)
-int launch_update(const double2 *V, long ldv, const double *vs, int nv, const double2 *coef, double2 *w,
-                  long N, int post, const Reduce &red, double2 *out, cudaStream_t s);
-// x += sum_i y[i] zs[i] Z_i
-int launch_combine(const double2 *Z, long ldz, const double *zs, int nz_, const double2 *y, double2 *x, long N,
-                   cudaStream_t s);
-// out = ||x||^2 over the box [x0,x1) x [y0,y1) x [z0,z1) (whole grid by default)
-int launch_norm2_box(const double2 *x, int nx, int ny, int nz, const int box[6], const Reduce &red,
-                     double2 *out, cudaStream_t s);
-// y = a*x + b*y
-int launch_axpby(double2 a, const double2 *x, double2 b, double2 *y, long N, cudaStream_t s);
+// out[r][i] = <vs_r[i] V_r[i], w_r>   (i < nv); with wnorm also out[r][nv].x = ||w_r||^2
+int launch_dots(const VecBatch &V, long ldv, const ScaleBatch &vs, int nv, const VecBatch &w, long N, int R,
+                const Reduce &red, double2 *out, long sOut, cudaStream_t s, bool wnorm = false);
+// w_r -= sum_i coef[r][i] vs_r[i] V_r[i]; post 1: out[r].x = ||w_r||^2
+int launch_update(const VecBatch &V, long ldv, const ScaleBatch &vs, int nv, const double2 *coef, long sCoef,
+                  const VecBatch &w, long N, int R, int post, const Reduce &red, double2 *out, long sOut,
+                  cudaStream_t s);
+// x_r += sum_i y[r][i] zs_r[i] Z_r[i]
+int launch_combine(const VecBatch &Z, long ldz, const ScaleBatch &zs, int nzv, const double2 *y, long sY,
+                   const VecBatch &x, long N, int R, cudaStream_t s);
+// out[r].x = ||x_r||^2 over the box [x0,x1) x [y0,y1) x [z0,z1)
+int launch_norm2_box(const VecBatch &x, int R, int nx, int ny, int nz, const int box[6], const Reduce &red,
+                     double2 *out, long sOut, cudaStream_t s);
+// y_r = a x_r + b y_r
+int launch_axpby(double2 a, const VecBatch &x, double2 b, const VecBatch &y, long N, int R, cudaStream_t s);
 // y = x - dl * t  (mode R's K x from t = L0^{-1} x)
 int launch_sub_dl(const double2 *x, const double2 *dl, const double2 *t, double2 *y, long N, cudaStream_t s);
-// vs[j] = 1/sqrt(nrm[0]); h[j] = sqrt(nrm) etc. -- small device helpers
-int launch_set_scale(const double2 *nrm, double *vs, int j, cudaStream_t s);
-int launch_add_vec(const double2 *a, const double2 *b, double2 *out, int n, cudaStream_t s);
-int launch_zero(void *p, size_t bytes, cudaStream_t s);
+// vs[r][j] = 1 / sqrt(nrm[r].x)
+int launch_set_scale(const double2 *nrm, long sNrm, double *vs, long sVs, int j, int R, cudaStream_t s);
 // base2d[q] = w2 (1 + i beta) mean_{zlo <= k < zhi} s2[k][q]  (P precision);
 // sets bit 4 of *status when s2 holds NaN/Inf
 int launch_base2d(bool c64, const double *s2, int nz, long plane, int zlo, int zhi, double w2, double beta,
                   void *base2d, int *status, cudaStream_t s);
-// gradient accumulation g += Re(conj(lam) * w2 * u)  (d A / d s2 = w2 (1 + i beta))
+// gradient accumulation g += Re(conj(lam) w2 (1 + i beta) u)
 int launch_grad_accum(const double2 *lam, const double2 *u, double w2, double beta, double *g, long N,
                       cudaStream_t s);
 int launch_gather_residual(const double2 *u, const long long *recv, int nrecv, const double2 *d, double2 *res,
@@ -192,11 +208,15 @@ struct helm3d_ctx {
     double2 *d_cmz64 = nullptr, *d_cpz64 = nullptr;
     double *d_s2 = nullptr;        // squared slowness (mode N operator)
     double2 *d_dl = nullptr;       // dL (mode R)
-    void *d_planes = nullptr;      // spectral planes, P precision (one RHS)
+    void *d_planes = nullptr;      // spectral planes, P precision (planes_R right-hand sides)
+    int planes_R = 0;
     int *d_status = nullptr;
-    // Krylov workspace
-    int m_alloc = 0;
+    // Krylov workspace for r_alloc right-hand sides of restart length m_alloc
+    int m_alloc = 0, r_alloc = 0;
+    size_t kry_bytes = 0;
     double2 *d_V = nullptr, *d_Z = nullptr;
+    double2 *d_Fw = nullptr, *d_Uw = nullptr;   // packed right-hand sides / iterates of the active batch
+    size_t f_cap = 0, u_cap = 0;                // staging capacities (vectors) of d_f, d_u
     double *d_vs = nullptr;
     double2 *d_h = nullptr;        // small device scalars
     double2 *d_partials = nullptr;
@@ -232,13 +252,15 @@ template <class F> int timed(helm3d_ctx *c, int kind, int kernels, F &&f) {
 int ctx_setup_grid(helm3d_ctx *c);                                   // grid/option tables, allocations
 int ctx_setup_medium(helm3d_ctx *c, const double *s2, bool s2_on_device);  // medium tables
 int ctx_factor(helm3d_ctx *c);
-int apply_prec(helm3d_ctx *c, const double2 *x, double xscale, double2 *y);
-int apply_op(helm3d_ctx *c, const double2 *x, double xscale, double2 *y);
-int apply_op_adjoint(helm3d_ctx *c, const double2 *x, double xscale, double2 *y);
-int apply_prec_adjoint(helm3d_ctx *c, const double2 *x, double xscale, double2 *y);
-int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, bool adjoint, helm3d_stats *st);
+// operators on R right-hand sides y_r = Op(xscale sc_r x_r) (R <= kMaxBatch)
+int apply_prec(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y, int R);
+int apply_op(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y, int R);
+int apply_op_adjoint(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y,
+                     int R);
+// FGMRES on R right-hand sides f + r N -> u + r N (device), iterated in lockstep
+int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, helm3d_stats *st);
 int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st);
-int ensure_krylov(helm3d_ctx *c, int m);
+int ensure_krylov(helm3d_ctx *c, int m, int R);
 int set_error(helm3d_ctx *c, int code, const std::string &msg);
 bool is_device_ptr(const void *p);   // device or managed memory
 int cuda_check(helm3d_ctx *c, cudaError_t e, const char *what);

@@ -2,8 +2,9 @@
 // Gram-Schmidt dot products and updates (the reference's zdotc/zaxpy loop,
 // Source/FGMRES.cpp:508-517), norms (dznrm2, :519; the physical-domain norm
 // after reducePML3D, :590-592), the solution update x = x0 + Z y (zgemv,
-// :575) and small helpers.  Reductions are two-level and deterministic:
-// fixed-size per-block partials, then one pass over the blocks.
+// :575) and small helpers.  Every kernel takes a batch of R right-hand sides
+// (blockIdx.y = r, per-r pointer strides).  Reductions are two-level and
+// deterministic: fixed-size per-block partials, then one pass over the blocks.
 #include <cuda_runtime.h>
 
 #include "cplx.cuh"
@@ -43,13 +44,18 @@ template <int CH> __device__ __forceinline__ void block_sum(double2 (&acc)[CH], 
     __syncthreads();
 }
 
-// partials[b][i] = sum over this block's l of conj(V_i[l]) w[l] * vs[i]
-// (i < nv); with wnorm, partials[b][nv].x = sum |w[l]|^2 as well
-__global__ void __launch_bounds__(kRedThreads) dots_kernel(const double2 *__restrict__ V, long ldv,
-                                                           const double *__restrict__ vs, int nv,
-                                                           const double2 *__restrict__ w, long N, int wnorm,
+// partials[r][b][i] = sum over this block's l of conj(V_i[l]) w[l] * vs[i]
+// (i < nv); with wnorm, partials[r][b][nv].x = sum |w[l]|^2 as well
+__global__ void __launch_bounds__(kRedThreads) dots_kernel(const double2 *__restrict__ V, long ldv, long sV,
+                                                           const double *__restrict__ vs, long sVs, int nv,
+                                                           const double2 *__restrict__ w, long sW, long N, int wnorm,
                                                            double2 *__restrict__ partials, int cap) {
     __shared__ double2 sh[(kRedThreads / 32) * (kDotChunk + 1)];
+    const int r = blockIdx.y;
+    V += r * sV;
+    w += r * sW;
+    if (vs) vs += r * sVs;
+    partials += (long)r * gridDim.x * cap;
     const long stride = (long)gridDim.x * blockDim.x;
     for (int c0 = 0; c0 < nv || (c0 == 0 && wnorm); c0 += kDotChunk) {
         double2 acc[kDotChunk + 1];
@@ -72,16 +78,17 @@ __global__ void __launch_bounds__(kRedThreads) dots_kernel(const double2 *__rest
     }
 }
 
-// out[i] = sum_b partials[b][i]: one block of kFinalThreads per output i,
+// out[r][i] = sum_b partials[r][b][i]: one block of kFinalThreads per (i, r),
 // threads stride over the block partials, then a fixed shuffle tree
 // (deterministic: the order depends only on nblocks)
 constexpr int kFinalThreads = 128;
 __global__ void __launch_bounds__(kFinalThreads) reduce_partials_kernel(const double2 *__restrict__ partials,
                                                                         int nblocks, int cap, int nv,
-                                                                        double2 *__restrict__ out) {
+                                                                        double2 *__restrict__ out, long sOut) {
     __shared__ double2 sh[kFinalThreads / 32];
-    const int i = blockIdx.x;
+    const int i = blockIdx.x, r = blockIdx.y;
     if (i >= nv) return;
+    partials += (long)r * nblocks * cap;
     double2 s = make_double2(0, 0);
     for (int b = threadIdx.x; b < nblocks; b += kFinalThreads) {
         const double2 p = partials[(long)b * cap + i];
@@ -94,18 +101,23 @@ __global__ void __launch_bounds__(kFinalThreads) reduce_partials_kernel(const do
     if (threadIdx.x == 0) {
         double2 t = sh[0];
         for (int w = 1; w < kFinalThreads / 32; w++) t = cadd(t, sh[w]);
-        out[i] = t;
+        out[r * sOut + i] = t;
     }
 }
 
-// w -= sum_i coef[i] vs[i] V_i ; post: 0 none, 1 ||w_new||^2 partial into partials[b][0]
-__global__ void __launch_bounds__(kRedThreads) update_kernel(const double2 *__restrict__ V, long ldv,
-                                                             const double *__restrict__ vs, int nv,
-                                                             const double2 *__restrict__ coef,
-                                                             double2 *__restrict__ w, long N, int post,
+// w -= sum_i coef[i] vs[i] V_i ; post 1: ||w_new||^2 partial into partials[r][b][0]
+__global__ void __launch_bounds__(kRedThreads) update_kernel(const double2 *__restrict__ V, long ldv, long sV,
+                                                             const double *__restrict__ vs, long sVs, int nv,
+                                                             const double2 *__restrict__ coef, long sCoef,
+                                                             double2 *__restrict__ w, long sW, long N, int post,
                                                              double2 *__restrict__ partials, int cap) {
     extern __shared__ double2 sc[];  // nv coefficients (coef * vs)
     __shared__ double2 sh[(kRedThreads / 32)];
+    const int r = blockIdx.y;
+    V += r * sV;
+    w += r * sW;
+    coef += r * sCoef;
+    if (vs) vs += r * sVs;
     for (int i = threadIdx.x; i < nv; i += blockDim.x) sc[i] = cscale(coef[i], vs ? vs[i] : 1.0);
     __syncthreads();
     double2 nrm[1] = {make_double2(0, 0)};
@@ -118,16 +130,21 @@ __global__ void __launch_bounds__(kRedThreads) update_kernel(const double2 *__re
     }
     if (post == 1) {
         block_sum<1>(nrm, sh);
-        if (threadIdx.x == 0) partials[(long)blockIdx.x * cap] = nrm[0];
+        if (threadIdx.x == 0) partials[(long)r * gridDim.x * cap + (long)blockIdx.x * cap] = nrm[0];
     }
 }
 
 // x += sum_i y[i] zs[i] Z_i
-__global__ void __launch_bounds__(kRedThreads) combine_kernel(const double2 *__restrict__ Z, long ldz,
-                                                              const double *__restrict__ zs, int nzv,
-                                                              const double2 *__restrict__ y, double2 *__restrict__ x,
-                                                              long N) {
+__global__ void __launch_bounds__(kRedThreads) combine_kernel(const double2 *__restrict__ Z, long ldz, long sZ,
+                                                              const double *__restrict__ zs, long sZs, int nzv,
+                                                              const double2 *__restrict__ y, long sY,
+                                                              double2 *__restrict__ x, long sX, long N) {
     extern __shared__ double2 sc[];
+    const int r = blockIdx.y;
+    Z += r * sZ;
+    y += r * sY;
+    x += r * sX;
+    if (zs) zs += r * sZs;
     for (int i = threadIdx.x; i < nzv; i += blockDim.x) sc[i] = cscale(y[i], zs ? zs[i] : 1.0);
     __syncthreads();
     const long stride = (long)gridDim.x * blockDim.x;
@@ -138,10 +155,12 @@ __global__ void __launch_bounds__(kRedThreads) combine_kernel(const double2 *__r
     }
 }
 
-__global__ void __launch_bounds__(kRedThreads) norm2_box_kernel(const double2 *__restrict__ x, int nx, int ny,
+__global__ void __launch_bounds__(kRedThreads) norm2_box_kernel(const double2 *__restrict__ x, long sX, int nx, int ny,
                                                                 int x0, int x1, int y0, int y1, int z0, int z1,
                                                                 double2 *__restrict__ partials, int cap) {
     __shared__ double2 sh[(kRedThreads / 32)];
+    const int r = blockIdx.y;
+    x += r * sX;
     const long bx = x1 - x0, by = y1 - y0, bz = z1 - z0;
     const long total = bx * by * bz;
     double2 acc[1] = {make_double2(0, 0)};
@@ -153,10 +172,14 @@ __global__ void __launch_bounds__(kRedThreads) norm2_box_kernel(const double2 *_
         acc[0].x += v.x * v.x + v.y * v.y;
     }
     block_sum<1>(acc, sh);
-    if (threadIdx.x == 0) partials[(long)blockIdx.x * cap] = acc[0];
+    if (threadIdx.x == 0) partials[(long)r * gridDim.x * cap + (long)blockIdx.x * cap] = acc[0];
 }
 
-__global__ void axpby_kernel(double2 a, const double2 *__restrict__ x, double2 b, double2 *__restrict__ y, long N) {
+__global__ void axpby_kernel(double2 a, const double2 *__restrict__ x, long sX, double2 b, double2 *__restrict__ y,
+                             long sY, long N) {
+    const int r = blockIdx.y;
+    x += r * sX;
+    y += r * sY;
     const long stride = (long)gridDim.x * blockDim.x;
     for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
         const double2 yv = y[l], xv = x[l];
@@ -170,23 +193,20 @@ __global__ void sub_dl_kernel(const double2 *__restrict__ x, const double2 *__re
     for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) y[l] = csub(x[l], cmul(dl[l], t[l]));
 }
 
-__global__ void set_scale_kernel(const double2 *nrm, double *vs, int j) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        const double s = sqrt(nrm[0].x);
-        vs[j] = s > 0 ? 1.0 / s : 0.0;
+// vs[r][j] = 1 / sqrt(nrm[r].x)
+__global__ void set_scale_kernel(const double2 *nrm, long sNrm, double *vs, long sVs, int j, int R) {
+    const int r = threadIdx.x;
+    if (r < R) {
+        const double s = sqrt(nrm[r * sNrm].x);
+        vs[r * sVs + j] = s > 0 ? 1.0 / s : 0.0;
     }
-}
-
-__global__ void add_vec_kernel(const double2 *a, const double2 *b, double2 *out, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = cadd(a[i], b[i]);
 }
 
 __global__ void grad_accum_kernel(const double2 *__restrict__ lam, const double2 *__restrict__ u, double w2,
                                   double beta, double *__restrict__ g, long N) {
     const long stride = (long)gridDim.x * blockDim.x;
     for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
-        // dA/ds2 = w2 (1 + i beta); contribution Re( conj(lam) * dA/ds2 * u )
+        // dA/ds2 = w2 (1 + i beta): contribution Re(conj(lam) (dA/ds2) u)
         const double2 du = cmul(make_double2(w2, w2 * beta), u[l]);
         const double2 lv = lam[l];
         g[l] += lv.x * du.x + lv.y * du.y;
@@ -227,48 +247,53 @@ __global__ void base2d_kernel(const double *__restrict__ s2, int nz, long plane,
 
 static inline bool ok() { return cudaGetLastError() == cudaSuccess; }
 
-static int grid_for(long N) {
+static int grid_for(long N, int R = 1) {
     const long b = (N + kRedThreads - 1) / kRedThreads;
-    const long cap = 4L * device_info().sm_count;
-    return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+    const long cap = (4L * device_info().sm_count + R - 1) / R;
+    return (int)(b < cap ? (b < 1 ? 1 : b) : (cap < 1 ? 1 : cap));
 }
 
-int launch_dots(const double2 *V, long ldv, const double *vs, int nv, const double2 *w, long N, const Reduce &red,
-                double2 *out, cudaStream_t s, bool wnorm) {
-    if (nv + (wnorm ? 1 : 0) > red.cap) return HELM3D_ERR_ARG;
+int launch_dots(const VecBatch &V, long ldv, const ScaleBatch &vs, int nv, const VecBatch &w, long N, int R,
+                const Reduce &red, double2 *out, long sOut, cudaStream_t s, bool wnorm) {
+    const int nout = nv + (wnorm ? 1 : 0);
+    if (nout > red.cap || R > red.rmax) return HELM3D_ERR_ARG;
     const int nb = red.nblocks;
-    dots_kernel<<<nb, kRedThreads, 0, s>>>(V, ldv, vs, nv, w, N, wnorm ? 1 : 0, red.partials, red.cap);
-    reduce_partials_kernel<<<nv + (wnorm ? 1 : 0), kFinalThreads, 0, s>>>(red.partials, nb, red.cap,
-                                                                         nv + (wnorm ? 1 : 0), out);
+    dots_kernel<<<dim3(nb, R), kRedThreads, 0, s>>>(V.p, ldv, V.stride, vs.p, vs.stride, nv, w.p, w.stride, N,
+                                                    wnorm ? 1 : 0, red.partials, red.cap);
+    reduce_partials_kernel<<<dim3(nout, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, nout, out, sOut);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
-int launch_update(const double2 *V, long ldv, const double *vs, int nv, const double2 *coef, double2 *w, long N,
-                  int post, const Reduce &red, double2 *out, cudaStream_t s) {
-    const int nb = post ? red.nblocks : grid_for(N);
-    update_kernel<<<nb, kRedThreads, sizeof(double2) * (nv > 0 ? nv : 1), s>>>(V, ldv, vs, nv, coef, w, N, post,
-                                                                               red.partials, red.cap);
-    if (post == 1) reduce_partials_kernel<<<1, kFinalThreads, 0, s>>>(red.partials, nb, red.cap, 1, out);
+int launch_update(const VecBatch &V, long ldv, const ScaleBatch &vs, int nv, const double2 *coef, long sCoef,
+                  const VecBatch &w, long N, int R, int post, const Reduce &red, double2 *out, long sOut,
+                  cudaStream_t s) {
+    if (R > red.rmax) return HELM3D_ERR_ARG;
+    const int nb = post ? red.nblocks : grid_for(N, R);
+    update_kernel<<<dim3(nb, R), kRedThreads, sizeof(double2) * (nv > 0 ? nv : 1), s>>>(
+        V.p, ldv, V.stride, vs.p, vs.stride, nv, coef, sCoef, w.p, w.stride, N, post, red.partials, red.cap);
+    if (post == 1) reduce_partials_kernel<<<dim3(1, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, 1, out, sOut);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
-int launch_combine(const double2 *Z, long ldz, const double *zs, int nzv, const double2 *y, double2 *x, long N,
-                   cudaStream_t s) {
-    combine_kernel<<<grid_for(N), kRedThreads, sizeof(double2) * (nzv > 0 ? nzv : 1), s>>>(Z, ldz, zs, nzv, y, x, N);
+int launch_combine(const VecBatch &Z, long ldz, const ScaleBatch &zs, int nzv, const double2 *y, long sY,
+                   const VecBatch &x, long N, int R, cudaStream_t s) {
+    combine_kernel<<<dim3(grid_for(N, R), R), kRedThreads, sizeof(double2) * (nzv > 0 ? nzv : 1), s>>>(
+        Z.p, ldz, Z.stride, zs.p, zs.stride, nzv, y, sY, x.p, x.stride, N);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
-int launch_norm2_box(const double2 *x, int nx, int ny, int nz, const int box[6], const Reduce &red, double2 *out,
-                     cudaStream_t s) {
+int launch_norm2_box(const VecBatch &x, int R, int nx, int ny, int nz, const int box[6], const Reduce &red,
+                     double2 *out, long sOut, cudaStream_t s) {
     (void)nz;
-    norm2_box_kernel<<<red.nblocks, kRedThreads, 0, s>>>(x, nx, ny, box[0], box[1], box[2], box[3], box[4], box[5],
-                                                         red.partials, red.cap);
-    reduce_partials_kernel<<<1, kFinalThreads, 0, s>>>(red.partials, red.nblocks, red.cap, 1, out);
+    if (R > red.rmax) return HELM3D_ERR_ARG;
+    norm2_box_kernel<<<dim3(red.nblocks, R), kRedThreads, 0, s>>>(x.p, x.stride, nx, ny, box[0], box[1], box[2],
+                                                                  box[3], box[4], box[5], red.partials, red.cap);
+    reduce_partials_kernel<<<dim3(1, R), kFinalThreads, 0, s>>>(red.partials, red.nblocks, red.cap, 1, out, sOut);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
-int launch_axpby(double2 a, const double2 *x, double2 b, double2 *y, long N, cudaStream_t s) {
-    axpby_kernel<<<grid_for(N), kRedThreads, 0, s>>>(a, x, b, y, N);
+int launch_axpby(double2 a, const VecBatch &x, double2 b, const VecBatch &y, long N, int R, cudaStream_t s) {
+    axpby_kernel<<<dim3(grid_for(N, R), R), kRedThreads, 0, s>>>(a, x.p, x.stride, b, y.p, y.stride, N);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
@@ -277,13 +302,8 @@ int launch_sub_dl(const double2 *x, const double2 *dl, const double2 *t, double2
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
-int launch_set_scale(const double2 *nrm, double *vs, int j, cudaStream_t s) {
-    set_scale_kernel<<<1, 32, 0, s>>>(nrm, vs, j);
-    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
-}
-
-int launch_add_vec(const double2 *a, const double2 *b, double2 *out, int n, cudaStream_t s) {
-    add_vec_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, b, out, n);
+int launch_set_scale(const double2 *nrm, long sNrm, double *vs, long sVs, int j, int R, cudaStream_t s) {
+    set_scale_kernel<<<1, 32 * ((R + 31) / 32), 0, s>>>(nrm, sNrm, vs, sVs, j, R);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
@@ -293,10 +313,6 @@ int launch_base2d(bool c64, const double *s2, int nz, long plane, int zlo, int z
     if (c64) base2d_kernel<float><<<grid, 256, 0, s>>>(s2, nz, plane, zlo, zhi, w2, beta, (float2 *)base2d, status);
     else base2d_kernel<double><<<grid, 256, 0, s>>>(s2, nz, plane, zlo, zhi, w2, beta, (double2 *)base2d, status);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
-}
-
-int launch_zero(void *p, size_t bytes, cudaStream_t s) {
-    return cudaMemsetAsync(p, 0, bytes, s) == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
 int launch_grad_accum(const double2 *lam, const double2 *u, double w2, double beta, double *g, long N,

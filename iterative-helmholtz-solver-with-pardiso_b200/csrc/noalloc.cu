@@ -65,10 +65,11 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
         }
         scratch = g_scratch_addr[c->device];
     }
-    rc = c->zeig ? launch_ztrans_forward(c->c64, (const double2 *)x, 1.0, scratch, c->grid.nz, c->plane, c->d_zWi64,
-                                         c->stream)
-                 : launch_fft_forward(c->c64, (const double2 *)x, 1.0, scratch, c->grid.nz, c->plane, c->plan, c->d_tw,
-                                      c->stream);
+    const VecBatch xb{(double2 *)x, 0}, yb{(double2 *)y, 0};
+    const ScaleBatch one{nullptr, 0};
+    const PlaneLayout L{c->grid.nx, c->grid.ny, c->grid.nz, 1, c->plane};
+    rc = c->zeig ? launch_ztrans_forward(c->c64, xb, 1.0, one, scratch, L, c->d_zWi64, c->stream)
+                 : launch_fft_forward(c->c64, xb, 1.0, one, scratch, L, c->plan, c->d_tw, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: forward FFT launch");
     SweepArgs s;
     s.n = c->grid.nx;
@@ -79,14 +80,13 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
     s.cmy = c->d_cmy;
     s.cpy = c->d_cpy;
     s.planes = scratch;
-    s.nrhs = 1;
-    s.rhs_stride = 0;
+    s.R = 1;
     s.status = c->d_status;
     rc = launch_sweep(c->c64, s, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: sweep launch");
-    rc = c->zeig ? launch_ztrans_inverse(c->c64, scratch, (double2 *)y, c->grid.nz, c->plane, c->d_zW64, c->stream)
-                 : launch_fft_inverse(c->c64, scratch, (double2 *)y, c->grid.nz, c->plane, c->plan, c->d_tw, 0,
-                                      nullptr, 0.0, nullptr, c->stream);
+    rc = c->zeig ? launch_ztrans_inverse(c->c64, scratch, L, yb, c->d_zW64, c->stream)
+                 : launch_fft_inverse(c->c64, scratch, L, yb, c->plan, c->d_tw, 0, VecBatch{nullptr, 0}, 0.0, one,
+                                      nullptr, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: inverse FFT launch");
     c->launches += 3;
     return cuda_check(c, cudaStreamSynchronize(c->stream), "apply_prec_noalloc");

@@ -358,6 +358,7 @@ int ctx_setup_grid(helm3d_ctx *c) {
     if (o.mode == HELM3D_MODE_N && (rc = dalloc(c, (void **)&c->d_s2, sizeof(double) * c->N, "s2"))) return rc;
     if (o.mode == HELM3D_MODE_R && (rc = dalloc(c, (void **)&c->d_dl, sizeof(double2) * c->N, "dL"))) return rc;
     if ((rc = dalloc(c, &c->d_planes, esz * c->N + 256, "planes"))) return rc;
+    c->planes_R = 1;
     if ((rc = dalloc(c, (void **)&c->d_status, 64, "status"))) return rc;
     c->ldg = (nx + 3) & ~3;
     c->Gt_bytes = esz * (size_t)nz * ny * nx * c->ldg;

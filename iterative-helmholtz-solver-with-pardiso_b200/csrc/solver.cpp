@@ -2,15 +2,22 @@
 //
 // FGMRES follows the reference's restarted loop (Source/FGMRES.cpp:464-684)
 // with three stated changes: the Arnoldi coefficients are V_i^H w (correct
-// Gram-Schmidt, applied twice: CGS2) instead of the conjugate the reference
-// computes (:511); the least-squares problem is updated by Givens rotations
-// instead of a fresh zgels every step (:552-570); and the true residual and
-// the preconditioner are applied once per iteration plus once per cycle
-// instead of three times per iteration (:503,579,601).
+// Gram-Schmidt, with a second pass when the first lost more than half of
+// ||w||^2) instead of the conjugate the reference computes (:511); the
+// least-squares problem is updated by Givens rotations instead of a fresh
+// zgels every step (:552-570); and the true residual and the preconditioner
+// are applied once per iteration plus once per cycle instead of three times
+// per iteration (:503,579,601).
 //   mode N: flexible, right preconditioned: z_j = M^{-1} v_j, w = A z_j,
 //           x = x0 + Z y.
 //   mode R: GMRES on K = I - dL L0^{-1} (the preconditioner is inside the
 //           operator), x = x0 + V y, u = L0^{-1} x.
+// Several right-hand sides (the reference's loop over sources,
+// Source/main.cpp) are iterated in lockstep: one operator / preconditioner
+// launch per Arnoldi step serves the whole batch, each right-hand side keeps
+// its own basis, Hessenberg matrix and Givens rotations, and a right-hand
+// side that has converged stops contributing columns (and leaves the batch
+// at the next restart).
 // BiCGStab follows BCGSTAB (Source/BcGSTAB.cpp:397-560): right
 // preconditioned, iterate kept in u-space, shadow residual 2 r0.
 #include <cuda_runtime.h>
@@ -30,36 +37,61 @@ namespace h3d {
         if (_rc) return _rc;           \
     } while (0)
 
+static const ScaleBatch kNoScale{nullptr, 0};
+static VecBatch one(const double2 *p) { return VecBatch{const_cast<double2 *>(p), 0}; }
+
 static Reduce reducer(helm3d_ctx *c) {
     Reduce r;
     r.partials = c->d_partials;
     r.nblocks = c->red_blocks;
     r.cap = c->red_cap;
+    r.rmax = c->r_alloc;
     return r;
 }
 
-int ensure_krylov(helm3d_ctx *c, int m) {
-    if (c->m_alloc >= m && c->d_V) return HELM3D_OK;
-    auto fre = [&](void *p) { if (p) cudaFree(p); };
-    fre(c->d_V);
-    fre(c->d_Z);
-    fre(c->d_vs);
-    fre(c->d_h);
-    fre(c->d_partials);
-    c->d_V = c->d_Z = nullptr;
+// small per-right-hand-side device scalars: h1 | h2 | norms | y, each m+2 long
+static int scalars_per_rhs(int m) { return 4 * (m + 2); }
+
+static void free_krylov(helm3d_ctx *c) {
+    void *bufs[] = {c->d_V, c->d_Z, c->d_vs, c->d_h, c->d_partials, c->d_Fw, c->d_Uw};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+    c->d_V = c->d_Z = c->d_h = c->d_partials = c->d_Fw = c->d_Uw = nullptr;
     c->d_vs = nullptr;
-    c->d_h = nullptr;
-    c->d_partials = nullptr;
+    c->bytes -= c->kry_bytes;
+    c->kry_bytes = 0;
+    c->m_alloc = c->r_alloc = 0;
+}
+
+int ensure_krylov(helm3d_ctx *c, int m, int R) {
+    if (c->d_V && c->m_alloc >= m && c->r_alloc >= R) return HELM3D_OK;
+    m = std::max(m, c->m_alloc);
+    R = std::max(R, c->r_alloc);
+    free_krylov(c);
     const size_t vb = sizeof(double2) * (size_t)c->N;
-    RC(cuda_check(c, cudaMalloc((void **)&c->d_V, vb * (m + 1)), "Krylov basis V"));
-    if (c->opts.mode == HELM3D_MODE_N) RC(cuda_check(c, cudaMalloc((void **)&c->d_Z, vb * m), "Krylov basis Z"));
-    RC(cuda_check(c, cudaMalloc((void **)&c->d_vs, sizeof(double) * (m + 2)), "scales"));
-    RC(cuda_check(c, cudaMalloc((void **)&c->d_h, sizeof(double2) * 4 * (m + 2)), "h"));
+    size_t total = 0;
+    auto get = [&](void **p, size_t bytes, const char *what) {
+        total += bytes;
+        return cuda_check(c, cudaMalloc(p, bytes), what);
+    };
     c->red_cap = std::max(m + 2, 8);
     c->red_blocks = 2 * device_info().sm_count;
-    RC(cuda_check(c, cudaMalloc((void **)&c->d_partials, sizeof(double2) * c->red_cap * c->red_blocks), "partials"));
+    int rc;
+    if ((rc = get((void **)&c->d_V, vb * (m + 1) * R, "Krylov basis V")) ||
+        (c->opts.mode == HELM3D_MODE_N && (rc = get((void **)&c->d_Z, vb * m * R, "Krylov basis Z"))) ||
+        (rc = get((void **)&c->d_vs, sizeof(double) * (m + 2) * R, "basis scales")) ||
+        (rc = get((void **)&c->d_h, sizeof(double2) * scalars_per_rhs(m) * R, "Krylov scalars")) ||
+        (rc = get((void **)&c->d_partials, sizeof(double2) * c->red_cap * c->red_blocks * R, "partials")) ||
+        (rc = get((void **)&c->d_Fw, vb * R, "packed right-hand sides")) ||
+        (rc = get((void **)&c->d_Uw, vb * R, "packed iterates"))) {
+        c->kry_bytes = 0;
+        free_krylov(c);
+        return rc;
+    }
     c->m_alloc = m;
-    c->bytes += vb * (m + 1) + (c->d_Z ? vb * m : 0);
+    c->r_alloc = R;
+    c->kry_bytes = total;
+    c->bytes += total;
     return HELM3D_OK;
 }
 
@@ -70,8 +102,29 @@ static int ensure_vec(helm3d_ctx *c, double2 **p, const char *what) {
     return HELM3D_OK;
 }
 
+// spectral planes for R right-hand sides
+static int ensure_planes(helm3d_ctx *c, int R) {
+    if (c->planes_R >= R && c->d_planes) return HELM3D_OK;
+    const size_t esz = c->c64 ? 8 : 16;
+    if (c->d_planes) {
+        RC(cuda_check(c, cudaStreamSynchronize(c->stream), "planes sync"));
+        cudaFree(c->d_planes);
+        c->bytes -= esz * c->N * c->planes_R + 256;
+        c->d_planes = nullptr;
+        c->planes_R = 0;
+    }
+    RC(cuda_check(c, cudaMalloc(&c->d_planes, esz * c->N * R + 256), "planes"));
+    c->bytes += esz * c->N * R + 256;
+    c->planes_R = R;
+    return HELM3D_OK;
+}
+
 // ---------------------------------------------------------------- operators
-static SweepArgs sweep_args(helm3d_ctx *c) {
+static PlaneLayout layout(helm3d_ctx *c, int R) {
+    return PlaneLayout{c->grid.nx, c->grid.ny, c->grid.nz, R, c->plane};
+}
+
+static SweepArgs sweep_args(helm3d_ctx *c, int R) {
     SweepArgs s;
     s.n = c->grid.nx;
     s.ny = c->grid.ny;
@@ -81,33 +134,41 @@ static SweepArgs sweep_args(helm3d_ctx *c) {
     s.cmy = c->d_cmy;
     s.cpy = c->d_cpy;
     s.planes = c->d_planes;
-    s.nrhs = 1;
-    s.rhs_stride = 0;
+    s.R = R;
     s.status = c->d_status;
     return s;
 }
 
-// planes = FFT_z(xscale * x); per-kz block sweep in place
-static int prec_to_planes(helm3d_ctx *c, const double2 *x, double xscale) {
+static int check_batch(helm3d_ctx *c, int R) {
+    if (R < 1 || R > kMaxBatch) return set_error(c, HELM3D_ERR_ARG, "batch of right-hand sides out of range");
+    return HELM3D_OK;
+}
+
+// planes = Z-transform(xscale sc_r x_r); per-kz block sweep in place
+static int prec_to_planes(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, int R) {
+    RC(check_batch(c, R));
+    RC(ensure_planes(c, R));
+    const PlaneLayout L = layout(c, R);
     RC(timed(c, HELM3D_K_FFT_FWD, 1, [&] {
-        if (c->zeig)
-            return launch_ztrans_forward(c->c64, x, xscale, c->d_planes, c->grid.nz, c->plane, c->d_zWi64, c->stream);
-        return launch_fft_forward(c->c64, x, xscale, c->d_planes, c->grid.nz, c->plane, c->plan, c->d_tw, c->stream);
+        if (c->zeig) return launch_ztrans_forward(c->c64, x, xscale, sc, c->d_planes, L, c->d_zWi64, c->stream);
+        return launch_fft_forward(c->c64, x, xscale, sc, c->d_planes, L, c->plan, c->d_tw, c->stream);
     }));
-    const SweepArgs s = sweep_args(c);
+    const SweepArgs s = sweep_args(c, R);
     return timed(c, HELM3D_K_SWEEP, 1, [&] { return launch_sweep(c->c64, s, c->stream); });
 }
 
-int apply_prec(helm3d_ctx *c, const double2 *x, double xscale, double2 *y) {
-    RC(prec_to_planes(c, x, xscale));
+int apply_prec(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y, int R) {
+    RC(prec_to_planes(c, x, xscale, sc, R));
+    const PlaneLayout L = layout(c, R);
     return timed(c, HELM3D_K_FFT_INV, 1, [&] {
-        if (c->zeig) return launch_ztrans_inverse(c->c64, c->d_planes, y, c->grid.nz, c->plane, c->d_zW64, c->stream);
-        return launch_fft_inverse(c->c64, c->d_planes, y, c->grid.nz, c->plane, c->plan, c->d_tw, 0, nullptr, 0.0,
-                                  nullptr, c->stream);
+        if (c->zeig) return launch_ztrans_inverse(c->c64, c->d_planes, L, y, c->d_zW64, c->stream);
+        return launch_fft_inverse(c->c64, c->d_planes, L, y, c->plan, c->d_tw, 0, VecBatch{nullptr, 0}, 0.0,
+                                  kNoScale, nullptr, c->stream);
     });
 }
 
-static StencilArgs stencil_args(helm3d_ctx *c, const double2 *x, double xscale, double2 *y, const double2 *f) {
+static StencilArgs stencil_args(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc,
+                                const VecBatch &y, const VecBatch &f, int R) {
     StencilArgs a;
     a.nx = c->grid.nx;
     a.ny = c->grid.ny;
@@ -123,42 +184,48 @@ static StencilArgs stencil_args(helm3d_ctx *c, const double2 *x, double xscale, 
     a.beta_phys = c->opts.beta_phys;
     a.x = x;
     a.xscale = xscale;
+    a.sc = sc;
     a.y = y;
     a.f = f;
+    a.R = R;
     return a;
 }
 
-int apply_op(helm3d_ctx *c, const double2 *x, double xscale, double2 *y) {
+int apply_op(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y, int R) {
+    RC(check_batch(c, R));
     if (c->opts.mode == HELM3D_MODE_N) {
-        const StencilArgs a = stencil_args(c, x, xscale, y, nullptr);
+        const StencilArgs a = stencil_args(c, x, xscale, sc, y, VecBatch{nullptr, 0}, R);
         return timed(c, HELM3D_K_STENCIL, 1, [&] { return launch_stencil(a, false, c->stream); });
     }
-    // mode R: y = xscale*x - dL * L0^{-1}(xscale*x), dL fused into the inverse FFT
-    RC(prec_to_planes(c, x, xscale));
+    // mode R: y = s x - dL * L0^{-1}(s x), dL fused into the inverse FFT
+    RC(prec_to_planes(c, x, xscale, sc, R));
+    const PlaneLayout L = layout(c, R);
     return timed(c, HELM3D_K_FFT_INV, 1, [&] {
-        return launch_fft_inverse(c->c64, c->d_planes, y, c->grid.nz, c->plane, c->plan, c->d_tw, 1, x, xscale,
-                                  c->d_dl, c->stream);
+        return launch_fft_inverse(c->c64, c->d_planes, L, y, c->plan, c->d_tw, 1, x, xscale, sc, c->d_dl,
+                                  c->stream);
     });
 }
 
-int apply_op_adjoint(helm3d_ctx *c, const double2 *x, double xscale, double2 *y) {
+int apply_op_adjoint(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y,
+                     int R) {
+    RC(check_batch(c, R));
     if (c->opts.mode != HELM3D_MODE_N) return set_error(c, HELM3D_ERR_ARG, "adjoint operator is mode N only");
-    const StencilArgs a = stencil_args(c, x, xscale, y, nullptr);
+    const StencilArgs a = stencil_args(c, x, xscale, sc, y, VecBatch{nullptr, 0}, R);
     return timed(c, HELM3D_K_STENCIL, 1, [&] { return launch_stencil(a, true, c->stream); });
 }
 
-static int axpby(helm3d_ctx *c, double2 a, const double2 *x, double2 b, double2 *y) {
-    return timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_axpby(a, x, b, y, c->N, c->stream); });
+static int axpby(helm3d_ctx *c, double2 a, const VecBatch &x, double2 b, const VecBatch &y, int R) {
+    return timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_axpby(a, x, b, y, c->N, R, c->stream); });
 }
 
-// r = f - A x
-static int residual(helm3d_ctx *c, const double2 *f, const double2 *x, double2 *r, bool adjoint) {
+// r_r = f_r - A x_r
+static int residual(helm3d_ctx *c, const VecBatch &f, const VecBatch &x, const VecBatch &r, int R, bool adjoint) {
     if (c->opts.mode == HELM3D_MODE_N) {
-        const StencilArgs a = stencil_args(c, x, 1.0, r, f);
+        const StencilArgs a = stencil_args(c, x, 1.0, kNoScale, r, f, R);
         return timed(c, HELM3D_K_STENCIL, 1, [&] { return launch_stencil(a, adjoint, c->stream); });
     }
-    RC(apply_op(c, x, 1.0, r));
-    return axpby(c, make_double2(1, 0), f, make_double2(-1, 0), r);
+    RC(apply_op(c, x, 1.0, kNoScale, r, R));
+    return axpby(c, make_double2(1, 0), f, make_double2(-1, 0), r, R);
 }
 
 // small pinned host mirror of device scalars
@@ -168,19 +235,21 @@ struct Pinned {
     ~Pinned() { if (h) cudaFreeHost(h); }
 };
 
-static int norm2(helm3d_ctx *c, const double2 *x, const int *box, double2 *d_out, double *host_out) {
-    int full[6] = {0, c->grid.nx, 0, c->grid.ny, 0, c->grid.nz};
-    const Reduce red = reducer(c);
-    RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
-        return launch_norm2_box(x, c->grid.nx, c->grid.ny, c->grid.nz, box ? box : full, red, d_out, c->stream);
-    }));
-    double2 v;
-    RC(cuda_check(c, cudaMemcpyAsync(&v, d_out, sizeof(double2), cudaMemcpyDeviceToHost, c->stream), "norm"));
-    RC(cuda_check(c, cudaStreamSynchronize(c->stream), "norm sync"));
-    *host_out = v.x;
-    return HELM3D_OK;
+static int fetch(helm3d_ctx *c, const double2 *d, size_t n, double2 *h, const char *what) {
+    RC(cuda_check(c, cudaMemcpyAsync(h, d, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->stream), what));
+    return cuda_check(c, cudaStreamSynchronize(c->stream), what);
 }
 
+static void full_box(helm3d_ctx *c, int box[6]) {
+    box[0] = 0;
+    box[1] = c->grid.nx;
+    box[2] = 0;
+    box[3] = c->grid.ny;
+    box[4] = 0;
+    box[5] = c->grid.nz;
+}
+
+// the physical domain: the grid without its PML (and mode R's sponge) layers
 static void phys_box(helm3d_ctx *c, int box[6]) {
     const helm3d_grid &g = c->grid;
     const int zl = std::max(g.spg_z, g.pml_z);
@@ -192,6 +261,22 @@ static void phys_box(helm3d_ctx *c, int box[6]) {
     box[5] = g.nz - zl;
 }
 
+// ||x_r||^2 into out[r * sOut].x (full grid) and, with phys, out[r * sOut + 1].x
+// (physical domain); no host synchronization
+static int norms(helm3d_ctx *c, const VecBatch &x, int R, bool phys, double2 *out, long sOut) {
+    const Reduce red = reducer(c);
+    int box[6];
+    full_box(c, box);
+    RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+        return launch_norm2_box(x, R, c->grid.nx, c->grid.ny, c->grid.nz, box, red, out, sOut, c->stream);
+    }));
+    if (!phys) return HELM3D_OK;
+    phys_box(c, box);
+    return timed(c, HELM3D_K_KRYLOV, 2, [&] {
+        return launch_norm2_box(x, R, c->grid.nx, c->grid.ny, c->grid.nz, box, red, out + 1, sOut, c->stream);
+    });
+}
+
 static int check_status(helm3d_ctx *c) {
     int st = 0;
     RC(cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status"));
@@ -200,196 +285,288 @@ static int check_status(helm3d_ctx *c) {
     return HELM3D_OK;
 }
 
+// complex Givens rotation zeroing b in (a, b)
+static void givens(zc a, zc b, zc &cs, zc &sn) {
+    const double den = std::hypot(std::abs(a), std::abs(b));
+    if (den == 0.0) {
+        cs = 1.0;
+        sn = 0.0;
+    } else if (std::abs(a) == 0.0) {
+        cs = 0.0;
+        sn = 1.0;
+    } else {
+        cs = std::abs(a) / den;
+        sn = (a / std::abs(a)) * std::conj(b) / den;
+    }
+}
+
 // --------------------------------------------------------------- FGMRES
-int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, bool adjoint, helm3d_stats *st) {
+namespace {
+// host state of one right-hand side of the batch
+struct Rhs {
+    int orig = 0;             // position in the caller's f/u
+    double nf = 0;            // ||f||
+    int it = 0, restarts = 0;
+    double relres = 1, relres_phys = 1;
+    int status = HELM3D_OK;
+    bool done = false;
+    bool frozen = false;      // converged inside the current cycle: no more columns
+    int k = 0;                // columns of the current cycle
+    double beta = 0;
+    std::vector<zc> H, cs, sn, gv;
+};
+}  // namespace
+
+int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, helm3d_stats *st) {
     const helm3d_opts &o = c->opts;
     const bool flexible = (o.mode == HELM3D_MODE_N);
     if (adjoint && !flexible) return set_error(c, HELM3D_ERR_ARG, "adjoint solve is mode N only");
+    RC(check_batch(c, R));
     const int m = std::max(1, o.restart);
-    RC(ensure_krylov(c, m));
-    RC(ensure_vec(c, &c->d_r, "residual"));
+    RC(ensure_krylov(c, m, R));
     const long N = c->N;
     const size_t vb = sizeof(double2) * (size_t)N;
-    double2 *V = c->d_V, *Z = c->d_Z;
-    double2 *d_h1 = c->d_h, *d_h2 = c->d_h + (m + 2), *d_nrm = c->d_h + 2 * (m + 2), *d_y = c->d_h + 3 * (m + 2);
-    Pinned hb(3 * (m + 2));
+    const long ldV = (long)(m + 1) * N, ldZ = (long)m * N;   // per right-hand side basis strides
+    const int M2 = m + 2, SH = scalars_per_rhs(m);
+    double2 *V = c->d_V, *Z = c->d_Z, *Fw = c->d_Fw, *Uw = c->d_Uw, *Hd = c->d_h;
+    double2 *d_h1 = Hd, *d_h2 = Hd + M2, *d_nrm = Hd + 2 * M2, *d_y = Hd + 3 * M2;
+    Pinned hb((size_t)SH * R);
     if (!hb.h) return set_error(c, HELM3D_ERR_OOM, "pinned host buffer");
+    const Reduce red = reducer(c);
+    const double tol = o.tol;
 
     cudaEventRecord(c->ev0, c->stream);
-    double nf2;
-    RC(norm2(c, f, nullptr, d_nrm, &nf2));
-    const double nf = std::sqrt(nf2);
-    if (!std::isfinite(nf)) return set_error(c, HELM3D_ERR_NONFINITE, "right-hand side has NaN/Inf");
-    RC(cuda_check(c, cudaMemsetAsync(u, 0, vb, c->stream), "x0"));
-    if (st) st->history_len = 0;
-    if (nf == 0.0) {
-        if (st) {
-            st->iterations = 0;
-            st->relres = 0;
-            st->relres_phys = 0;
-        }
-        return HELM3D_OK;
+    RC(cuda_check(c, cudaMemcpyAsync(Fw, f, vb * R, cudaMemcpyDeviceToDevice, c->stream), "f copy"));
+    RC(cuda_check(c, cudaMemsetAsync(Uw, 0, vb * R, c->stream), "x0"));
+    RC(cuda_check(c, cudaMemsetAsync(u, 0, vb * R, c->stream), "u0"));
+    RC(norms(c, VecBatch{Fw, N}, R, false, d_nrm, SH));
+    RC(fetch(c, Hd, (size_t)SH * R, hb.h, "norms of f"));
+    std::vector<Rhs> S(R);
+    std::vector<int> act;   // packed position p -> right-hand side
+    for (int r = 0; r < R; r++) {
+        Rhs &q = S[r];
+        q.orig = r;
+        q.nf = std::sqrt(hb.h[(size_t)r * SH + 2 * M2].x);
+        if (!std::isfinite(q.nf)) return set_error(c, HELM3D_ERR_NONFINITE, "right-hand side has NaN/Inf");
+        q.H.assign((size_t)(m + 1) * m, zc(0, 0));
+        q.cs.assign(m, zc(0, 0));
+        q.sn.assign(m, zc(0, 0));
+        q.gv.assign(m + 1, zc(0, 0));
+        act.push_back(r);
     }
-    const double tol = o.tol;
-    int it = 0, restarts = 0;
-    bool x_zero = true;
-    std::vector<zc> H((size_t)(m + 1) * m), cs(m), sn(m), gv(m + 1);
-    std::vector<double> vs_h(m + 2);
-    int status = HELM3D_OK;
-    double relres = 1.0;
-    while (true) {
-        // r0 = f - A x0 into V_0
-        if (x_zero) {
-            RC(cuda_check(c, cudaMemcpyAsync(V, f, vb, cudaMemcpyDeviceToDevice, c->stream), "r0"));
-        } else {
-            RC(residual(c, f, u, V, adjoint));
+    if (st) st->history_len = 0;
+
+    // Drop the finished right-hand sides from the packed batch: their iterate
+    // goes to u, the rest move down (iterate, right-hand side, and V_0 when
+    // it holds the current residual).
+    auto retire = [&](bool move_v0) -> int {
+        size_t q = 0;
+        for (size_t p = 0; p < act.size(); p++) {
+            Rhs &r = S[act[p]];
+            if (r.done) {
+                RC(cuda_check(c, cudaMemcpyAsync(u + (size_t)r.orig * N, Uw + p * N, vb, cudaMemcpyDeviceToDevice,
+                                                 c->stream),
+                              "retire"));
+                continue;
+            }
+            if (q != p) {
+                RC(cuda_check(c, cudaMemcpyAsync(Fw + q * N, Fw + p * N, vb, cudaMemcpyDeviceToDevice, c->stream),
+                              "pack f"));
+                RC(cuda_check(c, cudaMemcpyAsync(Uw + q * N, Uw + p * N, vb, cudaMemcpyDeviceToDevice, c->stream),
+                              "pack u"));
+                if (move_v0)
+                    RC(cuda_check(c, cudaMemcpyAsync(V + q * ldV, V + p * ldV, vb, cudaMemcpyDeviceToDevice,
+                                                     c->stream),
+                                  "pack v0"));
+            }
+            act[q++] = act[p];
         }
-        double beta2;
-        RC(norm2(c, V, nullptr, d_nrm, &beta2));
-        const double beta = std::sqrt(beta2);
-        relres = beta / nf;
-        if (!std::isfinite(beta)) return set_error(c, HELM3D_ERR_NONFINITE, "residual is NaN/Inf");
-        if (relres <= tol || it >= o.max_iter) break;
-        vs_h[0] = 1.0 / beta;
-        RC(cuda_check(c, cudaMemcpyAsync(c->d_vs, vs_h.data(), sizeof(double), cudaMemcpyHostToDevice, c->stream),
+        act.resize(q);
+        return HELM3D_OK;
+    };
+    for (int r : act)
+        if (S[r].nf == 0.0) {
+            S[r].done = true;
+            S[r].relres = S[r].relres_phys = 0;
+        }
+    RC(retire(false));
+
+    bool x_zero = true;
+    std::vector<double> vs0(R);
+    std::vector<double2> ybuf((size_t)M2 * R);
+    while (!act.empty()) {
+        const int A = (int)act.size();
+        // r0 = f - A x0 into V_0 of every active right-hand side, with its norms
+        const VecBatch V0{V, ldV};
+        if (x_zero) {
+            RC(cuda_check(c, cudaMemcpy2DAsync(V, sizeof(double2) * ldV, Fw, vb, vb, A, cudaMemcpyDeviceToDevice,
+                                               c->stream),
+                          "r0"));
+        } else {
+            RC(residual(c, VecBatch{Fw, N}, VecBatch{Uw, N}, V0, A, adjoint));
+        }
+        RC(norms(c, V0, A, true, d_nrm, SH));
+        RC(fetch(c, Hd, (size_t)SH * A, hb.h, "residual norms"));
+        bool any_done = false;
+        for (int p = 0; p < A; p++) {
+            Rhs &r = S[act[p]];
+            const double b2 = hb.h[(size_t)p * SH + 2 * M2].x, p2 = hb.h[(size_t)p * SH + 2 * M2 + 1].x;
+            r.beta = std::sqrt(b2);
+            if (!std::isfinite(r.beta)) return set_error(c, HELM3D_ERR_NONFINITE, "residual is NaN/Inf");
+            r.relres = r.beta / r.nf;
+            r.relres_phys = std::sqrt(p2) / r.nf;   // relative to ||f|| as the reference (:591-592)
+            if (r.relres <= tol || r.it >= o.max_iter) {
+                r.done = true;
+                r.status = (r.relres <= tol || o.max_iter == 0) ? HELM3D_OK : HELM3D_ERR_NOT_CONVERGED;
+                any_done = true;
+            }
+        }
+        if (any_done) RC(retire(true));
+        if (act.empty()) break;
+        const int B = (int)act.size();
+        for (int p = 0; p < B; p++) {
+            Rhs &r = S[act[p]];
+            vs0[p] = 1.0 / r.beta;
+            std::fill(r.H.begin(), r.H.end(), zc(0, 0));
+            std::fill(r.gv.begin(), r.gv.end(), zc(0, 0));
+            r.gv[0] = r.beta;
+            r.frozen = false;
+            r.k = 0;
+        }
+        RC(cuda_check(c, cudaMemcpy2DAsync(c->d_vs, sizeof(double) * M2, vs0.data(), sizeof(double), sizeof(double), B,
+                                           cudaMemcpyHostToDevice, c->stream),
                       "vs0"));
-        std::fill(H.begin(), H.end(), zc(0, 0));
-        std::fill(gv.begin(), gv.end(), zc(0, 0));
-        gv[0] = beta;
-        int k = 0;
+        const VecBatch Vall{V, ldV};
+        const ScaleBatch vsb{c->d_vs, M2};
         for (int j = 0; j < m; j++) {
-            double2 *w = V + (size_t)(j + 1) * N;
+            const VecBatch Vj{V + (size_t)j * N, ldV}, w{V + (size_t)(j + 1) * N, ldV};
+            const ScaleBatch vsj{c->d_vs + j, M2};
             if (flexible) {
-                double2 *z = Z + (size_t)j * N;
-                if (adjoint) {
-                    // M^H is not yet available: M^{-1} serves as the
-                    // (flexible) preconditioner of the adjoint system
-                    RC(apply_prec(c, V + (size_t)j * N, vs_h[j], z));
-                    RC(apply_op_adjoint(c, z, 1.0, w));
-                } else {
-                    RC(apply_prec(c, V + (size_t)j * N, vs_h[j], z));
-                    RC(apply_op(c, z, 1.0, w));
-                }
+                const VecBatch zj{Z + (size_t)j * N, ldZ};
+                // the adjoint system is preconditioned by M^{-1} as well
+                // (flexible FGMRES admits any preconditioner)
+                RC(apply_prec(c, Vj, 1.0, vsj, zj, B));
+                if (adjoint) RC(apply_op_adjoint(c, zj, 1.0, kNoScale, w, B));
+                else RC(apply_op(c, zj, 1.0, kNoScale, w, B));
             } else {
-                RC(apply_op(c, V + (size_t)j * N, vs_h[j], w));
+                RC(apply_op(c, Vj, 1.0, vsj, w, B));
             }
             // Classical Gram-Schmidt, repeated only when needed ("twice is
             // enough"): h1 = V^H w with ||w||^2 from the same pass, w -= V h1
-            // with ||w||^2 after; a second pass runs when the norm dropped
-            // below 1/sqrt(2) of its value.
-            const Reduce red = reducer(c);
+            // with ||w||^2 after; a second pass runs when the norm of some
+            // right-hand side dropped below 1/sqrt(2) of its value.
             RC(timed(c, HELM3D_K_KRYLOV, 2,
-                     [&] { return launch_dots(V, N, c->d_vs, j + 1, w, N, red, d_h1, c->stream, true); }));
+                     [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h1, SH, c->stream, true); }));
             RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
-                return launch_update(V, N, c->d_vs, j + 1, d_h1, w, N, 1, red, d_nrm, c->stream);
+                return launch_update(Vall, N, vsb, j + 1, d_h1, SH, w, N, B, 1, red, d_nrm, SH, c->stream);
             }));
-            RC(cuda_check(c, cudaMemcpyAsync(hb.h, d_h1, sizeof(double2) * 3 * (m + 2), cudaMemcpyDeviceToHost,
-                                             c->stream),
-                          "h"));
-            RC(cuda_check(c, cudaStreamSynchronize(c->stream), "h sync"));
-            for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = zc(hb.h[i].x, hb.h[i].y);
-            if (hb.h[2 * (m + 2)].x < 0.5 * hb.h[j + 1].x) {
+            RC(fetch(c, Hd, (size_t)SH * B, hb.h, "Arnoldi coefficients"));
+            bool again = false;
+            for (int p = 0; p < B; p++) {
+                const Rhs &r = S[act[p]];
+                const double2 *h = hb.h + (size_t)p * SH;
+                if (!r.frozen && h[2 * M2].x < 0.5 * h[j + 1].x) again = true;
+            }
+            for (int p = 0; p < B; p++) {
+                Rhs &r = S[act[p]];
+                const double2 *h = hb.h + (size_t)p * SH;
+                for (int i = 0; i <= j; i++) r.H[(size_t)i * m + j] = zc(h[i].x, h[i].y);
+            }
+            if (again) {
                 RC(timed(c, HELM3D_K_KRYLOV, 2,
-                         [&] { return launch_dots(V, N, c->d_vs, j + 1, w, N, red, d_h2, c->stream); }));
+                         [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h2, SH, c->stream); }));
                 RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
-                    return launch_update(V, N, c->d_vs, j + 1, d_h2, w, N, 1, red, d_nrm, c->stream);
+                    return launch_update(Vall, N, vsb, j + 1, d_h2, SH, w, N, B, 1, red, d_nrm, SH, c->stream);
                 }));
-                RC(cuda_check(c, cudaMemcpyAsync(hb.h + (m + 2), d_h2, sizeof(double2) * 2 * (m + 2),
-                                                 cudaMemcpyDeviceToHost, c->stream),
-                              "h2"));
-                RC(cuda_check(c, cudaStreamSynchronize(c->stream), "h2 sync"));
-                for (int i = 0; i <= j; i++) H[(size_t)i * m + j] += zc(hb.h[(m + 2) + i].x, hb.h[(m + 2) + i].y);
+                RC(fetch(c, Hd, (size_t)SH * B, hb.h, "Arnoldi second pass"));
+                for (int p = 0; p < B; p++) {
+                    Rhs &r = S[act[p]];
+                    const double2 *h = hb.h + (size_t)p * SH + M2;
+                    for (int i = 0; i <= j; i++) r.H[(size_t)i * m + j] += zc(h[i].x, h[i].y);
+                }
                 c->reorth++;
             }
-            const double hn = std::sqrt(std::max(0.0, hb.h[2 * (m + 2)].x));
-            if (!std::isfinite(hn)) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
-            H[(size_t)(j + 1) * m + j] = hn;
-            // Givens
-            for (int i = 0; i < j; i++) {
-                const zc a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
-                H[(size_t)i * m + j] = cs[i] * a + sn[i] * b;
-                H[(size_t)(i + 1) * m + j] = -std::conj(sn[i]) * a + cs[i] * b;
-            }
-            {
-                const zc a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
-                const double den = std::hypot(std::abs(a), std::abs(b));
-                if (den == 0.0) {
-                    cs[j] = 1.0;
-                    sn[j] = 0.0;
-                } else if (std::abs(a) == 0.0) {
-                    cs[j] = 0.0;
-                    sn[j] = 1.0;
-                } else {
-                    cs[j] = std::abs(a) / den;
-                    sn[j] = (a / std::abs(a)) * std::conj(b) / den;
+            double est_max = 0;
+            bool all_frozen = true;
+            for (int p = 0; p < B; p++) {
+                Rhs &r = S[act[p]];
+                if (r.frozen) continue;
+                const double hn = std::sqrt(std::max(0.0, hb.h[(size_t)p * SH + 2 * M2].x));
+                if (!std::isfinite(hn)) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
+                std::vector<zc> &H = r.H;
+                H[(size_t)(j + 1) * m + j] = hn;
+                for (int i = 0; i < j; i++) {
+                    const zc a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
+                    H[(size_t)i * m + j] = r.cs[i] * a + r.sn[i] * b;
+                    H[(size_t)(i + 1) * m + j] = -std::conj(r.sn[i]) * a + r.cs[i] * b;
                 }
-                H[(size_t)j * m + j] = cs[j] * a + sn[j] * b;
+                const zc a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
+                givens(a, b, r.cs[j], r.sn[j]);
+                H[(size_t)j * m + j] = r.cs[j] * a + r.sn[j] * b;
                 H[(size_t)(j + 1) * m + j] = 0.0;
-                gv[j + 1] = -std::conj(sn[j]) * gv[j];
-                gv[j] = cs[j] * gv[j];
+                r.gv[j + 1] = -std::conj(r.sn[j]) * r.gv[j];
+                r.gv[j] = r.cs[j] * r.gv[j];
+                r.it++;
+                r.k = j + 1;
+                const double est = std::abs(r.gv[j + 1]) / r.nf;
+                est_max = std::max(est_max, est);
+                if (hn == 0.0 || est <= tol || r.it >= o.max_iter) r.frozen = true;
+                else all_frozen = false;
             }
-            it++;
-            k = j + 1;
-            const double est = std::abs(gv[j + 1]) / nf;
-            if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = est;
-            if (o.verbose) fprintf(stderr, "helm3d: it %d  est relres %.3e\n", it, est);
-            if (hn == 0.0 || est <= tol || it >= o.max_iter) break;
-            vs_h[j + 1] = 1.0 / hn;
-            RC(timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_set_scale(d_nrm, c->d_vs, j + 1, c->stream); }));
+            if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = est_max;
+            if (o.verbose) fprintf(stderr, "helm3d: step %d  max est relres %.3e over %d rhs\n", j + 1, est_max, B);
+            if (all_frozen) break;
+            RC(timed(c, HELM3D_K_KRYLOV, 1,
+                     [&] { return launch_set_scale(d_nrm, SH, c->d_vs, M2, j + 1, B, c->stream); }));
         }
-        // y = H^{-1} g (upper triangular k x k), x += basis * y
-        std::vector<zc> y(k);
-        for (int i = k - 1; i >= 0; i--) {
-            zc s = gv[i];
-            for (int q = i + 1; q < k; q++) s -= H[(size_t)i * m + q] * y[q];
-            y[i] = s / H[(size_t)i * m + i];
+        // y = H^{-1} g (upper triangular k x k) per right-hand side, zero
+        // padded to the longest; x += basis * y
+        int kmax = 0;
+        for (int p = 0; p < B; p++) kmax = std::max(kmax, S[act[p]].k);
+        for (int p = 0; p < B; p++) {
+            const Rhs &r = S[act[p]];
+            double2 *y = ybuf.data() + (size_t)p * M2;
+            std::vector<zc> yz(r.k);
+            for (int i = r.k - 1; i >= 0; i--) {
+                zc s = r.gv[i];
+                for (int q = i + 1; q < r.k; q++) s -= r.H[(size_t)i * m + q] * yz[q];
+                yz[i] = s / r.H[(size_t)i * m + i];
+            }
+            for (int i = 0; i < kmax; i++) y[i] = i < r.k ? make_double2(yz[i].real(), yz[i].imag()) : make_double2(0, 0);
         }
-        RC(cuda_check(c, cudaMemcpyAsync(d_y, y.data(), sizeof(double2) * k, cudaMemcpyHostToDevice, c->stream),
-                      "y"));
-        RC(timed(c, HELM3D_K_KRYLOV, 1, [&] {
-            return flexible ? launch_combine(Z, N, nullptr, k, d_y, u, N, c->stream)
-                            : launch_combine(V, N, c->d_vs, k, d_y, u, N, c->stream);
-        }));
-        RC(cuda_check(c, cudaStreamSynchronize(c->stream), "combine"));
+        if (kmax > 0) {
+            RC(cuda_check(c, cudaMemcpy2DAsync(d_y, sizeof(double2) * SH, ybuf.data(), sizeof(double2) * M2,
+                                               sizeof(double2) * kmax, B, cudaMemcpyHostToDevice, c->stream),
+                          "y"));
+            RC(timed(c, HELM3D_K_KRYLOV, 1, [&] {
+                return flexible ? launch_combine(VecBatch{Z, ldZ}, N, kNoScale, kmax, d_y, SH, VecBatch{Uw, N}, N, B,
+                                                 c->stream)
+                                : launch_combine(Vall, N, vsb, kmax, d_y, SH, VecBatch{Uw, N}, N, B, c->stream);
+            }));
+        }
         x_zero = false;
-        restarts++;
-        if (it >= o.max_iter) {
-            RC(residual(c, f, u, c->d_r, adjoint));
-            double r2;
-            RC(norm2(c, c->d_r, nullptr, d_nrm, &r2));
-            relres = std::sqrt(r2) / nf;
-            if (relres > tol) status = HELM3D_ERR_NOT_CONVERGED;
-            break;
-        }
+        for (int p = 0; p < B; p++) S[act[p]].restarts++;
     }
-    // true residual (full and physical domain)
-    RC(residual(c, f, u, c->d_r, adjoint));
-    double r2, rp2, fp2;
-    RC(norm2(c, c->d_r, nullptr, d_nrm, &r2));
-    int box[6];
-    phys_box(c, box);
-    RC(norm2(c, c->d_r, box, d_nrm, &rp2));
-    RC(norm2(c, f, box, d_nrm, &fp2));
-    relres = std::sqrt(r2) / nf;
     if (!flexible) {
-        // u = L0^{-1} w
-        RC(ensure_vec(c, &c->d_t, "tmp"));
-        RC(cuda_check(c, cudaMemcpyAsync(c->d_t, u, vb, cudaMemcpyDeviceToDevice, c->stream), "w copy"));
-        RC(apply_prec(c, c->d_t, 1.0, u));
+        // u = L0^{-1} w for every right-hand side (in place: the forward
+        // transform reads all of u before the inverse writes it)
+        RC(apply_prec(c, VecBatch{u, N}, 1.0, kNoScale, VecBatch{u, N}, R));
     }
     cudaEventRecord(c->ev1, c->stream);
     RC(check_status(c));
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    if (st) {
-        st->iterations += it;
-        st->restarts += restarts;
-        st->relres = relres;
-        st->relres_phys = std::sqrt(rp2) / nf;   // relative to ||f|| as the reference (:591-592)
-        st->ms_solve += ms;
-        (void)fp2;
+    int status = HELM3D_OK;
+    for (const Rhs &r : S) {
+        if (r.status) status = r.status;
+        if (st) {
+            st->iterations += r.it;
+            st->restarts += r.restarts;
+            st->relres = std::max(st->relres, r.relres);
+            st->relres_phys = std::max(st->relres_phys, r.relres_phys);
+        }
     }
-    if (status == HELM3D_OK && relres > tol && o.max_iter > 0 && it >= o.max_iter) status = HELM3D_ERR_NOT_CONVERGED;
+    if (st) st->ms_solve += ms;
     return status;
 }
 
@@ -397,17 +574,31 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, bool adjoint, helm3d_sta
 // dot <a, b> = sum conj(a) b on the device, returned to the host
 static int zdot(helm3d_ctx *c, const double2 *a, const double2 *b, zc *out) {
     const Reduce red = reducer(c);
-    RC(timed(c, HELM3D_K_KRYLOV, 2, [&] { return launch_dots(a, c->N, nullptr, 1, b, c->N, red, c->d_h, c->stream); }));
+    RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+        return launch_dots(one(a), c->N, kNoScale, 1, one(b), c->N, 1, red, c->d_h, 0, c->stream);
+    }));
     double2 v;
-    RC(cuda_check(c, cudaMemcpyAsync(&v, c->d_h, sizeof(double2), cudaMemcpyDeviceToHost, c->stream), "dot"));
-    RC(cuda_check(c, cudaStreamSynchronize(c->stream), "dot sync"));
+    RC(fetch(c, c->d_h, 1, &v, "dot"));
     *out = zc(v.x, v.y);
     return HELM3D_OK;
 }
 
+static int norm2_one(helm3d_ctx *c, const double2 *x, bool phys, double *full, double *ph) {
+    RC(norms(c, one(x), 1, phys, c->d_h + 1, 0));
+    double2 v[2];
+    RC(fetch(c, c->d_h + 1, phys ? 2 : 1, v, "norm"));
+    *full = v[0].x;
+    if (ph) *ph = v[1].x;
+    return HELM3D_OK;
+}
+
+static int axpby1(helm3d_ctx *c, double2 a, const double2 *x, double2 b, double2 *y) {
+    return axpby(c, a, one(x), b, one(y), 1);
+}
+
 int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st) {
     const helm3d_opts &o = c->opts;
-    RC(ensure_krylov(c, std::max(1, o.restart)));
+    RC(ensure_krylov(c, 1, 1));
     const long N = c->N;
     const size_t vb = sizeof(double2) * (size_t)N;
     if (!c->d_bic) {
@@ -418,7 +609,7 @@ int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st) {
             *zv = Az + N;
     cudaEventRecord(c->ev0, c->stream);
     double nf2;
-    RC(norm2(c, f, nullptr, c->d_h + 1, &nf2));
+    RC(norm2_one(c, f, false, &nf2, nullptr));
     const double nf = std::sqrt(nf2);
     if (!std::isfinite(nf)) return set_error(c, HELM3D_ERR_NONFINITE, "right-hand side has NaN/Inf");
     RC(cuda_check(c, cudaMemsetAsync(u, 0, vb, c->stream), "x0"));
@@ -427,15 +618,15 @@ int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st) {
     RC(cuda_check(c, cudaMemcpyAsync(r, f, vb, cudaMemcpyDeviceToDevice, c->stream), "r0"));
     RC(cuda_check(c, cudaMemcpyAsync(p, f, vb, cudaMemcpyDeviceToDevice, c->stream), "p0"));
     RC(cuda_check(c, cudaMemsetAsync(rst, 0, vb, c->stream), "rst"));
-    RC(axpby(c, make_double2(2, 0), f, make_double2(0, 0), rst));
+    RC(axpby1(c, make_double2(2, 0), f, make_double2(0, 0), rst));
     int it = 0, status = HELM3D_OK;
     double relres = 1.0;
     const bool modeN = o.mode == HELM3D_MODE_N;
     // right preconditioned operator B = A M^{-1} (mode N) or K (mode R);
     // the u-space update uses M^{-1} p (mode N) or L0^{-1} p (mode R)
     auto opB = [&](const double2 *x, double2 *yout, double2 *pre) -> int {
-        RC(apply_prec(c, x, 1.0, pre));
-        if (modeN) return apply_op(c, pre, 1.0, yout);
+        RC(apply_prec(c, one(x), 1.0, kNoScale, one(pre), 1));
+        if (modeN) return apply_op(c, one(pre), 1.0, kNoScale, one(yout), 1);
         return timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_sub_dl(x, c->d_dl, pre, yout, N, c->stream); });
     };
     for (it = 0; it < o.max_iter;) {
@@ -447,7 +638,7 @@ int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st) {
         const zc alpha = rr / ra;
         // s = r - alpha Ay
         RC(cuda_check(c, cudaMemcpyAsync(s, r, vb, cudaMemcpyDeviceToDevice, c->stream), "s"));
-        RC(axpby(c, make_double2(-alpha.real(), -alpha.imag()), Ay, make_double2(1, 0), s));
+        RC(axpby1(c, make_double2(-alpha.real(), -alpha.imag()), Ay, make_double2(1, 0), s));
         RC(opB(s, Az, zv));
         zc as, aa;
         RC(zdot(c, Az, s, &as));
@@ -455,23 +646,23 @@ int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st) {
         if (aa == zc(0, 0)) { status = HELM3D_ERR_BREAKDOWN; break; }
         const zc om = as / aa;
         // x += alpha y + omega z
-        RC(axpby(c, make_double2(alpha.real(), alpha.imag()), yv, make_double2(1, 0), u));
-        RC(axpby(c, make_double2(om.real(), om.imag()), zv, make_double2(1, 0), u));
+        RC(axpby1(c, make_double2(alpha.real(), alpha.imag()), yv, make_double2(1, 0), u));
+        RC(axpby1(c, make_double2(om.real(), om.imag()), zv, make_double2(1, 0), u));
         // r_new = s - omega Az (into r)
         zc rr_old = rr;
         RC(cuda_check(c, cudaMemcpyAsync(r, s, vb, cudaMemcpyDeviceToDevice, c->stream), "r"));
-        RC(axpby(c, make_double2(-om.real(), -om.imag()), Az, make_double2(1, 0), r));
+        RC(axpby1(c, make_double2(-om.real(), -om.imag()), Az, make_double2(1, 0), r));
         zc rrn;
         RC(zdot(c, rst, r, &rrn));
         if (rr_old == zc(0, 0) || om == zc(0, 0)) { status = HELM3D_ERR_BREAKDOWN; break; }
         const zc beta = (alpha / om) * rrn / rr_old;
         // p = r + beta (p - omega Ay)
-        RC(axpby(c, make_double2(-om.real(), -om.imag()), Ay, make_double2(1, 0), p));
-        RC(axpby(c, make_double2(1, 0), r, make_double2(beta.real(), beta.imag()), p));
+        RC(axpby1(c, make_double2(-om.real(), -om.imag()), Ay, make_double2(1, 0), p));
+        RC(axpby1(c, make_double2(1, 0), r, make_double2(beta.real(), beta.imag()), p));
 
         it++;
         double r2;
-        RC(norm2(c, r, nullptr, c->d_h + 1, &r2));
+        RC(norm2_one(c, r, false, &r2, nullptr));
         relres = std::sqrt(r2) / nf;
         if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = relres;
         if (!std::isfinite(relres)) return set_error(c, HELM3D_ERR_NONFINITE, "BiCGStab residual is NaN/Inf");
@@ -480,17 +671,14 @@ int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st) {
     // true residual of the u-space system
     RC(ensure_vec(c, &c->d_r, "residual"));
     if (modeN) {
-        RC(residual(c, f, u, c->d_r, false));
+        RC(residual(c, one(f), one(u), one(c->d_r), 1, false));
     } else {
         // A_R u = L0 u - dL u is not formed directly: K(L0 u) = A_R u.  The
         // BiCGStab recursion residual r is reported for mode R.
         RC(cuda_check(c, cudaMemcpyAsync(c->d_r, r, vb, cudaMemcpyDeviceToDevice, c->stream), "r"));
     }
     double r2, rp2;
-    RC(norm2(c, c->d_r, nullptr, c->d_h + 1, &r2));
-    int box[6];
-    phys_box(c, box);
-    RC(norm2(c, c->d_r, box, c->d_h + 1, &rp2));
+    RC(norm2_one(c, c->d_r, true, &r2, &rp2));
     cudaEventRecord(c->ev1, c->stream);
     RC(check_status(c));
     float ms = 0;

@@ -20,12 +20,16 @@ __global__ void __launch_bounds__(kStX *kStY) stencil_kernel(StencilArgs a) {
     const int i = blockIdx.x * kStX + threadIdx.x;
     const int j = blockIdx.y * kStY + threadIdx.y;
     if (i >= a.nx || j >= a.ny) return;
-    const int k0 = blockIdx.z * kStZ;
+    const int nzc = (a.nz + kStZ - 1) / kStZ;
+    const int r = blockIdx.z / nzc;
+    const int k0 = (blockIdx.z - r * nzc) * kStZ;
     const int k1 = min(a.nz, k0 + kStZ);
     const long plane = (long)a.nx * a.ny;
     const long col = (long)j * a.nx + i;
-    const double2 *x = a.x;
-    const double xs = a.xscale;
+    const double2 *x = a.x.p + r * a.x.stride;
+    double2 *yout = a.y.p + r * a.y.stride;
+    const double2 *fin = a.f.p ? a.f.p + r * a.f.stride : nullptr;
+    const double xs = a.xscale * (a.sc.p ? a.sc.p[r * a.sc.stride] : 1.0);
 
     // per-axis couplings at this (i, j); for ADJ the ones that multiply the
     // neighbours are conj(cp[i-1]) (from i-1) and conj(cm[i+1]) (from i+1)
@@ -81,11 +85,11 @@ __global__ void __launch_bounds__(kStX *kStY) stencil_kernel(StencilArgs a) {
         acc = cfma(czp, up, acc);
         acc.x *= xs;
         acc.y *= xs;
-        if (a.f) {
-            const double2 fv = a.f[idx];
+        if (fin) {
+            const double2 fv = fin[idx];
             acc = make_double2(fv.x - acc.x, fv.y - acc.y);
         }
-        a.y[idx] = acc;
+        yout[idx] = acc;
         um = uc;
         uc = up;
     }
@@ -93,7 +97,7 @@ __global__ void __launch_bounds__(kStX *kStY) stencil_kernel(StencilArgs a) {
 
 int launch_stencil(const StencilArgs &a, bool adjoint, cudaStream_t s) {
     dim3 block(kStX, kStY);
-    dim3 grid((a.nx + kStX - 1) / kStX, (a.ny + kStY - 1) / kStY, (a.nz + kStZ - 1) / kStZ);
+    dim3 grid((a.nx + kStX - 1) / kStX, (a.ny + kStY - 1) / kStY, ((a.nz + kStZ - 1) / kStZ) * a.R);
     if (adjoint) stencil_kernel<true><<<grid, block, 0, s>>>(a);
     else stencil_kernel<false><<<grid, block, 0, s>>>(a);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;

@@ -12,13 +12,15 @@
 // mbarrier completion) that a dedicated producer warp issues as far ahead as
 // the ring allows, independently of the y_{j-1} -> y_j dependence chain.
 // Each of the 8 consumer warps owns RW = 32/G rows of y: lane (il, g) owns
-// row i = w*RW + il and accumulates G^T[m][i] v[m] over the rows m = g, g+G,
-// ... of every stage; the G partial sums of a row meet by warp shuffles, so a
-// y-line ends with one named barrier among the consumer warps and no
-// shared-memory reduction.  v[m] is formed on the fly from the previous
-// line's result and the current line's right-hand side, both double-buffered
-// in shared memory; the next line's right-hand side is prefetched into
-// registers while the current line streams.
+// row i = w*RW + il and accumulates G^T[m][i] v[m][r] over the rows m = g,
+// g+G, ... of every stage for all RR right-hand sides r (one G element feeds
+// RR complex FMAs); the G partial sums of a row meet by warp shuffles.  The
+// row owner also forms the next line's v[i][r] (f_{j+1} - cmy y_j forward,
+// x_j backward) into a double-buffered shared array, so a y-line ends with
+// one named barrier among the consumer warps and no shared-memory reduction.
+// The next line's right-hand side is prefetched into registers while the
+// current line streams.  Planes of R right-hand sides are laid out
+// [kz][line][r][i].
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -30,11 +32,10 @@
 namespace h3d {
 
 template <typename R> struct SweepK {
-    int n, ny, ldg;
+    int n, ny, ldg, nrhs;
     const cplx<R> *Gt;
     const cplx<R> *cmy, *cpy;
     cplx<R> *planes;
-    long rhs_stride;
     int rows_per_stage;  // rows of G^T per ring stage
     int nstage;          // ring depth
     uint32_t stage_bytes;
@@ -61,20 +62,20 @@ __device__ __forceinline__ const cplx<R> *stage_src(const SweepK<R> &a, int kz, 
     return a.Gt + (((long)kz * a.ny + line) * a.n + r0) * (long)a.ldg;
 }
 
-template <typename R, int G>
+// G groups of lanes split the rows m of each stage; RR right-hand sides
+template <typename R, int G, int RR>
 __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kernel(SweepK<R> a) {
     typedef cplx<R> Cx;
     constexpr int RW = 32 / G;  // rows of y per warp
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    const int n = a.n, ny = a.ny, ldg = a.ldg;
+    const int n = a.n, ny = a.ny, ldg = a.ldg, Rn = a.nrhs;
     const int kz = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Cx *ring = reinterpret_cast<Cx *>(smem_raw);
-    Cx *ybuf = reinterpret_cast<Cx *>(smem_raw + (size_t)a.nstage * a.stage_bytes);  // [2][kSweepMaxN]
-    Cx *fbuf = ybuf + 2 * kSweepMaxN;                                                 // [2][kSweepMaxN]
-    uint64_t *full = reinterpret_cast<uint64_t *>(fbuf + 2 * kSweepMaxN);
+    Cx *vbuf = reinterpret_cast<Cx *>(smem_raw + (size_t)a.nstage * a.stage_bytes);  // [2][n][RR]
+    uint64_t *full = reinterpret_cast<uint64_t *>(vbuf + 2 * (size_t)n * RR);
     uint64_t *empty = full + a.nstage;
-    Cx *P = a.planes + (long)blockIdx.y * a.rhs_stride + (long)kz * ny * n;
+    Cx *P = a.planes + (long)kz * ny * Rn * n;  // line j, rhs r, row i at ((j*Rn + r)*n + i)
     const int cpl = (n + a.rows_per_stage - 1) / a.rows_per_stage;
     const long nseq = (long)(2 * ny - 1) * cpl;
 
@@ -85,7 +86,10 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
         }
         fence_mbar_init_cluster();
     }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) fbuf[i] = P[i];  // f_0
+    for (int q = threadIdx.x; q < n * RR; q += blockDim.x) {  // v of line 0: f_0
+        const int m = q / RR, r = q - (q / RR) * RR;
+        vbuf[q] = r < Rn ? P[(long)r * n + m] : mkc<R>(0, 0);
+    }
     __syncthreads();
 
     if (warp == kSweepConsumerWarps) {
@@ -117,17 +121,21 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
     for (int step = 0; step < 2 * ny - 1; step++) {
         const bool fwd = step < ny;
         const int line = fwd ? step : 2 * ny - 2 - step;
-        const Cx *yprev = ybuf + ((step + 1) & 1) * kSweepMaxN;  // y_{line-1} (fwd) / x_{line+1} (bwd)
-        Cx *ycur = ybuf + (step & 1) * kSweepMaxN;
-        const Cx *fcur = fbuf + (step & 1) * kSweepMaxN;
-        const Cx c = fwd ? (line > 0 ? a.cmy[line] : mkc<R>(0, 0)) : mkc<R>(0, 0);
+        const Cx *v = vbuf + (size_t)(step & 1) * n * RR;
+        Cx *vnext = vbuf + (size_t)((step + 1) & 1) * n * RR;
         // prefetch: next line's right-hand side (forward) or this line's y (backward)
-        Cx pre = mkc<R>(0, 0);
-        if (own && g == 0) {
-            if (fwd && line + 1 < ny) pre = P[(long)(line + 1) * n + i];
-            else if (!fwd) pre = P[(long)line * n + i];
+        Cx pre[RR];
+#pragma unroll
+        for (int r = 0; r < RR; r++) {
+            pre[r] = mkc<R>(0, 0);
+            if (own && g == 0 && r < Rn) {
+                if (fwd && line + 1 < ny) pre[r] = P[((long)(line + 1) * Rn + r) * n + i];
+                else if (!fwd) pre[r] = P[((long)line * Rn + r) * n + i];
+            }
         }
-        Cx acc = mkc<R>(0, 0);
+        Cx acc[RR];
+#pragma unroll
+        for (int r = 0; r < RR; r++) acc[r] = mkc<R>(0, 0);
         for (int ch = 0; ch < cpl; ch++, seq++) {
             const int s = (int)(seq % a.nstage);
             const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
@@ -139,80 +147,99 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
             const int r0 = ch * a.rows_per_stage;
             const int rows = min(a.rows_per_stage, n - r0);
             if (own) {
-#pragma unroll 4
+#pragma unroll 2
                 for (int ml = g; ml < rows; ml += G) {
-                    const int m = r0 + ml;
-                    Cx v;
-                    if (fwd) v = (line > 0) ? cfms(c, yprev[m], fcur[m]) : fcur[m];
-                    else v = yprev[m];
-                    acc = cfma(st[(long)ml * ldg + i], v, acc);
+                    const Cx gv = st[(long)ml * ldg + i];
+                    const Cx *vm = v + (size_t)(r0 + ml) * RR;
+#pragma unroll
+                    for (int r = 0; r < RR; r++) acc[r] = cfma(gv, vm[r], acc[r]);
                 }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive_local(&empty[s]);
         }
 #pragma unroll
-        for (int off = RW; off < 32; off <<= 1) {
-            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
-            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
-        }
-        if (own && g == 0) {
-            Cx out;
-            if (fwd) {
-                out = acc;
-                if (line + 1 < ny) fbuf[((step + 1) & 1) * kSweepMaxN + i] = pre;
-            } else {
-                out = cfms(a.cpy[line], acc, pre);
+        for (int r = 0; r < RR; r++)
+#pragma unroll
+            for (int off = RW; off < 32; off <<= 1) {
+                acc[r].x += __shfl_xor_sync(0xffffffffu, acc[r].x, off);
+                acc[r].y += __shfl_xor_sync(0xffffffffu, acc[r].y, off);
             }
-            ycur[i] = out;
-            P[(long)line * n + i] = out;
+        if (own && g == 0) {
+            const Cx cn = (fwd && line + 1 < ny) ? a.cmy[line + 1] : mkc<R>(0, 0);
+            const Cx cp = fwd ? mkc<R>(0, 0) : a.cpy[line];
+#pragma unroll
+            for (int r = 0; r < RR; r++) {
+                if (r >= Rn) break;
+                Cx out, vn;
+                if (fwd) {
+                    out = acc[r];                                          // y_line
+                    vn = (line + 1 < ny) ? cfms(cn, out, pre[r]) : out;  // f_{line+1} - cmy y_line, or x_{ny-1}
+                } else {
+                    out = cfms(cp, acc[r], pre[r]);                        // x_line = y_line - cpy G x_{line+1}
+                    vn = out;
+                }
+                P[((long)line * Rn + r) * n + i] = out;
+                vnext[(size_t)i * RR + r] = vn;
+            }
         }
         consumer_barrier();
     }
 }
 
-template <typename R, int G> static int sweep_impl(const SweepArgs &sa, cudaStream_t st) {
+template <typename R, int G, int RR> static int sweep_impl(const SweepArgs &sa, cudaStream_t st) {
     typedef cplx<R> Cx;
     SweepK<R> k;
     k.n = sa.n;
     k.ny = sa.ny;
     k.ldg = sa.ldg;
+    k.nrhs = sa.R;
     k.Gt = (const Cx *)sa.Gt;
     k.cmy = (const Cx *)sa.cmy;
     k.cpy = (const Cx *)sa.cpy;
     k.planes = (Cx *)sa.planes;
-    k.rhs_stride = sa.rhs_stride;
     k.status = sa.status;
-    // ~16 KB stages, as many as fit in ~200 KB
+    const size_t vbytes = sizeof(Cx) * 2 * (size_t)sa.n * RR;
+    const size_t budget = device_info().smem_optin - vbytes - 1024;
+    // ~16 KB stages, as many as fit the rest of shared memory (at most ~200 KB)
     const size_t row_bytes = (size_t)sa.ldg * sizeof(Cx);
     int rows = (int)((16 * 1024) / row_bytes);
     if (rows < 1) rows = 1;
     if (rows > sa.n) rows = sa.n;
     k.rows_per_stage = rows;
     k.stage_bytes = (uint32_t)(((size_t)rows * row_bytes + 127) & ~(size_t)127);
-    int nst = (int)((200 * 1024) / k.stage_bytes);
+    size_t ring_cap = budget < (size_t)200 * 1024 ? budget : (size_t)200 * 1024;
+    int nst = (int)(ring_cap / k.stage_bytes);
     if (nst > 32) nst = 32;
-    if (nst < 2) nst = 2;
+    if (nst < 2) return HELM3D_ERR_ARG;
     k.nstage = nst;
-    const size_t smem = (size_t)nst * k.stage_bytes + sizeof(Cx) * 4 * kSweepMaxN + 2 * nst * sizeof(uint64_t);
-    auto kern = sweep_kernel<R, G>;
+    const size_t smem = (size_t)nst * k.stage_bytes + vbytes + 2 * nst * sizeof(uint64_t);
+    auto kern = sweep_kernel<R, G, RR>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return HELM3D_ERR_CUDA;
-    kern<<<dim3((unsigned)sa.nz, (unsigned)sa.nrhs), (kSweepConsumerWarps + 1) * 32, smem, st>>>(k);
+    kern<<<dim3((unsigned)sa.nz), (kSweepConsumerWarps + 1) * 32, smem, st>>>(k);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
+template <typename R, int G> static int sweep_rr(const SweepArgs &sa, cudaStream_t s) {
+    if (sa.R <= 1) return sweep_impl<R, G, 1>(sa, s);
+    if (sa.R <= 2) return sweep_impl<R, G, 2>(sa, s);
+    if (sa.R <= 4) return sweep_impl<R, G, 4>(sa, s);
+    if (sa.R <= 8) return sweep_impl<R, G, 8>(sa, s);
+    return sweep_impl<R, G, 16>(sa, s);
+}
+
 int launch_sweep(bool c64, const SweepArgs &sa, cudaStream_t s) {
-    if (sa.n < 1 || sa.n > kSweepMaxN) return HELM3D_ERR_ARG;
+    if (sa.n < 1 || sa.n > kSweepMaxN || sa.R < 1 || sa.R > kMaxBatch) return HELM3D_ERR_ARG;
     const int g = sa.n <= 64 ? 4 : (sa.n <= 128 ? 2 : 1);
     if (c64) {
-        if (g == 4) return sweep_impl<float, 4>(sa, s);
-        if (g == 2) return sweep_impl<float, 2>(sa, s);
-        return sweep_impl<float, 1>(sa, s);
+        if (g == 4) return sweep_rr<float, 4>(sa, s);
+        if (g == 2) return sweep_rr<float, 2>(sa, s);
+        return sweep_rr<float, 1>(sa, s);
     }
-    if (g == 4) return sweep_impl<double, 4>(sa, s);
-    if (g == 2) return sweep_impl<double, 2>(sa, s);
-    return sweep_impl<double, 1>(sa, s);
+    if (g == 4) return sweep_rr<double, 4>(sa, s);
+    if (g == 2) return sweep_rr<double, 2>(sa, s);
+    return sweep_rr<double, 1>(sa, s);
 }
 
 }  // namespace h3d

@@ -18,24 +18,35 @@ namespace h3d {
 
 constexpr int kZtCols = 32, kZtWarps = 8, kZtRows = 4;
 
+// plane index of (row k, column w = i + nx*j) for right-hand side r
+__device__ __forceinline__ long zt_plane_index(const PlaneLayout &L, int r, int k, long w) {
+    const long j = w / L.nx, i = w - j * L.nx;
+    return (long)k * L.plane * L.R + (j * L.R + r) * L.nx + i;
+}
+
 template <typename R, bool FWD>
-__global__ void __launch_bounds__(kZtCols *kZtWarps) ztrans_kernel(int nz, long plane, const void *__restrict__ in,
-                                                                   double scale, void *__restrict__ out,
+__global__ void __launch_bounds__(kZtCols *kZtWarps) ztrans_kernel(PlaneLayout L, VecBatch vec, double scale,
+                                                                   ScaleBatch sc, cplx<R> *__restrict__ planes,
                                                                    const double2 *__restrict__ M) {
     typedef cplx<R> Cx;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *tile = reinterpret_cast<double2 *>(smem_raw);  // [nz][kZtCols]
+    const int nz = L.nz;
+    const long plane = L.plane;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int r = blockIdx.y;
+    double2 *v_r = vec.p + r * vec.stride;
+    const double s = scale * (sc.p ? sc.p[r * sc.stride] : 1.0);
     const long w = (long)blockIdx.x * kZtCols + lane;
     const bool valid = w < plane;
     for (int j = warp; j < nz; j += kZtWarps) {
         double2 v = make_double2(0, 0);
         if (valid) {
             if (FWD) {
-                const double2 x = reinterpret_cast<const double2 *>(in)[(long)j * plane + w];
-                v = make_double2(scale * x.x, scale * x.y);
+                const double2 x = v_r[(long)j * plane + w];
+                v = make_double2(s * x.x, s * x.y);
             } else {
-                v = cvt<double2, Cx>(reinterpret_cast<const Cx *>(in)[(long)j * plane + w]);
+                v = cvt<double2, Cx>(planes[zt_plane_index(L, r, j, w)]);
             }
         }
         tile[j * kZtCols + lane] = v;
@@ -44,46 +55,48 @@ __global__ void __launch_bounds__(kZtCols *kZtWarps) ztrans_kernel(int nz, long 
     for (int k0 = warp * kZtRows; k0 < nz; k0 += kZtWarps * kZtRows) {
         double2 acc[kZtRows];
 #pragma unroll
-        for (int r = 0; r < kZtRows; r++) acc[r] = make_double2(0, 0);
+        for (int q = 0; q < kZtRows; q++) acc[q] = make_double2(0, 0);
         for (int j = 0; j < nz; j++) {
             const double2 t = tile[j * kZtCols + lane];
 #pragma unroll
-            for (int r = 0; r < kZtRows; r++)
-                if (k0 + r < nz) acc[r] = cfma(__ldg(&M[(long)(k0 + r) * nz + j]), t, acc[r]);
+            for (int q = 0; q < kZtRows; q++)
+                if (k0 + q < nz) acc[q] = cfma(__ldg(&M[(long)(k0 + q) * nz + j]), t, acc[q]);
         }
         if (!valid) continue;
 #pragma unroll
-        for (int r = 0; r < kZtRows; r++) {
-            const int k = k0 + r;
+        for (int q = 0; q < kZtRows; q++) {
+            const int k = k0 + q;
             if (k >= nz) break;
-            if (FWD) reinterpret_cast<Cx *>(out)[(long)k * plane + w] = cvt<Cx, double2>(acc[r]);
-            else reinterpret_cast<double2 *>(out)[(long)k * plane + w] = acc[r];
+            if (FWD) planes[zt_plane_index(L, r, k, w)] = cvt<Cx, double2>(acc[q]);
+            else v_r[(long)k * plane + w] = acc[q];
         }
     }
 }
 
 template <typename R, bool FWD>
-static int zt_impl(int nz, long plane, const void *in, double scale, void *out, const void *M, cudaStream_t s) {
-    const size_t smem = (size_t)nz * kZtCols * sizeof(double2);
+static int zt_impl(const PlaneLayout &L, const VecBatch &vec, double scale, const ScaleBatch &sc, void *planes,
+                   const double2 *M, cudaStream_t s) {
+    const size_t smem = (size_t)L.nz * kZtCols * sizeof(double2);
     auto kern = ztrans_kernel<R, FWD>;
     if (smem > device_info().smem_optin) return HELM3D_ERR_ARG;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return HELM3D_ERR_CUDA;
-    const unsigned grid = (unsigned)((plane + kZtCols - 1) / kZtCols);
-    kern<<<grid, kZtCols * kZtWarps, smem, s>>>(nz, plane, in, scale, out, (const double2 *)M);
+    const dim3 grid((unsigned)((L.plane + kZtCols - 1) / kZtCols), (unsigned)L.R);
+    kern<<<grid, kZtCols * kZtWarps, smem, s>>>(L, vec, scale, sc, (cplx<R> *)planes, M);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
-int launch_ztrans_forward(bool c64, const double2 *x, double scale, void *planes, int nz, long plane, const double2 *Wi,
-                          cudaStream_t s) {
-    return c64 ? zt_impl<float, true>(nz, plane, x, scale, planes, Wi, s)
-               : zt_impl<double, true>(nz, plane, x, scale, planes, Wi, s);
+int launch_ztrans_forward(bool c64, const VecBatch &x, double scale, const ScaleBatch &sc, void *planes,
+                          const PlaneLayout &L, const double2 *Wi, cudaStream_t s) {
+    return c64 ? zt_impl<float, true>(L, x, scale, sc, planes, Wi, s)
+               : zt_impl<double, true>(L, x, scale, sc, planes, Wi, s);
 }
 
-int launch_ztrans_inverse(bool c64, const void *planes, double2 *y, int nz, long plane, const double2 *W,
+int launch_ztrans_inverse(bool c64, const void *planes, const PlaneLayout &L, const VecBatch &y, const double2 *W,
                           cudaStream_t s) {
-    return c64 ? zt_impl<float, false>(nz, plane, planes, 1.0, y, W, s)
-               : zt_impl<double, false>(nz, plane, planes, 1.0, y, W, s);
+    const ScaleBatch none = {nullptr, 0};
+    return c64 ? zt_impl<float, false>(L, y, 1.0, none, (void *)planes, W, s)
+               : zt_impl<double, false>(L, y, 1.0, none, (void *)planes, W, s);
 }
 
 }  // namespace h3d

@@ -149,3 +149,53 @@ def test_zpml_eigen_fgmres(prec):
     t = mode_n_solver(p, precision=prec, tol=1e-10)
     t.solve(f)
     assert s.last_stats.iterations * 3 < t.last_stats.iterations
+
+
+# ------------------------------------------------- batched right-hand sides
+@pytest.mark.parametrize("prec", [0, 1])
+def test_batched_sources_match_single(prec):
+    """A lockstep batch (a zero right-hand side, a random one that converges
+    at another iteration than the point sources) returns the solutions that
+    single solves return."""
+    p = media.config_small(20, 4, seed=4, n_sources=3)
+    F = np.stack([p.rhs(0), p.rhs(1), np.zeros(p.shape, np.complex128), rand_c(p.shape, seed=7), p.rhs(2)])
+    s = mode_n_solver(p, precision=prec, tol=1e-10)
+    U = s.solve(F, nrhs=len(F))
+    assert s.last_stats.relres < 1e-10
+    on = mode_n.setup(p, factor=False)
+    assert np.all(U[2] == 0)
+    for i in (0, 1, 3, 4):
+        assert np.linalg.norm(on.apply_a(U[i]) - F[i]) / np.linalg.norm(F[i]) < 2e-10
+        assert rel(U[i], s.solve(F[i])) < 1e-7
+
+
+def test_batched_sources_more_than_one_batch():
+    """18 right-hand sides: two lockstep batches (at most 16 per batch)."""
+    p = small_problem(16, 14, 12, pml=3, seed=11)
+    F = np.stack([rand_c(p.shape, seed=100 + i) for i in range(18)])
+    s = mode_n_solver(p, precision=1, tol=1e-9)
+    U = s.solve(F, nrhs=18)
+    on = mode_n.setup(p, factor=False)
+    for i in range(18):
+        assert np.linalg.norm(on.apply_a(U[i]) - F[i]) / np.linalg.norm(F[i]) < 2e-9
+
+
+def test_batched_mode_r():
+    g, st = mode_r_case(10, 4, 3)
+    s = mode_r_solver(g, st, tol=1e-11, max_iter=3000)
+    F = np.stack([rand_c(g.shape_zyx, seed=21), rand_c(g.shape_zyx, seed=22)])
+    U = s.solve(F, nrhs=2)
+    for i in range(2):
+        assert rel(U[i], s.solve(F[i])) < 1e-7
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_batched_zpml_eigen(prec):
+    import helm3d
+    p = media.config_small(20, 4, seed=8, n_sources=2)
+    F = np.stack([p.rhs(0), p.rhs(1)])
+    s = mode_n_solver(p, precision=prec, tol=1e-10, z_transform=helm3d.ZT_PML_EIGEN)
+    U = s.solve(F, nrhs=2)
+    on = mode_n.setup(p, factor=False)
+    for i in range(2):
+        assert np.linalg.norm(on.apply_a(U[i]) - F[i]) / np.linalg.norm(F[i]) < 2e-10
