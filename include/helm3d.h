@@ -122,17 +122,21 @@ int helm3d_create(const helm3d_grid *grid, const double *s2, const helm3d_opts *
 /* New medium on the same grid: recompute dL / shifts and refactor. */
 int helm3d_set_medium(helm3d_ctx *ctx, const double *s2);
 
-/* Solve for nrhs right-hand sides f[r*N .. ] -> u[r*N ..] with FGMRES.
- * u on entry is the initial guess when stats->status == -1 on entry is not
- * used; initial guess is zero.  Replaces FGMRES (Source/FGMRES.cpp:6-725,
- * prototype Source/templates.h:59). */
+/* Solve for nrhs right-hand sides f[r*N .. ] -> u[r*N ..] with FGMRES from
+ * a zero initial guess.  The right-hand sides go through the iteration in
+ * lockstep batches of up to 16 (as many as device memory holds), one
+ * preconditioner and operator launch per step for the whole batch;
+ * stats->iterations is summed over the right-hand sides and relres is the
+ * largest.  Replaces FGMRES (Source/FGMRES.cpp:6-725, prototype
+ * Source/templates.h:59), which the reference calls once per source. */
 int helm3d_solve(helm3d_ctx *ctx, const double *f, double *u, int nrhs, helm3d_stats *stats);
 
 /* The same system by BiCGStab with the reference's shadow residual 2 r0.
  * Replaces BCGSTAB (Source/BcGSTAB.cpp:6-666, Source/templates.h:60). */
 int helm3d_solve_bicgstab(helm3d_ctx *ctx, const double *f, double *u, helm3d_stats *stats);
 
-/* Adjoint solve A^H lambda = g (mode N), with M^H as the preconditioner. */
+/* Adjoint solve A^H lambda = g (mode N) by FGMRES right-preconditioned with
+ * M^{-H}.  No counterpart in the reference. */
 int helm3d_solve_adjoint(helm3d_ctx *ctx, const double *g, double *lambda, helm3d_stats *stats);
 
 /* y = A x (mode N) or y = K x = x - dL L0^{-1} x (mode R,
@@ -146,6 +150,11 @@ int helm3d_apply_op_adjoint(helm3d_ctx *ctx, const double *x, double *y);
  * (Solve3DSparseUsingFT_CSR, Source/functions.cpp:5837-6061). */
 int helm3d_apply_prec(helm3d_ctx *ctx, const double *x, double *y);
 
+/* y = M^{-H} x (mode N): the conjugate transpose of the preconditioner, used
+ * by the adjoint solve.  No counterpart in the reference, which has no
+ * adjoint. */
+int helm3d_apply_prec_adjoint(helm3d_ctx *ctx, const double *x, double *y);
+
 /* The same y = M^{-1} x for callers that cannot allocate device memory at
  * the point of use (inside an allocator or pool callback, with free memory
  * held by a caching allocator, or on a path that must avoid cudaMalloc's
@@ -157,9 +166,13 @@ int helm3d_apply_prec(helm3d_ctx *ctx, const double *x, double *y);
  * array.  No counterpart in the reference, which has no device code. */
 int helm3d_apply_prec_noalloc(helm3d_ctx *ctx, const double *x, double *y);
 
-/* Gradient of J = 0.5 sum_s ||P u_s - d_s||^2 with respect to s2, where
- * A u_s = f_s; P samples u at nrecv grid indices.  f: nsrc vectors, data:
- * nsrc*nrecv complex, grad: N doubles (host or device), misfit: host. */
+/* Gradient of J = 0.5 sum_s ||P u_s - d_s||^2 with respect to s2 (mode N),
+ * where A u_s = f_s and P samples u at the nrecv grid indices recv (the same
+ * for every source; repeats allowed): forward solves, adjoint solves
+ * A^H lam_s = P^T (d_s - P u_s), then grad = sum_s Re(conj(lam_s) omega^2
+ * (1 + i beta_phys) u_s), all batched over sources.  f: nsrc vectors, data:
+ * nsrc*nrecv complex, grad: N doubles (overwritten), each host or device;
+ * misfit: host (may be NULL).  No counterpart in the reference. */
 int helm3d_misfit_grad(helm3d_ctx *ctx, const double *f, int nsrc, const long long *recv, int nrecv,
                        const double *data, double *grad, double *misfit, helm3d_stats *stats);
 

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <algorithm>
 #include <new>
+#include <vector>
 
 #include "helm3d_internal.h"
 
@@ -56,14 +57,15 @@ struct VecArg {
 };
 
 // Right-hand sides per lockstep batch: at most kMaxBatch, and as many as the
-// Krylov bases (V, Z), packed iterates, planes and staging of each fit in
-// 85% of the free device memory (plus what the context's Krylov workspace
-// already holds).
-int batch_size(helm3d_ctx *c, int nrhs, bool staged) {
+// Krylov bases (V, Z), packed iterates, planes, staging and `extra` further
+// vectors of each fit in 85% of the free device memory (plus what the
+// context's Krylov workspace already holds).
+int batch_size(helm3d_ctx *c, int nrhs, bool staged, int extra = 0) {
     const int m = std::max(1, c->opts.restart);
     const size_t vb = sizeof(double2) * (size_t)c->N;
-    const size_t per = vb * ((size_t)(m + 1) + (c->opts.mode == HELM3D_MODE_N ? m : 0) + 2 + (staged ? 2 : 0)) +
-                       (c->c64 ? 8 : 16) * (size_t)c->N;
+    const size_t per =
+        vb * ((size_t)(m + 1) + (c->opts.mode == HELM3D_MODE_N ? m : 0) + 2 + (staged ? 2 : 0) + extra) +
+        (c->c64 ? 8 : 16) * (size_t)c->N;
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
         cudaGetLastError();
@@ -271,6 +273,15 @@ int helm3d_solve_adjoint(helm3d_ctx *c, const double *g, double *lam, helm3d_sta
     return solve_common(c, g, lam, 1, st, 2);
 }
 
+// device memory released when the scope ends
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    int alloc(helm3d_ctx *c, size_t bytes, const char *what) { return cuda_check(c, cudaMalloc(&p, bytes), what); }
+};
+
 static int apply_common(helm3d_ctx *c, const double *x, double *y, int which) {
     if (!c || !x || !y) return HELM3D_ERR_ARG;
     cudaSetDevice(c->device);
@@ -283,7 +294,8 @@ static int apply_common(helm3d_ctx *c, const double *x, double *y, int which) {
     int rc;
     if (which == 0) rc = apply_op(c, xb, 1.0, one, yb, 1);
     else if (which == 1) rc = apply_op_adjoint(c, xb, 1.0, one, yb, 1);
-    else rc = apply_prec(c, xb, 1.0, one, yb, 1);
+    else if (which == 2) rc = apply_prec(c, xb, 1.0, one, yb, 1);
+    else rc = apply_prec_adjoint(c, xb, 1.0, one, yb, 1);
     if (rc) return rc;
     rc = ya.copy_out(y, c->N);
     if (rc) return rc;
@@ -293,25 +305,115 @@ static int apply_common(helm3d_ctx *c, const double *x, double *y, int which) {
 int helm3d_apply_op(helm3d_ctx *c, const double *x, double *y) { return apply_common(c, x, y, 0); }
 int helm3d_apply_op_adjoint(helm3d_ctx *c, const double *x, double *y) { return apply_common(c, x, y, 1); }
 int helm3d_apply_prec(helm3d_ctx *c, const double *x, double *y) { return apply_common(c, x, y, 2); }
+int helm3d_apply_prec_adjoint(helm3d_ctx *c, const double *x, double *y) { return apply_common(c, x, y, 3); }
 
 int helm3d_misfit_grad(helm3d_ctx *c, const double *f, int nsrc, const long long *recv, int nrecv, const double *data,
                        double *grad, double *misfit, helm3d_stats *st) {
-    (void)f;
-    (void)nsrc;
-    (void)recv;
-    (void)nrecv;
-    (void)data;
-    (void)grad;
-    (void)misfit;
-    (void)st;
-    return set_error(c, HELM3D_ERR_ARG, "misfit gradient not built yet");
+    if (!c) return HELM3D_ERR_ARG;
+    if (!f || !grad || nsrc < 1 || nrecv < 0 || (nrecv > 0 && (!recv || !data)))
+        return set_error(c, HELM3D_ERR_ARG, "misfit_grad: bad arguments");
+    if (c->opts.mode != HELM3D_MODE_N) return set_error(c, HELM3D_ERR_ARG, "misfit gradient is mode N only");
+    cudaSetDevice(c->device);
+    if (st) {
+        st->iterations = 0;
+        st->restarts = 0;
+        st->ms_solve = 0;
+        st->relres = 0;
+        st->relres_phys = 0;
+        st->history_len = 0;
+    }
+    const long N = c->N;
+    int rc;
+    // receivers: checked on the host, used from the device
+    std::vector<long long> hrecv((size_t)nrecv);
+    DevBuf d_recv, d_data, d_grad, d_u, d_lam, d_adj, d_res;
+    if (nrecv > 0) {
+        if ((rc = cuda_check(c, cudaMemcpy(hrecv.data(), recv, sizeof(long long) * nrecv, cudaMemcpyDefault),
+                             "receivers")))
+            return rc;
+        for (long long q : hrecv)
+            if (q < 0 || q >= N) return set_error(c, HELM3D_ERR_ARG, "misfit_grad: receiver index out of range");
+        if ((rc = d_recv.alloc(c, sizeof(long long) * nrecv, "receivers")) ||
+            (rc = cuda_check(c, cudaMemcpy(d_recv.p, hrecv.data(), sizeof(long long) * nrecv, cudaMemcpyHostToDevice),
+                             "receivers")))
+            return rc;
+    }
+    const double2 *dd = (const double2 *)data;
+    if (nrecv > 0 && !is_device_ptr(data)) {
+        const size_t b = sizeof(double2) * (size_t)nsrc * nrecv;
+        if ((rc = d_data.alloc(c, b, "data")) ||
+            (rc = cuda_check(c, cudaMemcpy(d_data.p, data, b, cudaMemcpyHostToDevice), "data")))
+            return rc;
+        dd = (const double2 *)d_data.p;
+    }
+    const bool gdev = is_device_ptr(grad);
+    double *g = grad;
+    if (!gdev) {
+        if ((rc = d_grad.alloc(c, sizeof(double) * N, "gradient"))) return rc;
+        g = (double *)d_grad.p;
+    }
+    if ((rc = cuda_check(c, cudaMemsetAsync(g, 0, sizeof(double) * N, c->stream), "gradient zero"))) return rc;
+    const bool fstaged = !is_device_ptr(f);
+    const int B = batch_size(c, nsrc, fstaged, 3);
+    const size_t vb = sizeof(double2) * (size_t)N;
+    if ((rc = d_u.alloc(c, vb * B, "wavefields")) || (rc = d_lam.alloc(c, vb * B, "adjoint wavefields")) ||
+        (rc = d_adj.alloc(c, vb * B, "adjoint sources")) ||
+        (nrecv > 0 && (rc = d_res.alloc(c, sizeof(double2) * (size_t)B * nrecv, "receiver residuals"))))
+        return rc;
+    double2 *U = (double2 *)d_u.p, *Lam = (double2 *)d_lam.p, *Adj = (double2 *)d_adj.p, *Res = (double2 *)d_res.p;
+    std::vector<double2> hres((size_t)B * std::max(nrecv, 0));
+    const double w2 = c->grid.omega * c->grid.omega;
+    double J = 0.0;
+    int worst = HELM3D_OK;
+    for (int r0 = 0; r0 < nsrc; r0 += B) {
+        const int R = std::min(B, nsrc - r0);
+        VecArg fa(c, f + 2 * (size_t)r0 * N, (size_t)R * N, true, &c->d_f, &c->f_cap);
+        if (fa.rc) return fa.rc;
+        // forward wavefields
+        rc = fgmres(c, fa.dev, U, R, false, st);
+        if (rc && rc != HELM3D_ERR_NOT_CONVERGED) return rc;
+        if (rc) worst = rc;
+        // receiver residuals P u - d, misfit, adjoint sources P^T (d - P u)
+        if ((rc = cuda_check(c, cudaMemsetAsync(Adj, 0, vb * R, c->stream), "adjoint source zero"))) return rc;
+        if (nrecv > 0) {
+            rc = timed(c, HELM3D_K_KRYLOV, 2, [&] {
+                int r1 = launch_receiver_residual(VecBatch{U, N}, R, (const long long *)d_recv.p, nrecv,
+                                                  dd + (size_t)r0 * nrecv, nrecv, Res, c->stream);
+                if (r1) return r1;
+                return launch_adjoint_source(Res, R, (const long long *)d_recv.p, nrecv, -1.0, VecBatch{Adj, N},
+                                             c->stream);
+            });
+            if (rc) return set_error(c, rc, "misfit_grad: receiver kernels");
+            if ((rc = cuda_check(c, cudaMemcpyAsync(hres.data(), Res, sizeof(double2) * (size_t)R * nrecv,
+                                                    cudaMemcpyDeviceToHost, c->stream),
+                                 "residuals")) ||
+                (rc = cuda_check(c, cudaStreamSynchronize(c->stream), "residuals")))
+                return rc;
+            for (size_t q = 0; q < (size_t)R * nrecv; q++) J += 0.5 * (hres[q].x * hres[q].x + hres[q].y * hres[q].y);
+        }
+        // adjoint wavefields A^H lam = P^T (d - P u)
+        rc = fgmres(c, Adj, Lam, R, true, st);
+        if (rc && rc != HELM3D_ERR_NOT_CONVERGED) return rc;
+        if (rc) worst = rc;
+        rc = timed(c, HELM3D_K_KRYLOV, 1, [&] {
+            return launch_grad_accum(VecBatch{Lam, N}, VecBatch{U, N}, R, w2, c->opts.beta_phys, g, N, c->stream);
+        });
+        if (rc) return set_error(c, rc, "misfit_grad: gradient kernel");
+    }
+    if (!gdev && (rc = cuda_check(c, cudaMemcpyAsync(grad, g, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream),
+                                  "gradient out")))
+        return rc;
+    if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "misfit_grad"))) return rc;
+    if (misfit) *misfit = J;
+    if (st) st->status = worst;
+    return worst;
 }
 
 int helm3d_destroy(helm3d_ctx *c) {
     if (!c) return HELM3D_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void *bufs[] = {c->d_Gt, c->d_tw, c->d_cmx, c->d_cpx, c->d_cmy, c->d_cpy, c->d_base2d, c->d_kz2, c->d_zW, c->d_zWi, c->d_zW64, c->d_zWi64,
+    void *bufs[] = {c->d_Gt, c->d_tw, c->d_cmx, c->d_cpx, c->d_cmy, c->d_cpy, c->d_base2d, c->d_kz2, c->d_zW, c->d_zWi, c->d_zW64, c->d_zWi64, c->d_zWH64, c->d_zWiH64, c->d_dxy,
                     c->d_cmx64, c->d_cpx64, c->d_cmy64, c->d_cpy64, c->d_cmz64, c->d_cpz64, c->d_s2, c->d_dl,
                     c->d_planes, c->d_status, c->d_V, c->d_Z, c->d_vs, c->d_h, c->d_partials, c->d_f, c->d_u,
                     c->d_r, c->d_t, c->d_t2, c->d_bic, c->d_Fw, c->d_Uw};

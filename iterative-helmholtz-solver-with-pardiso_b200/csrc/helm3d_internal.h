@@ -95,6 +95,7 @@ struct SweepArgs {
     const void *cmy, *cpy;
     void *planes;             // PlaneLayout with R right-hand sides
     int R;
+    const void *dxy;          // null: S^{-1}; else S^{-H} with the [2][ny][n] alpha_x alpha_y table
     int *status;              // device flag: bit 2 = a bounded wait expired
 };
 int launch_sweep(bool c64, const SweepArgs &a, cudaStream_t s);
@@ -149,13 +150,16 @@ int launch_set_scale(const double2 *nrm, long sNrm, double *vs, long sVs, int j,
 // sets bit 4 of *status when s2 holds NaN/Inf
 int launch_base2d(bool c64, const double *s2, int nz, long plane, int zlo, int zhi, double w2, double beta,
                   void *base2d, int *status, cudaStream_t s);
-// gradient accumulation g += Re(conj(lam) w2 (1 + i beta) u)
-int launch_grad_accum(const double2 *lam, const double2 *u, double w2, double beta, double *g, long N,
+// ---------------------------------------------------- misfit gradient
+// res[r][q] = u_r[recv[q]] - d[r][q]   (q < nrecv; res stride nrecv, d stride sD)
+int launch_receiver_residual(const VecBatch &u, int R, const long long *recv, int nrecv, const double2 *d, long sD,
+                             double2 *res, cudaStream_t s);
+// y_r[recv[q]] += sign * res[r][q]  (atomic: receivers may repeat)
+int launch_adjoint_source(const double2 *res, int R, const long long *recv, int nrecv, double sign,
+                          const VecBatch &y, cudaStream_t s);
+// g += sum_r Re(conj(lam_r) w2 (1 + i beta) u_r)
+int launch_grad_accum(const VecBatch &lam, const VecBatch &u, int R, double w2, double beta, double *g, long N,
                       cudaStream_t s);
-int launch_gather_residual(const double2 *u, const long long *recv, int nrecv, const double2 *d, double2 *res,
-                           cudaStream_t s);
-int launch_scatter_add(const double2 *vals, const long long *recv, int nrecv, double2 *y, double sign,
-                       cudaStream_t s);
 
 Dev &device_info();
 
@@ -204,6 +208,8 @@ struct helm3d_ctx {
     void *d_base2d = nullptr, *d_kz2 = nullptr;                                    // P precision (kz2: complex mode shifts)
     void *d_zW = nullptr, *d_zWi = nullptr;                                        // P precision
     double2 *d_zW64 = nullptr, *d_zWi64 = nullptr;
+    double2 *d_zWH64 = nullptr, *d_zWiH64 = nullptr;   // W^H, Wi^H (adjoint z-transforms)
+    void *d_dxy = nullptr;         // [2][ny][nx] alpha_x alpha_y and conj(1 / (alpha_x alpha_y)), P precision
     double2 *d_cmx64 = nullptr, *d_cpx64 = nullptr, *d_cmy64 = nullptr, *d_cpy64 = nullptr;
     double2 *d_cmz64 = nullptr, *d_cpz64 = nullptr;
     double *d_s2 = nullptr;        // squared slowness (mode N operator)
@@ -257,6 +263,9 @@ int apply_prec(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch
 int apply_op(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y, int R);
 int apply_op_adjoint(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y,
                      int R);
+// y_r = M^{-H} (xscale sc_r x_r)
+int apply_prec_adjoint(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y,
+                       int R);
 // FGMRES on R right-hand sides f + r N -> u + r N (device), iterated in lockstep
 int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, helm3d_stats *st);
 int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st);

@@ -202,32 +202,6 @@ __global__ void set_scale_kernel(const double2 *nrm, long sNrm, double *vs, long
     }
 }
 
-__global__ void grad_accum_kernel(const double2 *__restrict__ lam, const double2 *__restrict__ u, double w2,
-                                  double beta, double *__restrict__ g, long N) {
-    const long stride = (long)gridDim.x * blockDim.x;
-    for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
-        // dA/ds2 = w2 (1 + i beta): contribution Re(conj(lam) (dA/ds2) u)
-        const double2 du = cmul(make_double2(w2, w2 * beta), u[l]);
-        const double2 lv = lam[l];
-        g[l] += lv.x * du.x + lv.y * du.y;
-    }
-}
-
-__global__ void gather_residual_kernel(const double2 *__restrict__ u, const long long *__restrict__ recv, int nrecv,
-                                       const double2 *__restrict__ d, double2 *__restrict__ res) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < nrecv) res[q] = csub(u[recv[q]], d[q]);
-}
-
-__global__ void scatter_add_kernel(const double2 *__restrict__ vals, const long long *__restrict__ recv, int nrecv,
-                                   double2 *__restrict__ y, double sign) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < nrecv) {
-        const long long l = recv[q];
-        y[l] = make_double2(y[l].x + sign * vals[q].x, y[l].y + sign * vals[q].y);
-    }
-}
-
 template <typename R>
 __global__ void base2d_kernel(const double *__restrict__ s2, int nz, long plane, int zlo, int zhi, double w2,
                               double beta, cplx<R> *__restrict__ out, int *status) {
@@ -312,26 +286,6 @@ int launch_base2d(bool c64, const double *s2, int nz, long plane, int zlo, int z
     const unsigned grid = (unsigned)((plane + 255) / 256);
     if (c64) base2d_kernel<float><<<grid, 256, 0, s>>>(s2, nz, plane, zlo, zhi, w2, beta, (float2 *)base2d, status);
     else base2d_kernel<double><<<grid, 256, 0, s>>>(s2, nz, plane, zlo, zhi, w2, beta, (double2 *)base2d, status);
-    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
-}
-
-int launch_grad_accum(const double2 *lam, const double2 *u, double w2, double beta, double *g, long N,
-                      cudaStream_t s) {
-    grad_accum_kernel<<<grid_for(N), kRedThreads, 0, s>>>(lam, u, w2, beta, g, N);
-    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
-}
-
-int launch_gather_residual(const double2 *u, const long long *recv, int nrecv, const double2 *d, double2 *res,
-                           cudaStream_t s) {
-    if (nrecv <= 0) return HELM3D_OK;
-    gather_residual_kernel<<<(nrecv + 255) / 256, 256, 0, s>>>(u, recv, nrecv, d, res);
-    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
-}
-
-int launch_scatter_add(const double2 *vals, const long long *recv, int nrecv, double2 *y, double sign,
-                       cudaStream_t s) {
-    if (nrecv <= 0) return HELM3D_OK;
-    scatter_add_kernel<<<(nrecv + 255) / 256, 256, 0, s>>>(vals, recv, nrecv, y, sign);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 

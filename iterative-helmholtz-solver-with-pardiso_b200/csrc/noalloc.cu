@@ -81,6 +81,7 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
     s.cpy = c->d_cpy;
     s.planes = scratch;
     s.R = 1;
+    s.dxy = nullptr;
     s.status = c->d_status;
     rc = launch_sweep(c->c64, s, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: sweep launch");

@@ -332,6 +332,20 @@ int ctx_setup_grid(helm3d_ctx *c) {
         (rc = upload_c64(c, &c->d_cmy64, c->cmy, "cmy64")) || (rc = upload_c64(c, &c->d_cpy64, c->cpy, "cpy64")) ||
         (rc = upload_c64(c, &c->d_cmz64, c->cmz, "cmz64")) || (rc = upload_c64(c, &c->d_cpz64, c->cpz, "cpz64")))
         return rc;
+    // alpha_x(i) alpha_y(j) and conj(1 / (alpha_x(i) alpha_y(j))): the
+    // symmetrizing scale of the 2D systems used by the adjoint sweep
+    if (o.mode == HELM3D_MODE_N) {
+        std::vector<zc> dxy((size_t)2 * ny * nx);
+        for (int j = 0; j < ny; j++) {
+            const zc ay = alpha(ny, g.pml_y, (double)j, w);
+            for (int i = 0; i < nx; i++) {
+                const zc d = alpha(nx, g.pml_x, (double)i, w) * ay;
+                dxy[(size_t)j * nx + i] = d;
+                dxy[((size_t)ny + j) * nx + i] = std::conj(1.0 / d);
+            }
+        }
+        if ((rc = upload_c(c, &c->d_dxy, dxy, "alpha_x alpha_y"))) return rc;
+    }
     // per-mode complex shift added to the 2D diagonal: -kz^2 (FFT) or the
     // eigenvalue lambda_k of the z operator (PML eigenbasis)
     c->zeig = (o.mode == HELM3D_MODE_N && o.z_transform == HELM3D_ZT_PML_EIGEN);
@@ -341,8 +355,17 @@ int ctx_setup_grid(helm3d_ctx *c) {
         if (!zpml_eigen(c->cmz, c->cpz, c->zshift, c->zW, c->zWi, &resid))
             return set_error(c, HELM3D_ERR_ARG, "eigen-decomposition of the z operator failed (residual " +
                                                     std::to_string(resid) + ")");
+        // conjugate transposes for the adjoint preconditioner Wi^H D^{-H} W^H
+        std::vector<zc> wh((size_t)nz * nz), wih((size_t)nz * nz);
+        for (int a = 0; a < nz; a++)
+            for (int b = 0; b < nz; b++) {
+                wh[(size_t)a * nz + b] = std::conj(c->zW[(size_t)b * nz + a]);
+                wih[(size_t)a * nz + b] = std::conj(c->zWi[(size_t)b * nz + a]);
+            }
         if ((rc = upload_c64(c, &c->d_zW64, c->zW, "z eigenvectors c128")) ||
-            (rc = upload_c64(c, &c->d_zWi64, c->zWi, "z eigenvectors inverse c128")))
+            (rc = upload_c64(c, &c->d_zWi64, c->zWi, "z eigenvectors inverse c128")) ||
+            (rc = upload_c64(c, &c->d_zWH64, wh, "z eigenvectors^H")) ||
+            (rc = upload_c64(c, &c->d_zWiH64, wih, "z eigenvectors inverse^H")))
             return rc;
     } else {
         for (int k = 0; k < nz; k++) c->zshift[k] = -c->kz2[k];

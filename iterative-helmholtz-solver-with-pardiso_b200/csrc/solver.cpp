@@ -124,7 +124,7 @@ static PlaneLayout layout(helm3d_ctx *c, int R) {
     return PlaneLayout{c->grid.nx, c->grid.ny, c->grid.nz, R, c->plane};
 }
 
-static SweepArgs sweep_args(helm3d_ctx *c, int R) {
+static SweepArgs sweep_args(helm3d_ctx *c, int R, bool adjoint) {
     SweepArgs s;
     s.n = c->grid.nx;
     s.ny = c->grid.ny;
@@ -135,6 +135,7 @@ static SweepArgs sweep_args(helm3d_ctx *c, int R) {
     s.cpy = c->d_cpy;
     s.planes = c->d_planes;
     s.R = R;
+    s.dxy = adjoint ? c->d_dxy : nullptr;
     s.status = c->d_status;
     return s;
 }
@@ -144,27 +145,46 @@ static int check_batch(helm3d_ctx *c, int R) {
     return HELM3D_OK;
 }
 
-// planes = Z-transform(xscale sc_r x_r); per-kz block sweep in place
-static int prec_to_planes(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, int R) {
+// planes = Z-transform(xscale sc_r x_r); per-kz block sweep in place.
+// M^{-1} = T^{-1} diag_k(S_k^{-1}) T with T the z-FFT or Wi (eigenbasis);
+// M^{-H} = T^H diag_k(S_k^{-H}) T^{-H}: the same FFT pair (F^H = nz F^{-1}),
+// or W^H forward and Wi^H inverse.
+static int prec_to_planes(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, int R,
+                          bool adjoint) {
     RC(check_batch(c, R));
     RC(ensure_planes(c, R));
     const PlaneLayout L = layout(c, R);
     RC(timed(c, HELM3D_K_FFT_FWD, 1, [&] {
-        if (c->zeig) return launch_ztrans_forward(c->c64, x, xscale, sc, c->d_planes, L, c->d_zWi64, c->stream);
+        if (c->zeig)
+            return launch_ztrans_forward(c->c64, x, xscale, sc, c->d_planes, L, adjoint ? c->d_zWH64 : c->d_zWi64,
+                                         c->stream);
         return launch_fft_forward(c->c64, x, xscale, sc, c->d_planes, L, c->plan, c->d_tw, c->stream);
     }));
-    const SweepArgs s = sweep_args(c, R);
+    const SweepArgs s = sweep_args(c, R, adjoint);
     return timed(c, HELM3D_K_SWEEP, 1, [&] { return launch_sweep(c->c64, s, c->stream); });
 }
 
-int apply_prec(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y, int R) {
-    RC(prec_to_planes(c, x, xscale, sc, R));
+static int prec_common(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y,
+                       int R, bool adjoint) {
+    RC(prec_to_planes(c, x, xscale, sc, R, adjoint));
     const PlaneLayout L = layout(c, R);
     return timed(c, HELM3D_K_FFT_INV, 1, [&] {
-        if (c->zeig) return launch_ztrans_inverse(c->c64, c->d_planes, L, y, c->d_zW64, c->stream);
+        if (c->zeig)
+            return launch_ztrans_inverse(c->c64, c->d_planes, L, y, adjoint ? c->d_zWiH64 : c->d_zW64, c->stream);
         return launch_fft_inverse(c->c64, c->d_planes, L, y, c->plan, c->d_tw, 0, VecBatch{nullptr, 0}, 0.0,
                                   kNoScale, nullptr, c->stream);
     });
+}
+
+int apply_prec(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y, int R) {
+    return prec_common(c, x, xscale, sc, y, R, false);
+}
+
+int apply_prec_adjoint(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc, const VecBatch &y,
+                       int R) {
+    if (c->opts.mode != HELM3D_MODE_N || !c->d_dxy)
+        return set_error(c, HELM3D_ERR_ARG, "adjoint preconditioner is mode N only");
+    return prec_common(c, x, xscale, sc, y, R, true);
 }
 
 static StencilArgs stencil_args(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &sc,
@@ -198,7 +218,7 @@ int apply_op(helm3d_ctx *c, const VecBatch &x, double xscale, const ScaleBatch &
         return timed(c, HELM3D_K_STENCIL, 1, [&] { return launch_stencil(a, false, c->stream); });
     }
     // mode R: y = s x - dL * L0^{-1}(s x), dL fused into the inverse FFT
-    RC(prec_to_planes(c, x, xscale, sc, R));
+    RC(prec_to_planes(c, x, xscale, sc, R, false));
     const PlaneLayout L = layout(c, R);
     return timed(c, HELM3D_K_FFT_INV, 1, [&] {
         return launch_fft_inverse(c->c64, c->d_planes, L, y, c->plan, c->d_tw, 1, x, xscale, sc, c->d_dl,
@@ -443,11 +463,15 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, hel
             const ScaleBatch vsj{c->d_vs + j, M2};
             if (flexible) {
                 const VecBatch zj{Z + (size_t)j * N, ldZ};
-                // the adjoint system is preconditioned by M^{-1} as well
-                // (flexible FGMRES admits any preconditioner)
-                RC(apply_prec(c, Vj, 1.0, vsj, zj, B));
-                if (adjoint) RC(apply_op_adjoint(c, zj, 1.0, kNoScale, w, B));
-                else RC(apply_op(c, zj, 1.0, kNoScale, w, B));
+                if (adjoint) {
+                    // A^H M^{-H} = (M^{-1} A)^H: the adjoint of the forward
+                    // preconditioned operator, with the same singular values
+                    RC(apply_prec_adjoint(c, Vj, 1.0, vsj, zj, B));
+                    RC(apply_op_adjoint(c, zj, 1.0, kNoScale, w, B));
+                } else {
+                    RC(apply_prec(c, Vj, 1.0, vsj, zj, B));
+                    RC(apply_op(c, zj, 1.0, kNoScale, w, B));
+                }
             } else {
                 RC(apply_op(c, Vj, 1.0, vsj, w, B));
             }

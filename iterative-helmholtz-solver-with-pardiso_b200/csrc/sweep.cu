@@ -36,6 +36,7 @@ template <typename R> struct SweepK {
     const cplx<R> *Gt;
     const cplx<R> *cmy, *cpy;
     cplx<R> *planes;
+    const cplx<R> *dxy;  // adjoint: [2][ny][n] = alpha_x alpha_y, conj(1 / (alpha_x alpha_y))
     int rows_per_stage;  // rows of G^T per ring stage
     int nstage;          // ring depth
     uint32_t stage_bytes;
@@ -62,8 +63,24 @@ __device__ __forceinline__ const cplx<R> *stage_src(const SweepK<R> &a, int kz, 
     return a.Gt + (((long)kz * a.ny + line) * a.n + r0) * (long)a.ldg;
 }
 
-// G groups of lanes split the rows m of each stage; RR right-hand sides
-template <typename R, int G, int RR>
+// G groups of lanes split the rows m of each stage; RR right-hand sides.
+// ADJ: the conjugate-transposed solve S^{-H} v = conj(Dxy)^{-1} conj(S^{-1}
+// (Dxy conj(v))), Dxy = diag(alpha_x(i) alpha_y(j)): Dxy^{-1} S is complex
+// symmetric (every coupling is alpha(node) alpha(half node) / h^2), so the
+// same factor serves; the input is scaled and conjugated where it is loaded
+// and the output where it is stored.
+template <typename R, bool ADJ>
+__device__ __forceinline__ cplx<R> adj_in(const SweepK<R> &a, int line, int i, cplx<R> f) {
+    if (!ADJ) return f;
+    return cmul(a.dxy[(long)line * a.n + i], mkc<R>(f.x, -f.y));
+}
+template <typename R, bool ADJ>
+__device__ __forceinline__ cplx<R> adj_out(const SweepK<R> &a, int line, int i, cplx<R> x) {
+    if (!ADJ) return x;
+    return cmul(mkc<R>(x.x, -x.y), a.dxy[(long)(a.ny + line) * a.n + i]);
+}
+
+template <typename R, int G, int RR, bool ADJ>
 __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kernel(SweepK<R> a) {
     typedef cplx<R> Cx;
     constexpr int RW = 32 / G;  // rows of y per warp
@@ -88,7 +105,7 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
     }
     for (int q = threadIdx.x; q < n * RR; q += blockDim.x) {  // v of line 0: f_0
         const int m = q / RR, r = q - (q / RR) * RR;
-        vbuf[q] = r < Rn ? P[(long)r * n + m] : mkc<R>(0, 0);
+        vbuf[q] = r < Rn ? adj_in<R, ADJ>(a, 0, m, P[(long)r * n + m]) : mkc<R>(0, 0);
     }
     __syncthreads();
 
@@ -129,7 +146,7 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
         for (int r = 0; r < RR; r++) {
             pre[r] = mkc<R>(0, 0);
             if (own && g == 0 && r < Rn) {
-                if (fwd && line + 1 < ny) pre[r] = P[((long)(line + 1) * Rn + r) * n + i];
+                if (fwd && line + 1 < ny) pre[r] = adj_in<R, ADJ>(a, line + 1, i, P[((long)(line + 1) * Rn + r) * n + i]);
                 else if (!fwd) pre[r] = P[((long)line * Rn + r) * n + i];
             }
         }
@@ -172,14 +189,17 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
             for (int r = 0; r < RR; r++) {
                 if (r >= Rn) break;
                 Cx out, vn;
+                bool last;  // out is the final x of this line
                 if (fwd) {
                     out = acc[r];                                          // y_line
-                    vn = (line + 1 < ny) ? cfms(cn, out, pre[r]) : out;  // f_{line+1} - cmy y_line, or x_{ny-1}
+                    last = line + 1 == ny;
+                    vn = last ? out : cfms(cn, out, pre[r]);               // f_{line+1} - cmy y_line, or x_{ny-1}
                 } else {
                     out = cfms(cp, acc[r], pre[r]);                        // x_line = y_line - cpy G x_{line+1}
+                    last = true;
                     vn = out;
                 }
-                P[((long)line * Rn + r) * n + i] = out;
+                P[((long)line * Rn + r) * n + i] = last ? adj_out<R, ADJ>(a, line, i, out) : out;
                 vnext[(size_t)i * RR + r] = vn;
             }
         }
@@ -187,7 +207,7 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
     }
 }
 
-template <typename R, int G, int RR> static int sweep_impl(const SweepArgs &sa, cudaStream_t st) {
+template <typename R, int G, int RR, bool ADJ> static int sweep_impl(const SweepArgs &sa, cudaStream_t st) {
     typedef cplx<R> Cx;
     SweepK<R> k;
     k.n = sa.n;
@@ -198,6 +218,7 @@ template <typename R, int G, int RR> static int sweep_impl(const SweepArgs &sa, 
     k.cmy = (const Cx *)sa.cmy;
     k.cpy = (const Cx *)sa.cpy;
     k.planes = (Cx *)sa.planes;
+    k.dxy = (const Cx *)sa.dxy;
     k.status = sa.status;
     const size_t vbytes = sizeof(Cx) * 2 * (size_t)sa.n * RR;
     const size_t budget = device_info().smem_optin - vbytes - 1024;
@@ -214,32 +235,36 @@ template <typename R, int G, int RR> static int sweep_impl(const SweepArgs &sa, 
     if (nst < 2) return HELM3D_ERR_ARG;
     k.nstage = nst;
     const size_t smem = (size_t)nst * k.stage_bytes + vbytes + 2 * nst * sizeof(uint64_t);
-    auto kern = sweep_kernel<R, G, RR>;
+    auto kern = sweep_kernel<R, G, RR, ADJ>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return HELM3D_ERR_CUDA;
     kern<<<dim3((unsigned)sa.nz), (kSweepConsumerWarps + 1) * 32, smem, st>>>(k);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
-template <typename R, int G> static int sweep_rr(const SweepArgs &sa, cudaStream_t s) {
-    if (sa.R <= 1) return sweep_impl<R, G, 1>(sa, s);
-    if (sa.R <= 2) return sweep_impl<R, G, 2>(sa, s);
-    if (sa.R <= 4) return sweep_impl<R, G, 4>(sa, s);
-    if (sa.R <= 8) return sweep_impl<R, G, 8>(sa, s);
-    return sweep_impl<R, G, 16>(sa, s);
+template <typename R, int G, bool ADJ> static int sweep_rr(const SweepArgs &sa, cudaStream_t s) {
+    if (sa.R <= 1) return sweep_impl<R, G, 1, ADJ>(sa, s);
+    if (sa.R <= 2) return sweep_impl<R, G, 2, ADJ>(sa, s);
+    if (sa.R <= 4) return sweep_impl<R, G, 4, ADJ>(sa, s);
+    if (sa.R <= 8) return sweep_impl<R, G, 8, ADJ>(sa, s);
+    return sweep_impl<R, G, 16, ADJ>(sa, s);
+}
+
+template <typename R, int G> static int sweep_g(const SweepArgs &sa, cudaStream_t s) {
+    return sa.dxy ? sweep_rr<R, G, true>(sa, s) : sweep_rr<R, G, false>(sa, s);
 }
 
 int launch_sweep(bool c64, const SweepArgs &sa, cudaStream_t s) {
     if (sa.n < 1 || sa.n > kSweepMaxN || sa.R < 1 || sa.R > kMaxBatch) return HELM3D_ERR_ARG;
     const int g = sa.n <= 64 ? 4 : (sa.n <= 128 ? 2 : 1);
     if (c64) {
-        if (g == 4) return sweep_rr<float, 4>(sa, s);
-        if (g == 2) return sweep_rr<float, 2>(sa, s);
-        return sweep_rr<float, 1>(sa, s);
+        if (g == 4) return sweep_g<float, 4>(sa, s);
+        if (g == 2) return sweep_g<float, 2>(sa, s);
+        return sweep_g<float, 1>(sa, s);
     }
-    if (g == 4) return sweep_rr<double, 4>(sa, s);
-    if (g == 2) return sweep_rr<double, 2>(sa, s);
-    return sweep_rr<double, 1>(sa, s);
+    if (g == 4) return sweep_g<double, 4>(sa, s);
+    if (g == 2) return sweep_g<double, 2>(sa, s);
+    return sweep_g<double, 1>(sa, s);
 }
 
 }  // namespace h3d

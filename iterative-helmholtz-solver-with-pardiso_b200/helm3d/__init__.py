@@ -65,6 +65,8 @@ _sig = {
     "helm3d_apply_op": (ctypes.c_int, [_vp, _vp, _vp]),
     "helm3d_apply_op_adjoint": (ctypes.c_int, [_vp, _vp, _vp]),
     "helm3d_apply_prec": (ctypes.c_int, [_vp, _vp, _vp]),
+    "helm3d_apply_prec_adjoint": (ctypes.c_int, [_vp, _vp, _vp]),
+    "helm3d_apply_prec_noalloc": (ctypes.c_int, [_vp, _vp, _vp]),
     "helm3d_misfit_grad": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp,
                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(Stats)]),
     "helm3d_set_stream": (ctypes.c_int, [_vp, _vp]),
@@ -210,6 +212,38 @@ class Solver:
 
     def apply_prec(self, x):
         return self._apply(lib.helm3d_apply_prec, x, "apply_prec")
+
+    def apply_prec_adjoint(self, x):
+        return self._apply(lib.helm3d_apply_prec_adjoint, x, "apply_prec_adjoint")
+
+    def misfit_grad(self, f, recv, data, nsrc: int | None = None, grad=None, allow_not_converged=False):
+        """(J, dJ/ds2) for J = 1/2 sum_s ||u_s[recv] - data_s||^2, A u_s = f_s.
+
+        f: (nsrc, nz, ny, nx) complex128, recv: int64 linear indices, data:
+        (nsrc, nrecv) complex128; NumPy arrays (host) or torch tensors
+        (device).  The gradient comes back like f (a float64 tensor on f's
+        device, or a NumPy array)."""
+        f = _c128(f)
+        nsrc = int(f.shape[0]) if nsrc is None else nsrc
+        if hasattr(recv, "data_ptr"):
+            recv_c = recv.contiguous()
+        else:
+            recv_c = np.ascontiguousarray(recv, dtype=np.int64)
+        data_c = _c128(data)
+        if grad is None:
+            if hasattr(f, "data_ptr"):
+                import torch
+                grad = torch.empty(self.shape, dtype=torch.float64, device=f.device)
+            else:
+                grad = np.empty(self.shape, dtype=np.float64)
+        J = ctypes.c_double()
+        st = Stats()
+        rc = lib.helm3d_misfit_grad(self.h, _ptr(f), nsrc, _ptr(recv_c), int(recv_c.shape[0]), _ptr(data_c),
+                                    _ptr(grad), ctypes.byref(J), ctypes.byref(st))
+        if rc != OK and not (allow_not_converged and rc == ERR_NOT_CONVERGED):
+            self._err(rc, "misfit_grad")
+        self.last_stats = st
+        return J.value, grad
 
     def set_medium(self, s2):
         s2 = s2 if hasattr(s2, "data_ptr") else np.ascontiguousarray(s2, dtype=np.float64)

@@ -143,12 +143,35 @@ class ModeN:
         return np.fft.ifft(out, axis=0)
 
     def apply_prec_adjoint(self, v: np.ndarray) -> np.ndarray:
-        """M^H v: the FFT pair is unitary up to 1/nz, so M^H = F^H diag(M_kz^H) F / nz."""
-        vh = np.fft.fft(v.reshape(self.shape), axis=0)
+        """(M^{-1})^H v.  FFT: M^{-1} = F^{-1} D^{-1} F and F^H = nz F^{-1}, so
+        (M^{-1})^H = F^{-1} D^{-H} F; eigenbasis: (W D^{-1} Wi)^H = Wi^H D^{-H} W^H."""
+        if self.zW is not None:
+            vh = np.tensordot(self.zW.conj().T, v.reshape(self.shape), axes=(1, 0))
+        else:
+            vh = np.fft.fft(v.reshape(self.shape), axis=0)
         out = np.empty_like(vh)
         for k in range(self.shape[0]):
             out[k] = self.lus[k].solve(vh[k].ravel(), trans="H").reshape(vh[k].shape)
+        if self.zW is not None:
+            return np.tensordot(self.zWi.conj().T, out, axes=(1, 0))
         return np.fft.ifft(out, axis=0)
+
+    # ------------------------------------------------- sparse A and gradient
+    def assemble_a(self, s2: np.ndarray | None = None):
+        """A as a sparse matrix (Kronecker sum of the 1D PML operators plus
+        the mass term), unknowns ordered (z, y, x) with x fastest."""
+        import scipy.sparse as sp
+        p = self.prob
+        s2 = p.s2 if s2 is None else s2
+
+        def t1(name):
+            cm, cp = self.coef[name]
+            return sp.diags([cm[1:], -(cm + cp), cp[:-1]], [-1, 0, 1], format="csr")
+
+        ix, iy, iz = (sp.identity(n, format="csr") for n in (p.nx, p.ny, p.nz))
+        a = sp.kron(iz, sp.kron(iy, t1("x"))) + sp.kron(iz, sp.kron(t1("y"), ix)) + sp.kron(t1("z"), sp.kron(iy, ix))
+        a = a + sp.diags((p.omega ** 2) * complex(1.0, p.beta_phys) * s2.ravel())
+        return a.tocsc()
 
 
 def zpml_eigen(cm: np.ndarray, cp: np.ndarray):
@@ -263,3 +286,54 @@ def fgmres(apply_a, apply_m, f: np.ndarray, tol: float = 1e-8, m: int = 20, max_
         k = jlast + 1
         y = np.linalg.solve(np.triu(H[:k, :k]), gv[:k])
         x = x + np.array(Z[:k]).T @ y
+
+
+# ------------------------------------------------------------ misfit gradient
+def misfit(on: ModeN, F: np.ndarray, recv: np.ndarray, data: np.ndarray, s2: np.ndarray | None = None) -> float:
+    """J = 1/2 sum_s ||P u_s - d_s||^2 with u_s from a sparse direct solve."""
+    import scipy.sparse.linalg as spla
+    lu = spla.splu(on.assemble_a(s2))
+    j = 0.0
+    for s in range(len(F)):
+        r = lu.solve(F[s].ravel())[recv] - data[s]
+        j += 0.5 * float(np.vdot(r, r).real)
+    return j
+
+
+def misfit_grad(on: ModeN, F: np.ndarray, recv: np.ndarray, data: np.ndarray, solver: str = "direct",
+                tol: float = 1e-12):
+    """Gradient of J with respect to s2 from two solves per source: A u = f and
+    A^H lam = P^T (d - P u); dJ/ds2 = sum_s Re(conj(lam_s) omega^2 (1 + i beta) u_s).
+    solver "direct": sparse LU; "fgmres": the preconditioned FGMRES pair."""
+    import scipy.sparse.linalg as spla
+    p = on.prob
+    dA = (p.omega ** 2) * complex(1.0, p.beta_phys)
+    g = np.zeros(on.shape)
+    j = 0.0
+    lu = spla.splu(on.assemble_a()) if solver == "direct" else None
+    for s in range(len(F)):
+        if lu is not None:
+            u = lu.solve(F[s].ravel())
+        else:
+            u = fgmres(on.apply_a, on.apply_prec, F[s], tol=tol, m=40, max_iter=5000).x.ravel()
+        r = u[recv] - data[s]
+        j += 0.5 * float(np.vdot(r, r).real)
+        adj = np.zeros(u.size, dtype=np.complex128)
+        np.add.at(adj, recv, -r)
+        if lu is not None:
+            lam = lu.solve(adj, trans="H")
+        else:
+            lam = fgmres(on.apply_a_adjoint, on.apply_prec_adjoint, adj.reshape(on.shape), tol=tol, m=40,
+                         max_iter=5000).x.ravel()
+        g += (np.conj(lam) * dA * u).real.reshape(on.shape)
+    return j, g
+
+
+def receiver_plane(prob: Problem, stride: int = 1, depth: int = 1) -> np.ndarray:
+    """Linear indices of a receiver plane at the top of the interior: the
+    y-row pml + depth, interior x and z (every `stride`-th point)."""
+    j = prob.pml + depth
+    ks = np.arange(prob.pml, prob.nz - prob.pml, stride)
+    is_ = np.arange(prob.pml, prob.nx - prob.pml, stride)
+    kk, ii = np.meshgrid(ks, is_, indexing="ij")
+    return ((kk * prob.ny + j) * prob.nx + ii).ravel().astype(np.int64)
