@@ -3,21 +3,23 @@
 Workload (default): the 128^3 heterogeneous medium (1500 -> 3000 m/s linear
 depth gradient along y, three seeded Gaussian anomalies of +-20 %, radius
 8-15 h), h = 10 m, 12-point PML on every face, 8 points per minimum
-wavelength, a seeded Gaussian point source; the 7-point PML operator solved
-by FGMRES(20) to ||f - A u|| / ||f|| <= 1e-8, preconditioned by the FFT-z /
-per-kz block LU (complex shift 0.25).  Inputs are synthetic (seeded
-splitmix64), no dataset is read.
+wavelength, 16 seeded Gaussian point sources; the 7-point PML operator
+solved by FGMRES(20) to ||f - A u|| / ||f|| <= 1e-8 for every source.
+Inputs are synthetic (seeded splitmix64), no dataset is read.
 
-One step = one complete solve: set-up + block LU factor of all 128 kz
-systems + FGMRES iterations to 1e-8.  `value` is seconds per solve with the
-medium and the right-hand side resident on the device, timed with CUDA
-events on the solver's stream; the headline path factors and applies the
-preconditioner in complex64 (outer loop complex128); the plain complex128
-path is timed beside it (`fp64_plain`).  `e2e` repeats the headline solve
-through the C ABI with host buffers (medium and RHS copied in, solution
-copied out inside the timed region).
+One step = one medium: set-up + block LU factor of all kz systems + one
+lockstep batched FGMRES over the 16 sources, with the preconditioner in
+complex64 and the z-transform in the PML eigenbasis (outer loop, operator
+and Gram-Schmidt in complex128).  `value` is seconds per source-solve (step
+time / 16) with the medium and the sources resident on the device, timed
+with CUDA events on the solver's stream.  Beside it: the same preconditioner
+with one source per step, the FFT-z preconditioner (the reference's method)
+in complex64, and the plain complex128 FFT-z path with one source per step
+(`fp64_plain`, the drop-in baseline).  `e2e` repeats the headline step
+through the C ABI with pinned host buffers (medium and sources copied in,
+solutions copied out inside the timed region).
 
-    python bench.py [--steps K] [--warmup W] [--impl ours|reference] [--n 128]
+    python bench.py [--steps K] [--warmup W] [--impl ours|reference] [--grid 128]
     torchrun --nproc-per-node N bench.py --gpus N     (N independent replicas)
 """
 from __future__ import annotations
@@ -44,15 +46,19 @@ METRIC = "time to 1e-8 residual per 3D solve: FP32-precond/batched vs plain FP64
 TOL = 1e-8
 RESTART = 20
 BETA_PREC = 0.25
-# FGMRES iterations the complex128 path needs at the 128^3 workload (measured
-# on a B200 with this bench); the CPU port times a sample of iterations and
-# scales to this count.
-ITERS_128 = None
+BATCH = 16
+# FGMRES iterations the complex128 FFT-z path needs at the 128^3 workload
+# (measured on a B200 with this bench: 513); the CPU port times a sample of
+# iterations and scales to this count.
+ITERS_128 = 513
 
 
-def workload(n: int):
+def workload(n: int, nsrc: int = 1):
+    """The 128^3 heterogeneous medium recipe at size n with nsrc seeded
+    sources (the medium does not depend on nsrc; source 0 is the same)."""
     from oracle import media
-    p = media.config_c2(n=n, pml=12, seed=2024)
+    p = media.layered_medium(n, n, n, 10.0, 12, 2024, ppw=8.0, n_sources=nsrc)
+    p.meta["config"] = "C2"
     return p
 
 
@@ -121,6 +127,34 @@ class Clocks:
         return out
 
 
+def dist_max(dist, x: float, device=None) -> float:
+    """Max of a per-rank float over all ranks (identity without a process group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def init_dist(world: int):
+    """One process per GPU over NCCL (gloo where no GPU is visible), with a
+    short timeout so that ranks waiting on a dead peer end with an error."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as tdist
+    if torch.cuda.is_available():
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        backend = "nccl"
+    else:
+        backend = "gloo"
+    tdist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return tdist
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args, rank, world, dist):
     import torch
@@ -129,19 +163,19 @@ def run_ours(args, rank, world, dist):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    p = workload(args.n)
-    f_host = p.rhs(0)
+    p = workload(args.n, BATCH)
+    F_host = np.stack([p.rhs(i) for i in range(BATCH)])
     s2_host = np.ascontiguousarray(p.s2)
     grid = helm3d.grid_mode_n(p.nx, p.ny, p.nz, p.h, p.pml, p.omega)
     N = p.nx * p.ny * p.nz
     # a dedicated stream: the solver's launches and the timing events share it
     stream = torch.cuda.Stream(dev)
 
-    f_dev = torch.from_numpy(f_host).to(dev)
+    F_dev = torch.from_numpy(F_host).to(dev)
     s2_dev = torch.from_numpy(s2_host).to(dev)
-    u_dev = torch.empty_like(f_dev)
+    U_dev = torch.empty_like(F_dev)
 
-    def make(prec, zt=0):
+    def make(prec, zt):
         o = helm3d.default_opts(precision=prec, restart=RESTART, tol=TOL, beta_prec=BETA_PREC, max_iter=20000,
                                 device=dev.index, z_transform=zt)
         s = helm3d.Solver(grid, s2_dev, o)
@@ -154,141 +188,144 @@ def run_ours(args, rank, world, dist):
         torch.cuda.synchronize(dev)
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return dist_max(dist, x, dev)
 
-    def timed_solves(s, steps, warmup):
-        its = []
+    def step(s, nrhs, s2=s2_dev, F=F_dev, U=U_dev):
+        s.set_medium(s2)
+        s.solve(F[:nrhs], nrhs=nrhs, u=U[:nrhs], allow_not_converged=True)
+
+    def timed_steps(s, nrhs, steps, warmup):
+        """ms per step (max over ranks), iterations per source of the last
+        step, launches in the timed region, last stats."""
         for _ in range(warmup):
-            s.set_medium(s2_dev)
-            s.solve(f_dev, u=u_dev, allow_not_converged=True)
+            step(s, nrhs)
         barrier()
         launches0 = s.kernel_launches
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(steps):
-            s.set_medium(s2_dev)
-            s.solve(f_dev, u=u_dev, allow_not_converged=True)
-            its.append(s.last_stats.iterations)
+            step(s, nrhs)
         e1.record(stream)
         barrier()
-        ms = e0.elapsed_time(e1)
-        return max_over_ranks(ms) / steps, its, s.kernel_launches - launches0, s.last_stats
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps)
+        st = s.last_stats
+        return ms, st.iterations / nrhs, s.kernel_launches - launches0, st
 
-    # headline: complex64 preconditioner
-    s32 = make(helm3d.PREC_C64)
+    def profiled(s, nrhs):
+        s.profile(True)
+        step(s, nrhs)
+        prof = s.profile_read()
+        s.profile(False)
+        return prof
+
+    # headline: eigenbasis z-transform, complex64 preconditioner, 16 sources per step
+    sh = make(helm3d.PREC_C64, helm3d.ZT_PML_EIGEN)
     clocks = Clocks(dev.index)
     clocks.start()
-    ms32, its32, launches32, st32 = timed_solves(s32, args.steps, args.warmup)
+    time.sleep(1.5)   # let the sampler start up before the timed region
+    ms_h, its_h, launches_h, st_h = timed_steps(sh, BATCH, args.steps, args.warmup)
     clk = clocks.stop()
+    prof = profiled(sh, BATCH)
+    relres_h = sh.last_stats.relres
+    U_h = U_dev.clone()
 
-    # profile pass: per-kernel-family device time of one solve
-    s32.profile(True)
-    s32.set_medium(s2_dev)
-    s32.solve(f_dev, u=u_dev, allow_not_converged=True)
-    prof = s32.profile_read()
-    s32.profile(False)
-    relres32 = s32.last_stats.relres
-
-    # e2e through the C ABI with host buffers (pinned)
-    f_pin = torch.from_numpy(f_host).pin_memory()
+    # e2e through the C ABI with host buffers (pinned): medium and sources in,
+    # solutions out, every step
+    F_pin = torch.from_numpy(F_host).pin_memory()
     s2_pin = torch.from_numpy(s2_host).pin_memory()
-    u_pin = torch.empty_like(f_pin).pin_memory()
-    for _ in range(1):
-        s32.set_medium(s2_pin)
-        s32.solve(f_pin, u=u_pin, allow_not_converged=True)
+    U_pin = torch.empty_like(F_pin).pin_memory()
+    step(sh, BATCH, s2_pin, F_pin, U_pin)
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        s32.set_medium(s2_pin)
-        s32.solve(f_pin, u=u_pin, allow_not_converged=True)
+        step(sh, BATCH, s2_pin, F_pin, U_pin)
     e1.record(stream)
     barrier()
-    e2e_s = max_over_ranks(e0.elapsed_time(e1) / 1e3 / args.steps)
-    # error of the FP32-preconditioned solution against the FP64 path
-    u32 = u_dev.clone()
-    s32.close()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    # the same preconditioner, one source per step
+    ms_1, its_1, _, _ = timed_steps(sh, 1, args.steps, 1)
+    sh.close()
 
-    # plain complex128 path
-    s64 = make(helm3d.PREC_C128)
-    ms64, its64, launches64, st64 = timed_solves(s64, max(1, args.steps // 2), 1)
-    u64 = u_dev.clone()
-    relerr_vs_fp64 = float(torch.linalg.vector_norm(u32 - u64) / torch.linalg.vector_norm(u64))
-    relres64 = s64.last_stats.relres
+    # the reference's method (FFT-z) with the complex64 preconditioner, one source
+    sf = make(helm3d.PREC_C64, helm3d.ZT_FFT)
+    ms_f, its_f, _, st_f = timed_steps(sf, 1, max(1, args.steps // 2), 1)
+    relres_f = st_f.relres
+    sf.close()
+
+    # plain complex128 FFT-z path, one source per step
+    s64 = make(helm3d.PREC_C128, helm3d.ZT_FFT)
+    ms64, its64, _, st64 = timed_steps(s64, 1, max(1, args.steps // 2), 1)
+    u64 = U_dev[0].clone()
+    relres64 = st64.relres
     s64.close()
-
-    # the same solve with the PML-eigenbasis z-transform (c64 and c128)
-    zeig = {}
-    for prec, key in ((helm3d.PREC_C64, "c64"), (helm3d.PREC_C128, "c128")):
-        sz = make(prec, helm3d.ZT_PML_EIGEN)
-        msz, itsz, _, _ = timed_solves(sz, args.steps, 1)
-        sz.profile(True)
-        sz.set_medium(s2_dev)
-        sz.solve(f_dev, u=u_dev, allow_not_converged=True)
-        pz = sz.profile_read()
-        uz = u_dev.clone()
-        zeig[key] = {"value": msz / 1e3 / world, "unit": "s", "iterations": itsz[-1] if itsz else None,
-                     "relres": sz.last_stats.relres,
-                     "relerr_vs_fft_fp64_path": float(torch.linalg.vector_norm(uz - u64) / torch.linalg.vector_norm(u64)),
-                     "kernel_ms_per_solve": {k: round(v[0], 3) for k, v in pz.items()}}
-        sz.close()
+    relerr = float(torch.linalg.vector_norm(U_h[0] - u64) / torch.linalg.vector_norm(u64))
 
     if rank != 0:
         return None
 
-    # roofline of the dominant kernel (the block sweep): G^T read twice per
-    # launch plus the planes read/written forward and backward
+    # roofline of the dominant single kernel of the headline step (the
+    # preconditioner kernels; the Krylov family is several kernels)
     e = 8
-    sweep_ms, sweep_n = prof["sweep"]
-    sweep_bytes = 2.0 * p.nz * p.ny * p.nx * p.nx * e + 4.0 * N * e
-    sweep_avg_s = (sweep_ms / max(1, sweep_n)) / 1e3
-    achieved = sweep_bytes / sweep_avg_s / 1e9 if sweep_avg_s > 0 else None
+    nbytes = {
+        # G^T read in both passes, planes of all sources read + written in both
+        "sweep": 2.0 * p.nz * p.ny * p.nx * p.nx * e + 4.0 * N * e * BATCH,
+        # x (complex128) in, planes (complex64) out; W from L2
+        "fft_fwd": (16.0 + e) * N * BATCH,
+        "fft_inv": (16.0 + e) * N * BATCH,
+        "stencil": (16.0 * 2 + 8.0) * N * BATCH,
+    }
+    top = max(nbytes, key=lambda k: prof[k][0])
+    k_ms, k_n = prof[top]
+    avg_s = (k_ms / max(1, k_n)) / 1e3
+    achieved = nbytes[top] / avg_s / 1e9 if avg_s > 0 else None
     peak, peak_kind = read_peaks()
     total_prof = sum(v[0] for v in prof.values())
+    per_src = ms_h / BATCH
     line = {
         "metric": METRIC,
-        "value": ms32 / 1e3 / world,
+        "value": per_src / 1e3 / world,
         "unit": "s",
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": ms32,
+        "ms_per_step": ms_h,
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "c64 preconditioner / c128 outer",
-        "data": "synthetic (seeded splitmix64 media and sources)",
+        "data": "synthetic (seeded splitmix64 medium and sources)",
         "config": {
-            "workload": f"{p.nx}^3 heterogeneous medium, PML 12, 8 ppw, Gaussian source; "
-                        f"one step = set-up + block LU factor + FGMRES({RESTART}) to 1e-8",
-            "n": p.nx, "pml": p.pml, "restart": RESTART, "tol": TOL, "beta_prec": BETA_PREC,
-            "l2": "inputs larger than L2 (factor 2.1 GB c64 / 4.3 GB c128, Krylov basis 0.7 GB)",
+            "workload": f"{p.nx}^3 heterogeneous medium, PML 12, 8 ppw, {BATCH} Gaussian sources; one step = "
+                        f"set-up + block LU factor + batched FGMRES({RESTART}) to 1e-8 for all sources; "
+                        f"value = step time / {BATCH}",
+            "n": p.nx, "pml": p.pml, "sources_per_step": BATCH, "restart": RESTART, "tol": TOL,
+            "beta_prec": BETA_PREC, "z_transform": "PML eigenbasis",
+            "l2": "inputs larger than L2 (factor 2.1 GB, sources 0.54 GB, Krylov bases 22 GB)",
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         },
-        "iterations": its32[-1] if its32 else None,
-        "relres": relres32,
-        "relerr_vs_fp64_path": relerr_vs_fp64,
-        "fp64_plain": {"value": ms64 / 1e3 / world, "unit": "s", "iterations": its64[-1] if its64 else None,
-                       "relres": relres64},
-        "speedup_vs_fp64_plain": (ms64 / ms32) if ms32 > 0 else None,
-        "zpml_eigen": zeig,
-        "e2e": {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": N * 8 + N * 16,
-                "d2h_bytes_per_step": N * 16},
-        "gpu_launches": int(launches32 / max(1, args.steps)) * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "sweep", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "solves_per_s": world * 1e3 / per_src,
+        "iterations_per_source": its_h,
+        "relres": relres_h,
+        "relerr_vs_fp64_plain": relerr,
+        "single_source": {"value": ms_1 / 1e3 / world, "unit": "s", "iterations": its_1},
+        "fft_z_c64_single": {"value": ms_f / 1e3 / world, "unit": "s", "iterations": its_f, "relres": relres_f},
+        "fp64_plain": {"value": ms64 / 1e3 / world, "unit": "s", "iterations": its64, "relres": relres64},
+        "speedup_vs_fp64_plain": (ms64 / per_src) if per_src > 0 else None,
+        "e2e": {"value": e2e_ms / BATCH / 1e3 / world, "unit": "s",
+                "h2d_bytes_per_step": N * 8 + BATCH * N * 16, "d2h_bytes_per_step": BATCH * N * 16},
+        "gpu_launches": int(launches_h),
+        "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                     "bytes_per_launch": sweep_bytes, "traffic": None},
-        "kernel_ms_per_solve": {k: round(v[0], 3) for k, v in prof.items()},
+                     "bytes_per_launch": nbytes[top], "traffic": None},
+        "kernel_ms_per_step": {k: round(v[0], 3) for k, v in prof.items()},
+        "kernel_launches_per_step": {k: int(v[1]) for k, v in prof.items()},
         "kernel_share": {k: round(v[0] / total_prof, 4) for k, v in prof.items()} if total_prof > 0 else None,
         "clocks": clk,
     }
-    return line, its64[-1] if its64 else None
+    return line, round(its64) if its64 else None
 
 
 # ------------------------------------------------------------ CPU baseline
@@ -375,8 +412,9 @@ def run_reference(args, rank):
         "higher_is_better": False,
         "dtype": "c128",
         "data": "synthetic (seeded splitmix64 media and sources)",
-        "config": {"workload": f"{p.nx}^3 heterogeneous medium, PML 12, 8 ppw, Gaussian source; FGMRES({RESTART}) "
-                               f"to 1e-8", "n": p.nx},
+        "config": {"workload": f"{p.nx}^3 heterogeneous medium, PML 12, 8 ppw, Gaussian source; the reference's "
+                               f"method (FFT-z + per-kz sparse LU, FGMRES({RESTART}) to 1e-8, complex128) per "
+                               f"source-solve", "n": p.nx},
         "cpu_baseline": base,
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -388,33 +426,25 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--grid", dest="n", type=int, default=128, help="grid points per axis")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as tdist
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-        dist = tdist
-
     if args.impl == "reference":
+        # the CPU reference runs on rank 0 only; the other ranks exit at once
         out = run_reference(args, rank)
         if rank == 0 and out is not None:
             print(json.dumps(out))
-    else:
-        res = run_ours(args, rank, world, dist)
-        if rank == 0 and res is not None:
-            line, its64 = res
-            if world == 1 and not args.no_cpu_baseline:
-                line["cpu_baseline"] = cpu_port_sample(args.n, its64, os.cpu_count() or 1)
-            print(json.dumps(line))
+        return
+    dist = init_dist(world)
+    res = run_ours(args, rank, world, dist)
+    if rank == 0 and res is not None:
+        line, its64 = res
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_port_sample(args.n, its64, os.cpu_count() or 1)
+        print(json.dumps(line))
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
