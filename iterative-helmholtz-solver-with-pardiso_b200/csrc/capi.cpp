@@ -3,6 +3,7 @@
 
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <algorithm>
 #include <new>
@@ -207,6 +208,9 @@ int helm3d_create(const helm3d_grid *grid, const double *s2, const helm3d_opts *
         (rc = cuda_check(c, cudaEventCreate(&c->ev1), "event")))
         return fail(rc);
     c->stream = c->own_stream;
+    // HELM3D_GRAPH=0 keeps the host-driven restart cycle (no CUDA graphs)
+    const char *genv = std::getenv("HELM3D_GRAPH");
+    c->use_graphs = !(genv && genv[0] == '0');
     auto t0 = std::chrono::steady_clock::now();
     if ((rc = ctx_setup_grid(c)) || (rc = ctx_setup_medium(c, s2, is_device_ptr(s2))) || (rc = ctx_factor(c)))
         return fail(rc);
@@ -419,6 +423,10 @@ int helm3d_destroy(helm3d_ctx *c) {
                     c->d_r, c->d_t, c->d_t2, c->d_bic, c->d_Fw, c->d_Uw};
     for (void *p : bufs)
         if (p) cudaFree(p);
+    for (float *p : c->d_ztc)
+        if (p) cudaFree(p);
+    for (auto &g : c->graphs) cudaGraphExecDestroy(g.exec);
+    if (c->d_arn) cudaFree(c->d_arn);
     for (auto &e : c->prof_ev) {
         cudaEventDestroy(e.a);
         cudaEventDestroy(e.b);

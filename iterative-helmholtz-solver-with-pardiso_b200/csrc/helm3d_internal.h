@@ -74,6 +74,16 @@ int launch_ztrans_forward(bool c64, const VecBatch &x, double scale, const Scale
 int launch_ztrans_inverse(bool c64, const void *planes, const PlaneLayout &L, const VecBatch &y, const double2 *W,
                           cudaStream_t s);
 
+// The same eigenbasis transforms for complex64 planes on the tensor cores
+// (tcgen05 kind::tf32, three TF32 products per real product): B is the matrix
+// prepared by ztc_prepare (real form, hi/lo split, tensor-core layout).
+bool ztc_supported(int nz);
+void ztc_prepare(const std::vector<std::complex<double>> &M, int nz, std::vector<float> &out);
+int launch_ztc_forward(const VecBatch &x, double scale, const ScaleBatch &sc, void *planes, const PlaneLayout &L,
+                       const float *B, int *status, cudaStream_t s);
+int launch_ztc_inverse(const void *planes, const PlaneLayout &L, const VecBatch &y, const float *B, int *status,
+                       cudaStream_t s);
+
 // Block-tridiagonal factor of all nz systems: G^T of every (kz, y-line).
 struct FactorArgs {
     int n, ny, nz, ldg;
@@ -128,15 +138,41 @@ struct Reduce {
     int rmax;
 };
 // out[r][i] = <vs_r[i] V_r[i], w_r>   (i < nv); with wnorm also out[r][nv].x = ||w_r||^2
+// (pred: when given and *pred == 0 on the device, the kernels do nothing)
 int launch_dots(const VecBatch &V, long ldv, const ScaleBatch &vs, int nv, const VecBatch &w, long N, int R,
-                const Reduce &red, double2 *out, long sOut, cudaStream_t s, bool wnorm = false);
+                const Reduce &red, double2 *out, long sOut, cudaStream_t s, bool wnorm = false,
+                const int *pred = nullptr);
 // w_r -= sum_i coef[r][i] vs_r[i] V_r[i]; post 1: out[r].x = ||w_r||^2
 int launch_update(const VecBatch &V, long ldv, const ScaleBatch &vs, int nv, const double2 *coef, long sCoef,
                   const VecBatch &w, long N, int R, int post, const Reduce &red, double2 *out, long sOut,
-                  cudaStream_t s);
-// x_r += sum_i y[r][i] zs_r[i] Z_r[i]
+                  cudaStream_t s, const int *pred = nullptr);
+// x_r += sum_i y[r][i] zs_r[i] Z_r[i]  (i < min(nzv, *nzv_dev) when nzv_dev is given)
 int launch_combine(const VecBatch &Z, long ldz, const ScaleBatch &zs, int nzv, const double2 *y, long sY,
-                   const VecBatch &x, long N, int R, cudaStream_t s);
+                   const VecBatch &x, long N, int R, cudaStream_t s, const int *nzv_dev = nullptr);
+
+// ------------------------------------------- device-side Arnoldi bookkeeping
+// Per right-hand side p of a lockstep batch of B (the host FGMRES state, on
+// the device so that a whole restart cycle runs without the host):
+struct ArnState {
+    double2 *H;        // [B][m+1][m] Hessenberg columns, Givens-rotated (upper triangle = R)
+    double2 *cs, *sn;  // [B][m] rotations
+    double2 *g;        // [B][m+1] rotated right-hand side (g[0] = beta on entry)
+    double *est;       // [B][m] |g[j+1]| / ||f|| after step j
+    double *nf, *tol;  // [B]
+    int *frozen, *k, *it, *max_iter;   // [B]
+    int *flags;        // [0] second Gram-Schmidt pass wanted, [1] second passes taken, [2] longest k, [3] error
+    int m, B;
+    double2 *h;        // Krylov scalars: [B][SH], h1 at 0, h2 at M2, norms at 2 M2, y at 3 M2
+    int SH, M2;
+    double *vs;        // basis scales [B][M2]
+};
+// flags[0] = any unfrozen p with ||w||^2 after the first pass < 1/2 of before
+int launch_reorth_check(const ArnState &a, int j, cudaStream_t s);
+// column j of H (h1 + h2 when flags[0]), rotations, g, est, frozen, k, it,
+// vs[j + 1]; sets `next` (if has_next) to "some p is still unfrozen"
+int launch_givens(const ArnState &a, int j, bool has_next, cudaGraphConditionalHandle next, cudaStream_t s);
+// y = R^{-1} g (k x k per p, zero padded to m) into h at 3 M2; flags[2] = max k
+int launch_backsub(const ArnState &a, cudaStream_t s);
 // out[r].x = ||x_r||^2 over the box [x0,x1) x [y0,y1) x [z0,z1)
 int launch_norm2_box(const VecBatch &x, int R, int nx, int ny, int nz, const int box[6], const Reduce &red,
                      double2 *out, long sOut, cudaStream_t s);
@@ -209,6 +245,9 @@ struct helm3d_ctx {
     void *d_zW = nullptr, *d_zWi = nullptr;                                        // P precision
     double2 *d_zW64 = nullptr, *d_zWi64 = nullptr;
     double2 *d_zWH64 = nullptr, *d_zWiH64 = nullptr;   // W^H, Wi^H (adjoint z-transforms)
+    // tensor-core forms of Wi, W, W^H, Wi^H (complex64 eigenbasis path)
+    bool ztc = false;
+    float *d_ztc[4] = {nullptr, nullptr, nullptr, nullptr};
     void *d_dxy = nullptr;         // [2][ny][nx] alpha_x alpha_y and conj(1 / (alpha_x alpha_y)), P precision
     double2 *d_cmx64 = nullptr, *d_cpx64 = nullptr, *d_cmy64 = nullptr, *d_cpy64 = nullptr;
     double2 *d_cmz64 = nullptr, *d_cpz64 = nullptr;
@@ -222,6 +261,16 @@ struct helm3d_ctx {
     size_t kry_bytes = 0;
     double2 *d_V = nullptr, *d_Z = nullptr;
     double2 *d_Fw = nullptr, *d_Uw = nullptr;   // packed right-hand sides / iterates of the active batch
+    void *d_arn = nullptr;                      // device-side Arnoldi state (ArnState arrays)
+    // restart cycles captured as CUDA graphs, one per (batch size, adjoint)
+    struct CycleGraph {
+        int B;
+        bool adjoint;
+        cudaGraphExec_t exec;
+        long long kernels_per_step, tail_kernels;
+    };
+    std::vector<CycleGraph> graphs;
+    bool use_graphs = true;
     size_t f_cap = 0, u_cap = 0;                // staging capacities (vectors) of d_f, d_u
     double *d_vs = nullptr;
     double2 *d_h = nullptr;        // small device scalars

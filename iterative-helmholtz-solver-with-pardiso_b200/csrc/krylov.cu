@@ -49,8 +49,9 @@ template <int CH> __device__ __forceinline__ void block_sum(double2 (&acc)[CH], 
 __global__ void __launch_bounds__(kRedThreads) dots_kernel(const double2 *__restrict__ V, long ldv, long sV,
                                                            const double *__restrict__ vs, long sVs, int nv,
                                                            const double2 *__restrict__ w, long sW, long N, int wnorm,
-                                                           double2 *__restrict__ partials, int cap) {
+                                                           double2 *__restrict__ partials, int cap, const int *pred) {
     __shared__ double2 sh[(kRedThreads / 32) * (kDotChunk + 1)];
+    if (pred && *pred == 0) return;
     const int r = blockIdx.y;
     V += r * sV;
     w += r * sW;
@@ -84,8 +85,10 @@ __global__ void __launch_bounds__(kRedThreads) dots_kernel(const double2 *__rest
 constexpr int kFinalThreads = 128;
 __global__ void __launch_bounds__(kFinalThreads) reduce_partials_kernel(const double2 *__restrict__ partials,
                                                                         int nblocks, int cap, int nv,
-                                                                        double2 *__restrict__ out, long sOut) {
+                                                                        double2 *__restrict__ out, long sOut,
+                                                                        const int *pred) {
     __shared__ double2 sh[kFinalThreads / 32];
+    if (pred && *pred == 0) return;
     const int i = blockIdx.x, r = blockIdx.y;
     if (i >= nv) return;
     partials += (long)r * nblocks * cap;
@@ -110,9 +113,11 @@ __global__ void __launch_bounds__(kRedThreads) update_kernel(const double2 *__re
                                                              const double *__restrict__ vs, long sVs, int nv,
                                                              const double2 *__restrict__ coef, long sCoef,
                                                              double2 *__restrict__ w, long sW, long N, int post,
-                                                             double2 *__restrict__ partials, int cap) {
+                                                             double2 *__restrict__ partials, int cap,
+                                                             const int *pred) {
     extern __shared__ double2 sc[];  // nv coefficients (coef * vs)
     __shared__ double2 sh[(kRedThreads / 32)];
+    if (pred && *pred == 0) return;
     const int r = blockIdx.y;
     V += r * sV;
     w += r * sW;
@@ -134,12 +139,14 @@ __global__ void __launch_bounds__(kRedThreads) update_kernel(const double2 *__re
     }
 }
 
-// x += sum_i y[i] zs[i] Z_i
+// x += sum_i y[i] zs[i] Z_i  (i < *nzv_dev when given, else nzv)
 __global__ void __launch_bounds__(kRedThreads) combine_kernel(const double2 *__restrict__ Z, long ldz, long sZ,
                                                               const double *__restrict__ zs, long sZs, int nzv,
                                                               const double2 *__restrict__ y, long sY,
-                                                              double2 *__restrict__ x, long sX, long N) {
+                                                              double2 *__restrict__ x, long sX, long N,
+                                                              const int *nzv_dev) {
     extern __shared__ double2 sc[];
+    if (nzv_dev) nzv = min(nzv, *nzv_dev);
     const int r = blockIdx.y;
     Z += r * sZ;
     y += r * sY;
@@ -228,31 +235,33 @@ static int grid_for(long N, int R = 1) {
 }
 
 int launch_dots(const VecBatch &V, long ldv, const ScaleBatch &vs, int nv, const VecBatch &w, long N, int R,
-                const Reduce &red, double2 *out, long sOut, cudaStream_t s, bool wnorm) {
+                const Reduce &red, double2 *out, long sOut, cudaStream_t s, bool wnorm, const int *pred) {
     const int nout = nv + (wnorm ? 1 : 0);
     if (nout > red.cap || R > red.rmax) return HELM3D_ERR_ARG;
     const int nb = red.nblocks;
     dots_kernel<<<dim3(nb, R), kRedThreads, 0, s>>>(V.p, ldv, V.stride, vs.p, vs.stride, nv, w.p, w.stride, N,
-                                                    wnorm ? 1 : 0, red.partials, red.cap);
-    reduce_partials_kernel<<<dim3(nout, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, nout, out, sOut);
+                                                    wnorm ? 1 : 0, red.partials, red.cap, pred);
+    reduce_partials_kernel<<<dim3(nout, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, nout, out, sOut,
+                                                                    pred);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
 int launch_update(const VecBatch &V, long ldv, const ScaleBatch &vs, int nv, const double2 *coef, long sCoef,
                   const VecBatch &w, long N, int R, int post, const Reduce &red, double2 *out, long sOut,
-                  cudaStream_t s) {
+                  cudaStream_t s, const int *pred) {
     if (R > red.rmax) return HELM3D_ERR_ARG;
     const int nb = post ? red.nblocks : grid_for(N, R);
     update_kernel<<<dim3(nb, R), kRedThreads, sizeof(double2) * (nv > 0 ? nv : 1), s>>>(
-        V.p, ldv, V.stride, vs.p, vs.stride, nv, coef, sCoef, w.p, w.stride, N, post, red.partials, red.cap);
-    if (post == 1) reduce_partials_kernel<<<dim3(1, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, 1, out, sOut);
+        V.p, ldv, V.stride, vs.p, vs.stride, nv, coef, sCoef, w.p, w.stride, N, post, red.partials, red.cap, pred);
+    if (post == 1)
+        reduce_partials_kernel<<<dim3(1, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, 1, out, sOut, pred);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
 int launch_combine(const VecBatch &Z, long ldz, const ScaleBatch &zs, int nzv, const double2 *y, long sY,
-                   const VecBatch &x, long N, int R, cudaStream_t s) {
+                   const VecBatch &x, long N, int R, cudaStream_t s, const int *nzv_dev) {
     combine_kernel<<<dim3(grid_for(N, R), R), kRedThreads, sizeof(double2) * (nzv > 0 ? nzv : 1), s>>>(
-        Z.p, ldz, Z.stride, zs.p, zs.stride, nzv, y, sY, x.p, x.stride, N);
+        Z.p, ldz, Z.stride, zs.p, zs.stride, nzv, y, sY, x.p, x.stride, N, nzv_dev);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
@@ -262,7 +271,8 @@ int launch_norm2_box(const VecBatch &x, int R, int nx, int ny, int nz, const int
     if (R > red.rmax) return HELM3D_ERR_ARG;
     norm2_box_kernel<<<dim3(red.nblocks, R), kRedThreads, 0, s>>>(x.p, x.stride, nx, ny, box[0], box[1], box[2],
                                                                   box[3], box[4], box[5], red.partials, red.cap);
-    reduce_partials_kernel<<<dim3(1, R), kFinalThreads, 0, s>>>(red.partials, red.nblocks, red.cap, 1, out, sOut);
+    reduce_partials_kernel<<<dim3(1, R), kFinalThreads, 0, s>>>(red.partials, red.nblocks, red.cap, 1, out, sOut,
+                                                                 nullptr);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 

@@ -68,8 +68,9 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
     const VecBatch xb{(double2 *)x, 0}, yb{(double2 *)y, 0};
     const ScaleBatch one{nullptr, 0};
     const PlaneLayout L{c->grid.nx, c->grid.ny, c->grid.nz, 1, c->plane};
-    rc = c->zeig ? launch_ztrans_forward(c->c64, xb, 1.0, one, scratch, L, c->d_zWi64, c->stream)
-                 : launch_fft_forward(c->c64, xb, 1.0, one, scratch, L, c->plan, c->d_tw, c->stream);
+    rc = c->ztc    ? launch_ztc_forward(xb, 1.0, one, scratch, L, c->d_ztc[0], c->d_status, c->stream)
+         : c->zeig ? launch_ztrans_forward(c->c64, xb, 1.0, one, scratch, L, c->d_zWi64, c->stream)
+                   : launch_fft_forward(c->c64, xb, 1.0, one, scratch, L, c->plan, c->d_tw, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: forward FFT launch");
     SweepArgs s;
     s.n = c->grid.nx;
@@ -85,8 +86,9 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
     s.status = c->d_status;
     rc = launch_sweep(c->c64, s, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: sweep launch");
-    rc = c->zeig ? launch_ztrans_inverse(c->c64, scratch, L, yb, c->d_zW64, c->stream)
-                 : launch_fft_inverse(c->c64, scratch, L, yb, c->plan, c->d_tw, 0, VecBatch{nullptr, 0}, 0.0, one,
+    rc = c->ztc    ? launch_ztc_inverse(scratch, L, yb, c->d_ztc[1], c->d_status, c->stream)
+         : c->zeig ? launch_ztrans_inverse(c->c64, scratch, L, yb, c->d_zW64, c->stream)
+                   : launch_fft_inverse(c->c64, scratch, L, yb, c->plan, c->d_tw, 0, VecBatch{nullptr, 0}, 0.0, one,
                                       nullptr, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: inverse FFT launch");
     c->launches += 3;

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "helm3d_internal.h"
@@ -367,6 +368,21 @@ int ctx_setup_grid(helm3d_ctx *c) {
             (rc = upload_c64(c, &c->d_zWH64, wh, "z eigenvectors^H")) ||
             (rc = upload_c64(c, &c->d_zWiH64, wih, "z eigenvectors inverse^H")))
             return rc;
+        // complex64 planes: the transforms run on the tensor cores (3xTF32);
+        // HELM3D_ZT_TENSOR=0 in the environment keeps the FP64 kernels
+        const char *env = std::getenv("HELM3D_ZT_TENSOR");
+        c->ztc = c->c64 && ztc_supported(nz) && !(env && env[0] == '0');
+        if (c->ztc) {
+            const std::vector<zc> *mats[4] = {&c->zWi, &c->zW, &wh, &wih};
+            for (int q = 0; q < 4; q++) {
+                std::vector<float> b;
+                ztc_prepare(*mats[q], nz, b);
+                if ((rc = dalloc(c, (void **)&c->d_ztc[q], b.size() * 4, "tensor-core z-transform")) ||
+                    (rc = cuda_check(c, cudaMemcpy(c->d_ztc[q], b.data(), b.size() * 4, cudaMemcpyHostToDevice),
+                                     "tensor-core z-transform")))
+                    return rc;
+            }
+        }
     } else {
         for (int k = 0; k < nz; k++) c->zshift[k] = -c->kz2[k];
     }

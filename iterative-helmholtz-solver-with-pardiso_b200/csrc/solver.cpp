@@ -52,11 +52,57 @@ static Reduce reducer(helm3d_ctx *c) {
 // small per-right-hand-side device scalars: h1 | h2 | norms | y, each m+2 long
 static int scalars_per_rhs(int m) { return 4 * (m + 2); }
 
+// bytes of the device Arnoldi state for R right-hand sides and restart m
+static size_t arn_bytes(int m, int R) {
+    return sizeof(double2) * (size_t)R * ((size_t)(m + 1) * m + 2 * m + (m + 1)) +
+           sizeof(double) * (size_t)R * (m + 2) + sizeof(int) * ((size_t)4 * R + 4) + 256;
+}
+
+// the state arrays of a batch of B (restart m) carved from c->d_arn:
+// doubles first (est, nf, tol), then ints (frozen, k, it, max_iter, flags)
+static ArnState arn_state(helm3d_ctx *c, int m, int B) {
+    ArnState a;
+    const int R = c->r_alloc;
+    char *q = (char *)c->d_arn;
+    a.H = (double2 *)q;
+    q += sizeof(double2) * (size_t)R * (m + 1) * m;
+    a.cs = (double2 *)q;
+    q += sizeof(double2) * (size_t)R * m;
+    a.sn = (double2 *)q;
+    q += sizeof(double2) * (size_t)R * m;
+    a.g = (double2 *)q;
+    q += sizeof(double2) * (size_t)R * (m + 1);
+    a.est = (double *)q;
+    q += sizeof(double) * (size_t)R * m;
+    a.nf = (double *)q;
+    a.tol = a.nf + R;
+    q += sizeof(double) * (size_t)2 * R;
+    a.frozen = (int *)q;
+    a.k = a.frozen + R;
+    a.it = a.k + R;
+    a.max_iter = a.it + R;
+    a.flags = a.max_iter + R;
+    a.m = m;
+    a.B = B;
+    a.h = c->d_h;
+    a.M2 = m + 2;
+    a.SH = 4 * (m + 2);
+    a.vs = c->d_vs;
+    return a;
+}
+
+static void drop_graphs(helm3d_ctx *c) {
+    for (auto &g : c->graphs) cudaGraphExecDestroy(g.exec);
+    c->graphs.clear();
+}
+
 static void free_krylov(helm3d_ctx *c) {
-    void *bufs[] = {c->d_V, c->d_Z, c->d_vs, c->d_h, c->d_partials, c->d_Fw, c->d_Uw};
+    drop_graphs(c);
+    void *bufs[] = {c->d_V, c->d_Z, c->d_vs, c->d_h, c->d_partials, c->d_Fw, c->d_Uw, c->d_arn};
     for (void *p : bufs)
         if (p) cudaFree(p);
     c->d_V = c->d_Z = c->d_h = c->d_partials = c->d_Fw = c->d_Uw = nullptr;
+    c->d_arn = nullptr;
     c->d_vs = nullptr;
     c->bytes -= c->kry_bytes;
     c->kry_bytes = 0;
@@ -83,7 +129,8 @@ int ensure_krylov(helm3d_ctx *c, int m, int R) {
         (rc = get((void **)&c->d_h, sizeof(double2) * scalars_per_rhs(m) * R, "Krylov scalars")) ||
         (rc = get((void **)&c->d_partials, sizeof(double2) * c->red_cap * c->red_blocks * R, "partials")) ||
         (rc = get((void **)&c->d_Fw, vb * R, "packed right-hand sides")) ||
-        (rc = get((void **)&c->d_Uw, vb * R, "packed iterates"))) {
+        (rc = get((void **)&c->d_Uw, vb * R, "packed iterates")) ||
+        (rc = get(&c->d_arn, arn_bytes(m, R), "Arnoldi state"))) {
         c->kry_bytes = 0;
         free_krylov(c);
         return rc;
@@ -106,6 +153,7 @@ static int ensure_vec(helm3d_ctx *c, double2 **p, const char *what) {
 static int ensure_planes(helm3d_ctx *c, int R) {
     if (c->planes_R >= R && c->d_planes) return HELM3D_OK;
     const size_t esz = c->c64 ? 8 : 16;
+    drop_graphs(c);   // captured launches hold the old planes
     if (c->d_planes) {
         RC(cuda_check(c, cudaStreamSynchronize(c->stream), "planes sync"));
         cudaFree(c->d_planes);
@@ -155,6 +203,9 @@ static int prec_to_planes(helm3d_ctx *c, const VecBatch &x, double xscale, const
     RC(ensure_planes(c, R));
     const PlaneLayout L = layout(c, R);
     RC(timed(c, HELM3D_K_FFT_FWD, 1, [&] {
+        if (c->ztc)
+            return launch_ztc_forward(x, xscale, sc, c->d_planes, L, c->d_ztc[adjoint ? 2 : 0], c->d_status,
+                                      c->stream);
         if (c->zeig)
             return launch_ztrans_forward(c->c64, x, xscale, sc, c->d_planes, L, adjoint ? c->d_zWH64 : c->d_zWi64,
                                          c->stream);
@@ -169,6 +220,7 @@ static int prec_common(helm3d_ctx *c, const VecBatch &x, double xscale, const Sc
     RC(prec_to_planes(c, x, xscale, sc, R, adjoint));
     const PlaneLayout L = layout(c, R);
     return timed(c, HELM3D_K_FFT_INV, 1, [&] {
+        if (c->ztc) return launch_ztc_inverse(c->d_planes, L, y, c->d_ztc[adjoint ? 3 : 1], c->d_status, c->stream);
         if (c->zeig)
             return launch_ztrans_inverse(c->c64, c->d_planes, L, y, adjoint ? c->d_zWiH64 : c->d_zW64, c->stream);
         return launch_fft_inverse(c->c64, c->d_planes, L, y, c->plan, c->d_tw, 0, VecBatch{nullptr, 0}, 0.0,
@@ -320,6 +372,137 @@ static void givens(zc a, zc b, zc &cs, zc &sn) {
     }
 }
 
+// ------------------------------------------------ restart cycle as a graph
+// One Arnoldi step j of a batch of B, kernels only: the operator and
+// preconditioner applications, classical Gram-Schmidt with its norms, the
+// predicated second pass and the device Givens update, which arms (or not)
+// the conditional node of step j + 1.
+static int arnoldi_step(helm3d_ctx *c, int m, int B, int j, bool adjoint, const ArnState &a, bool has_next,
+                        cudaGraphConditionalHandle next) {
+    const long N = c->N;
+    const long ldV = (long)(m + 1) * N, ldZ = (long)m * N;
+    const int M2 = m + 2, SH = scalars_per_rhs(m);
+    double2 *V = c->d_V, *Z = c->d_Z, *Hd = c->d_h;
+    double2 *d_h1 = Hd, *d_h2 = Hd + M2, *d_nrm = Hd + 2 * M2;
+    const Reduce red = reducer(c);
+    const VecBatch Vall{V, ldV}, Vj{V + (size_t)j * N, ldV}, w{V + (size_t)(j + 1) * N, ldV};
+    const ScaleBatch vsb{c->d_vs, M2}, vsj{c->d_vs + j, M2};
+    if (c->opts.mode == HELM3D_MODE_N) {
+        const VecBatch zj{Z + (size_t)j * N, ldZ};
+        if (adjoint) {
+            RC(apply_prec_adjoint(c, Vj, 1.0, vsj, zj, B));
+            RC(apply_op_adjoint(c, zj, 1.0, kNoScale, w, B));
+        } else {
+            RC(apply_prec(c, Vj, 1.0, vsj, zj, B));
+            RC(apply_op(c, zj, 1.0, kNoScale, w, B));
+        }
+    } else {
+        RC(apply_op(c, Vj, 1.0, vsj, w, B));
+    }
+    RC(timed(c, HELM3D_K_KRYLOV, 2,
+             [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h1, SH, c->stream, true); }));
+    RC(timed(c, HELM3D_K_KRYLOV, 2,
+             [&] { return launch_update(Vall, N, vsb, j + 1, d_h1, SH, w, N, B, 1, red, d_nrm, SH, c->stream); }));
+    RC(timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_reorth_check(a, j, c->stream); }));
+    RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+        return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h2, SH, c->stream, false, a.flags);
+    }));
+    RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+        return launch_update(Vall, N, vsb, j + 1, d_h2, SH, w, N, B, 1, red, d_nrm, SH, c->stream, a.flags);
+    }));
+    return timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_givens(a, j, has_next, next, c->stream); });
+}
+
+// end of a cycle: y = R^{-1} g on the device, x += Z y (mode R: V y)
+static int cycle_tail(helm3d_ctx *c, int m, int B, const ArnState &a) {
+    const long N = c->N;
+    const long ldV = (long)(m + 1) * N, ldZ = (long)m * N;
+    const int M2 = m + 2, SH = scalars_per_rhs(m);
+    double2 *d_y = c->d_h + 3 * M2;
+    RC(timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_backsub(a, c->stream); }));
+    return timed(c, HELM3D_K_KRYLOV, 1, [&] {
+        return c->opts.mode == HELM3D_MODE_N
+                   ? launch_combine(VecBatch{c->d_Z, ldZ}, N, kNoScale, m, d_y, SH, VecBatch{c->d_Uw, N}, N, B,
+                                    c->stream, a.flags + 2)
+                   : launch_combine(VecBatch{c->d_V, ldV}, N, ScaleBatch{c->d_vs, M2}, m, d_y, SH,
+                                    VecBatch{c->d_Uw, N}, N, B, c->stream, a.flags + 2);
+    });
+}
+
+// The cycle graph of a batch of B: m conditional (IF) nodes in sequence, the
+// body of node j holding step j, then the tail.  Step 0 always runs; the
+// Givens kernel of step j sets the condition of step j + 1.  Built once per
+// (B, adjoint) and kept until the workspace moves.  Returns the index in
+// c->graphs, or -1 when graphs are unavailable (the caller falls back to
+// the host-driven cycle).
+static int cycle_graph(helm3d_ctx *c, int m, int B, bool adjoint) {
+    for (size_t q = 0; q < c->graphs.size(); q++)
+        if (c->graphs[q].B == B && c->graphs[q].adjoint == adjoint) return (int)q;
+    if (ensure_planes(c, B)) return -1;   // every allocation before the capture
+    const ArnState a = arn_state(c, m, B);
+    cudaStream_t cap = nullptr;
+    if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    cudaStream_t saved = c->stream;
+    const bool prof = c->prof;
+    const long long launches0 = c->launches;
+    c->stream = cap;
+    c->prof = false;
+    cudaGraph_t G = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long per_step = 0, tail = 0;
+    bool ok = cudaGraphCreate(&G, 0) == cudaSuccess;
+    std::vector<cudaGraphConditionalHandle> hs(m);
+    for (int j = 0; ok && j < m; j++)
+        ok = cudaGraphConditionalHandleCreate(&hs[j], G, j == 0 ? 1u : 0u, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNode_t prev = nullptr;
+    for (int j = 0; ok && j < m; j++) {
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = hs[j];
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        ok = cudaGraphAddNode(&node, G, prev ? &prev : nullptr, prev ? 1 : 0, &cp) == cudaSuccess;
+        if (!ok) break;
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        ok = cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+             cudaSuccess;
+        if (!ok) break;
+        const long long l0 = c->launches;
+        const int rc = arnoldi_step(c, m, B, j, adjoint, a, j + 1 < m, j + 1 < m ? hs[j + 1] : 0);
+        cudaGraph_t out = nullptr;
+        ok = cudaStreamEndCapture(cap, &out) == cudaSuccess && rc == HELM3D_OK;
+        per_step = c->launches - l0;
+        prev = node;
+    }
+    if (ok) {
+        ok = cudaStreamBeginCaptureToGraph(cap, G, &prev, nullptr, 1, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+        if (ok) {
+            const long long l0 = c->launches;
+            const int rc = cycle_tail(c, m, B, a);
+            cudaGraph_t out = nullptr;
+            ok = cudaStreamEndCapture(cap, &out) == cudaSuccess && rc == HELM3D_OK;
+            tail = c->launches - l0;
+        }
+    }
+    if (ok) ok = cudaGraphInstantiate(&exec, G, 0) == cudaSuccess;
+    if (G) cudaGraphDestroy(G);
+    cudaStreamDestroy(cap);
+    c->stream = saved;
+    c->prof = prof;
+    c->launches = launches0;
+    if (!ok) {
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        return -1;
+    }
+    c->graphs.push_back({B, adjoint, exec, per_step, tail});
+    return (int)c->graphs.size() - 1;
+}
+
 // --------------------------------------------------------------- FGMRES
 namespace {
 // host state of one right-hand side of the batch
@@ -458,115 +641,167 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, hel
                       "vs0"));
         const VecBatch Vall{V, ldV};
         const ScaleBatch vsb{c->d_vs, M2};
-        for (int j = 0; j < m; j++) {
-            const VecBatch Vj{V + (size_t)j * N, ldV}, w{V + (size_t)(j + 1) * N, ldV};
-            const ScaleBatch vsj{c->d_vs + j, M2};
-            if (flexible) {
-                const VecBatch zj{Z + (size_t)j * N, ldZ};
-                if (adjoint) {
-                    // A^H M^{-H} = (M^{-1} A)^H: the adjoint of the forward
-                    // preconditioned operator, with the same singular values
-                    RC(apply_prec_adjoint(c, Vj, 1.0, vsj, zj, B));
-                    RC(apply_op_adjoint(c, zj, 1.0, kNoScale, w, B));
-                } else {
-                    RC(apply_prec(c, Vj, 1.0, vsj, zj, B));
-                    RC(apply_op(c, zj, 1.0, kNoScale, w, B));
-                }
-            } else {
-                RC(apply_op(c, Vj, 1.0, vsj, w, B));
-            }
-            // Classical Gram-Schmidt, repeated only when needed ("twice is
-            // enough"): h1 = V^H w with ||w||^2 from the same pass, w -= V h1
-            // with ||w||^2 after; a second pass runs when the norm of some
-            // right-hand side dropped below 1/sqrt(2) of its value.
-            RC(timed(c, HELM3D_K_KRYLOV, 2,
-                     [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h1, SH, c->stream, true); }));
-            RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
-                return launch_update(Vall, N, vsb, j + 1, d_h1, SH, w, N, B, 1, red, d_nrm, SH, c->stream);
-            }));
-            RC(fetch(c, Hd, (size_t)SH * B, hb.h, "Arnoldi coefficients"));
-            bool again = false;
+        const int gi = (c->use_graphs && !c->prof && !o.verbose) ? cycle_graph(c, m, B, adjoint) : -1;
+        if (gi >= 0) {
+            // the whole cycle on the device: state in, one graph launch, state out
+            const ArnState a = arn_state(c, m, B);
+            const int Ra = c->r_alloc;
+            std::vector<double> dv((size_t)2 * Ra, 0.0);
+            std::vector<int> iv((size_t)4 * Ra + 4, 0);
+            std::vector<double2> g0((size_t)B);
             for (int p = 0; p < B; p++) {
                 const Rhs &r = S[act[p]];
-                const double2 *h = hb.h + (size_t)p * SH;
-                if (!r.frozen && h[2 * M2].x < 0.5 * h[j + 1].x) again = true;
+                dv[p] = r.nf;
+                dv[Ra + p] = tol;
+                iv[2 * Ra + p] = r.it;
+                iv[3 * Ra + p] = o.max_iter;
+                g0[p] = make_double2(r.beta, 0.0);
             }
+            RC(cuda_check(c, cudaMemcpyAsync(a.nf, dv.data(), sizeof(double) * dv.size(), cudaMemcpyHostToDevice,
+                                             c->stream),
+                          "cycle state"));
+            RC(cuda_check(c, cudaMemcpyAsync(a.frozen, iv.data(), sizeof(int) * iv.size(), cudaMemcpyHostToDevice,
+                                             c->stream),
+                          "cycle state"));
+            RC(cuda_check(c, cudaMemcpy2DAsync(a.g, sizeof(double2) * (m + 1), g0.data(), sizeof(double2),
+                                               sizeof(double2), B, cudaMemcpyHostToDevice, c->stream),
+                          "cycle state"));
+            RC(cuda_check(c, cudaGraphLaunch(c->graphs[gi].exec, c->stream), "cycle graph"));
+            std::vector<double> est((size_t)Ra * m);
+            RC(cuda_check(c, cudaMemcpyAsync(iv.data(), a.frozen, sizeof(int) * iv.size(), cudaMemcpyDeviceToHost,
+                                             c->stream),
+                          "cycle result"));
+            RC(cuda_check(c, cudaMemcpyAsync(est.data(), a.est, sizeof(double) * est.size(), cudaMemcpyDeviceToHost,
+                                             c->stream),
+                          "cycle result"));
+            RC(cuda_check(c, cudaStreamSynchronize(c->stream), "cycle"));
+            const int *flags = iv.data() + 4 * Ra;
+            if (flags[3]) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
+            const int kmax = flags[2];
+            c->reorth += flags[1];
+            c->launches += kmax * c->graphs[gi].kernels_per_step + c->graphs[gi].tail_kernels;
             for (int p = 0; p < B; p++) {
                 Rhs &r = S[act[p]];
-                const double2 *h = hb.h + (size_t)p * SH;
-                for (int i = 0; i <= j; i++) r.H[(size_t)i * m + j] = zc(h[i].x, h[i].y);
+                r.it = iv[2 * Ra + p];
+                r.k = iv[Ra + p];
             }
-            if (again) {
+            for (int j = 0; j < kmax; j++) {
+                double e = 0;
+                for (int p = 0; p < B; p++)
+                    if (S[act[p]].k > j) e = std::max(e, est[(size_t)p * m + j]);
+                if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = e;
+            }
+        } else {
+            for (int j = 0; j < m; j++) {
+                const VecBatch Vj{V + (size_t)j * N, ldV}, w{V + (size_t)(j + 1) * N, ldV};
+                const ScaleBatch vsj{c->d_vs + j, M2};
+                if (flexible) {
+                    const VecBatch zj{Z + (size_t)j * N, ldZ};
+                    if (adjoint) {
+                        // A^H M^{-H} = (M^{-1} A)^H: the adjoint of the forward
+                        // preconditioned operator, with the same singular values
+                        RC(apply_prec_adjoint(c, Vj, 1.0, vsj, zj, B));
+                        RC(apply_op_adjoint(c, zj, 1.0, kNoScale, w, B));
+                    } else {
+                        RC(apply_prec(c, Vj, 1.0, vsj, zj, B));
+                        RC(apply_op(c, zj, 1.0, kNoScale, w, B));
+                    }
+                } else {
+                    RC(apply_op(c, Vj, 1.0, vsj, w, B));
+                }
+                // Classical Gram-Schmidt, repeated only when needed ("twice is
+                // enough"): h1 = V^H w with ||w||^2 from the same pass, w -= V h1
+                // with ||w||^2 after; a second pass runs when the norm of some
+                // right-hand side dropped below 1/sqrt(2) of its value.
                 RC(timed(c, HELM3D_K_KRYLOV, 2,
-                         [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h2, SH, c->stream); }));
+                         [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h1, SH, c->stream, true); }));
                 RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
-                    return launch_update(Vall, N, vsb, j + 1, d_h2, SH, w, N, B, 1, red, d_nrm, SH, c->stream);
+                    return launch_update(Vall, N, vsb, j + 1, d_h1, SH, w, N, B, 1, red, d_nrm, SH, c->stream);
                 }));
-                RC(fetch(c, Hd, (size_t)SH * B, hb.h, "Arnoldi second pass"));
+                RC(fetch(c, Hd, (size_t)SH * B, hb.h, "Arnoldi coefficients"));
+                bool again = false;
+                for (int p = 0; p < B; p++) {
+                    const Rhs &r = S[act[p]];
+                    const double2 *h = hb.h + (size_t)p * SH;
+                    if (!r.frozen && h[2 * M2].x < 0.5 * h[j + 1].x) again = true;
+                }
                 for (int p = 0; p < B; p++) {
                     Rhs &r = S[act[p]];
-                    const double2 *h = hb.h + (size_t)p * SH + M2;
-                    for (int i = 0; i <= j; i++) r.H[(size_t)i * m + j] += zc(h[i].x, h[i].y);
+                    const double2 *h = hb.h + (size_t)p * SH;
+                    for (int i = 0; i <= j; i++) r.H[(size_t)i * m + j] = zc(h[i].x, h[i].y);
                 }
-                c->reorth++;
+                if (again) {
+                    RC(timed(c, HELM3D_K_KRYLOV, 2,
+                             [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h2, SH, c->stream); }));
+                    RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+                        return launch_update(Vall, N, vsb, j + 1, d_h2, SH, w, N, B, 1, red, d_nrm, SH, c->stream);
+                    }));
+                    RC(fetch(c, Hd, (size_t)SH * B, hb.h, "Arnoldi second pass"));
+                    for (int p = 0; p < B; p++) {
+                        Rhs &r = S[act[p]];
+                        const double2 *h = hb.h + (size_t)p * SH + M2;
+                        for (int i = 0; i <= j; i++) r.H[(size_t)i * m + j] += zc(h[i].x, h[i].y);
+                    }
+                    c->reorth++;
+                }
+                double est_max = 0;
+                bool all_frozen = true;
+                for (int p = 0; p < B; p++) {
+                    Rhs &r = S[act[p]];
+                    if (r.frozen) continue;
+                    const double hn = std::sqrt(std::max(0.0, hb.h[(size_t)p * SH + 2 * M2].x));
+                    if (!std::isfinite(hn)) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
+                    std::vector<zc> &H = r.H;
+                    H[(size_t)(j + 1) * m + j] = hn;
+                    for (int i = 0; i < j; i++) {
+                        const zc a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
+                        H[(size_t)i * m + j] = r.cs[i] * a + r.sn[i] * b;
+                        H[(size_t)(i + 1) * m + j] = -std::conj(r.sn[i]) * a + r.cs[i] * b;
+                    }
+                    const zc a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
+                    givens(a, b, r.cs[j], r.sn[j]);
+                    H[(size_t)j * m + j] = r.cs[j] * a + r.sn[j] * b;
+                    H[(size_t)(j + 1) * m + j] = 0.0;
+                    r.gv[j + 1] = -std::conj(r.sn[j]) * r.gv[j];
+                    r.gv[j] = r.cs[j] * r.gv[j];
+                    r.it++;
+                    r.k = j + 1;
+                    const double est = std::abs(r.gv[j + 1]) / r.nf;
+                    est_max = std::max(est_max, est);
+                    if (hn == 0.0 || est <= tol || r.it >= o.max_iter) r.frozen = true;
+                    else all_frozen = false;
+                }
+                if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = est_max;
+                if (o.verbose) fprintf(stderr, "helm3d: step %d  max est relres %.3e over %d rhs\n", j + 1, est_max, B);
+                if (all_frozen) break;
+                RC(timed(c, HELM3D_K_KRYLOV, 1,
+                         [&] { return launch_set_scale(d_nrm, SH, c->d_vs, M2, j + 1, B, c->stream); }));
             }
-            double est_max = 0;
-            bool all_frozen = true;
+            // y = H^{-1} g (upper triangular k x k) per right-hand side, zero
+            // padded to the longest; x += basis * y
+            int kmax = 0;
+            for (int p = 0; p < B; p++) kmax = std::max(kmax, S[act[p]].k);
             for (int p = 0; p < B; p++) {
-                Rhs &r = S[act[p]];
-                if (r.frozen) continue;
-                const double hn = std::sqrt(std::max(0.0, hb.h[(size_t)p * SH + 2 * M2].x));
-                if (!std::isfinite(hn)) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
-                std::vector<zc> &H = r.H;
-                H[(size_t)(j + 1) * m + j] = hn;
-                for (int i = 0; i < j; i++) {
-                    const zc a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
-                    H[(size_t)i * m + j] = r.cs[i] * a + r.sn[i] * b;
-                    H[(size_t)(i + 1) * m + j] = -std::conj(r.sn[i]) * a + r.cs[i] * b;
+                const Rhs &r = S[act[p]];
+                double2 *y = ybuf.data() + (size_t)p * M2;
+                std::vector<zc> yz(r.k);
+                for (int i = r.k - 1; i >= 0; i--) {
+                    zc s = r.gv[i];
+                    for (int q = i + 1; q < r.k; q++) s -= r.H[(size_t)i * m + q] * yz[q];
+                    yz[i] = s / r.H[(size_t)i * m + i];
                 }
-                const zc a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
-                givens(a, b, r.cs[j], r.sn[j]);
-                H[(size_t)j * m + j] = r.cs[j] * a + r.sn[j] * b;
-                H[(size_t)(j + 1) * m + j] = 0.0;
-                r.gv[j + 1] = -std::conj(r.sn[j]) * r.gv[j];
-                r.gv[j] = r.cs[j] * r.gv[j];
-                r.it++;
-                r.k = j + 1;
-                const double est = std::abs(r.gv[j + 1]) / r.nf;
-                est_max = std::max(est_max, est);
-                if (hn == 0.0 || est <= tol || r.it >= o.max_iter) r.frozen = true;
-                else all_frozen = false;
+                for (int i = 0; i < kmax; i++) y[i] = i < r.k ? make_double2(yz[i].real(), yz[i].imag()) : make_double2(0, 0);
             }
-            if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = est_max;
-            if (o.verbose) fprintf(stderr, "helm3d: step %d  max est relres %.3e over %d rhs\n", j + 1, est_max, B);
-            if (all_frozen) break;
-            RC(timed(c, HELM3D_K_KRYLOV, 1,
-                     [&] { return launch_set_scale(d_nrm, SH, c->d_vs, M2, j + 1, B, c->stream); }));
-        }
-        // y = H^{-1} g (upper triangular k x k) per right-hand side, zero
-        // padded to the longest; x += basis * y
-        int kmax = 0;
-        for (int p = 0; p < B; p++) kmax = std::max(kmax, S[act[p]].k);
-        for (int p = 0; p < B; p++) {
-            const Rhs &r = S[act[p]];
-            double2 *y = ybuf.data() + (size_t)p * M2;
-            std::vector<zc> yz(r.k);
-            for (int i = r.k - 1; i >= 0; i--) {
-                zc s = r.gv[i];
-                for (int q = i + 1; q < r.k; q++) s -= r.H[(size_t)i * m + q] * yz[q];
-                yz[i] = s / r.H[(size_t)i * m + i];
+            if (kmax > 0) {
+                RC(cuda_check(c, cudaMemcpy2DAsync(d_y, sizeof(double2) * SH, ybuf.data(), sizeof(double2) * M2,
+                                                   sizeof(double2) * kmax, B, cudaMemcpyHostToDevice, c->stream),
+                              "y"));
+                RC(timed(c, HELM3D_K_KRYLOV, 1, [&] {
+                    return flexible ? launch_combine(VecBatch{Z, ldZ}, N, kNoScale, kmax, d_y, SH, VecBatch{Uw, N}, N, B,
+                                                     c->stream)
+                                    : launch_combine(Vall, N, vsb, kmax, d_y, SH, VecBatch{Uw, N}, N, B, c->stream);
+                }));
             }
-            for (int i = 0; i < kmax; i++) y[i] = i < r.k ? make_double2(yz[i].real(), yz[i].imag()) : make_double2(0, 0);
-        }
-        if (kmax > 0) {
-            RC(cuda_check(c, cudaMemcpy2DAsync(d_y, sizeof(double2) * SH, ybuf.data(), sizeof(double2) * M2,
-                                               sizeof(double2) * kmax, B, cudaMemcpyHostToDevice, c->stream),
-                          "y"));
-            RC(timed(c, HELM3D_K_KRYLOV, 1, [&] {
-                return flexible ? launch_combine(VecBatch{Z, ldZ}, N, kNoScale, kmax, d_y, SH, VecBatch{Uw, N}, N, B,
-                                                 c->stream)
-                                : launch_combine(Vall, N, vsb, kmax, d_y, SH, VecBatch{Uw, N}, N, B, c->stream);
-            }));
         }
         x_zero = false;
         for (int p = 0; p < B; p++) S[act[p]].restarts++;

@@ -199,3 +199,75 @@ def test_batched_zpml_eigen(prec):
     on = mode_n.setup(p, factor=False)
     for i in range(2):
         assert np.linalg.norm(on.apply_a(U[i]) - F[i]) / np.linalg.norm(F[i]) < 2e-10
+
+
+@pytest.mark.parametrize("nz", [17, 48, 130])
+def test_zpml_eigen_tensor_core_transforms(nz, monkeypatch):
+    """The complex64 eigenbasis transforms run on the tensor cores (3xTF32);
+    they agree with the FP64 transforms to FP32 accuracy and take the same
+    FGMRES iterations.  nz = 130 exercises the two-part (N > 256) MMA."""
+    import helm3d
+    p = small_problem(24, 20, nz, pml=4, seed=nz + 3)
+    v = rand_c(p.shape, seed=2)
+    ref = mode_n.setup(p, beta_prec=0.25, z_transform="eigen").apply_prec(v)
+    out, its = {}, {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("HELM3D_ZT_TENSOR", flag)
+        s = mode_n_solver(p, precision=1, tol=1e-9, z_transform=helm3d.ZT_PML_EIGEN)
+        out[flag] = s.apply_prec(v)
+        s.solve(p.rhs(0))
+        its[flag] = s.last_stats.iterations
+        s.close()
+    # the complex64 preconditioner's own error (the eigenbasis amplifies
+    # FP32 rounding) bounds both paths alike against the FP64 oracle
+    assert rel(out["1"], ref) < 1e-3 and rel(out["0"], ref) < 1e-3
+    assert rel(out["1"], ref) < 2.0 * rel(out["0"], ref) + 1e-5
+    assert abs(its["1"] - its["0"]) <= 1
+
+
+# ------------------------------------------ graph-captured restart cycles
+def _solve_both_ways(make, F, monkeypatch):
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("HELM3D_GRAPH", flag)
+        s = make()
+        U = s.solve(F, nrhs=len(F))
+        out[flag] = (U, s.last_stats.iterations, s.last_stats.relres, None)
+        s.close()
+    return out
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_graph_cycle_matches_host_cycle_mode_n(prec, monkeypatch):
+    """A restart cycle captured as a CUDA graph (device Givens, conditional
+    steps) computes what the host-driven cycle computes."""
+    p = media.config_small(20, 4, seed=12, n_sources=3)
+    F = np.stack([p.rhs(i) for i in range(3)])
+    out = _solve_both_ways(lambda: mode_n_solver(p, precision=prec, tol=1e-10), F, monkeypatch)
+    (Ug, itg, rg, _), (Ue, ite, re, _) = out["1"], out["0"]
+    assert abs(itg - ite) <= 1
+    assert rg < 1e-10 and re < 1e-10
+    assert rel(Ug, Ue) < 1e-9
+
+
+def test_graph_cycle_matches_host_cycle_mode_r(monkeypatch):
+    g, st = mode_r_case(10, 4, 3)
+    F = np.stack([rand_c(g.shape_zyx, seed=31), rand_c(g.shape_zyx, seed=32)])
+    out = _solve_both_ways(lambda: mode_r_solver(g, st, tol=1e-11, max_iter=3000), F, monkeypatch)
+    (Ug, itg, rg, _), (Ue, ite, re, _) = out["1"], out["0"]
+    assert abs(itg - ite) <= 1
+    assert rel(Ug, Ue) < 1e-8
+
+
+def test_graph_cycle_eigen_batch(monkeypatch):
+    import helm3d
+    p = media.config_small(24, 4, seed=13, n_sources=3)
+    F = np.stack([p.rhs(i) for i in range(3)])
+    out = _solve_both_ways(lambda: mode_n_solver(p, precision=1, tol=1e-10, z_transform=helm3d.ZT_PML_EIGEN),
+                           F, monkeypatch)
+    (Ug, itg, rg, _), (Ue, ite, re, _) = out["1"], out["0"]
+    assert abs(itg - ite) <= 1
+    assert rel(Ug, Ue) < 1e-9
+    on = mode_n.setup(p, factor=False)
+    for i in range(3):
+        assert np.linalg.norm(on.apply_a(Ug[i]) - F[i]) / np.linalg.norm(F[i]) < 2e-10
