@@ -207,6 +207,235 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
     }
 }
 
+// ------------------------------------------------------------------------
+// Register-tiled variant for complex64 batches of RR >= 4 right-hand sides.
+// Each line is Y (n x RR) = G_j V.  The CW consumer warps form GM groups of
+// CW / GM warps; group g takes the rows m = g, g + GM, ... of every stage,
+// so the 32 lanes of a warp always read one G row and one v row (contiguous,
+// no bank conflicts).  Thread t of a group owns a tile of TM = 4 rows x
+// TR = 4 right-hand sides: per m it loads 4 G and 4 v entries (four 16-byte
+// shared loads) for 16 complex FMAs.  At the end of a line groups 1..GM-1
+// leave their partial tiles in shared memory and group 0 adds them and
+// finishes the tile (next line's v into shared memory, x or y into the
+// planes).  Producer warp, ring and mbarriers as in sweep_kernel.
+constexpr int kTileM = 4, kTileR = 4;
+
+template <int CW> __device__ __forceinline__ void consumer_barrier_n() {
+    asm volatile("bar.sync 1, %0;" ::"n"(CW * 32) : "memory");
+}
+
+template <int RR, int GM, bool ADJ, int CW>
+__global__ void __launch_bounds__((CW + 1) * 32, 1) sweep_tiled_kernel(SweepK<float> a) {
+    typedef float2 Cx;
+    constexpr int RB = RR / kTileR;             // right-hand-side blocks
+    constexpr int NQ = kTileM * kTileR;          // outputs per tile
+    constexpr int TPG = CW * 32 / GM;            // threads (tiles) per group
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int n = a.n, ny = a.ny, ldg = a.ldg, Rn = a.nrhs;
+    const int kz = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Cx *ring = reinterpret_cast<Cx *>(smem_raw);
+    Cx *vbuf = reinterpret_cast<Cx *>(smem_raw + (size_t)a.nstage * a.stage_bytes);  // [2][n][RR]
+    Cx *red = vbuf + 2 * (size_t)n * RR;                                               // [GM-1][NQ][TPG]
+    uint64_t *full = reinterpret_cast<uint64_t *>(red + (size_t)(GM - 1) * NQ * TPG);
+    uint64_t *empty = full + a.nstage;
+    Cx *P = a.planes + (long)kz * ny * Rn * n;
+    const int cpl = (n + a.rows_per_stage - 1) / a.rows_per_stage;
+    const long nseq = (long)(2 * ny - 1) * cpl;
+    const int NB = (n + kTileM - 1) / kTileM;   // row blocks
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < a.nstage; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], CW);
+        }
+        fence_mbar_init_cluster();
+    }
+    for (int q = threadIdx.x; q < 2 * n * RR; q += blockDim.x) {
+        const int m = (q / RR) % n, r = q % RR;
+        vbuf[q] = (q < n * RR && r < Rn) ? adj_in<float, ADJ>(a, 0, m, P[(long)r * n + m]) : make_float2(0, 0);
+    }
+    __syncthreads();
+
+    if (warp == CW) {
+        if (lane == 0) {
+            bool dead = false;
+            for (long seq = 0; seq < nseq; seq++) {
+                const int s = (int)(seq % a.nstage);
+                const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
+                if (!dead && !mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, kSweepWaitLimit)) {
+                    dead = true;
+                    atomicOr(a.status, 4);
+                }
+                int rows;
+                const Cx *src = stage_src(a, kz, seq, cpl, &rows);
+                const uint32_t bytes = (uint32_t)rows * ldg * (uint32_t)sizeof(Cx);
+                mbar_expect_tx(&full[s], bytes);
+                bulk_g2s(ring + (size_t)s * (a.stage_bytes / sizeof(Cx)), src, bytes, &full[s]);
+            }
+        }
+        return;
+    }
+
+    const int t = threadIdx.x;
+    const int g = t / TPG, tile = t % TPG;
+    const int rb = tile % RB, ib = tile / RB;
+    const bool busy = ib < NB;                  // threads past the last tile only synchronize
+    const int i0 = ib * kTileM, r0 = rb * kTileR;
+    bool dead = false;
+    long seq = 0;
+    for (int step = 0; step < 2 * ny - 1; step++) {
+        const bool fwd = step < ny;
+        const int line = fwd ? step : 2 * ny - 2 - step;
+        const Cx *v = vbuf + (size_t)(step & 1) * n * RR;
+        Cx *vnext = vbuf + (size_t)((step + 1) & 1) * n * RR;
+        // group 0 prefetches the values it needs to finish the tile
+        Cx pre[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            pre[q] = make_float2(0, 0);
+            const int i = i0 + q / kTileR, r = r0 + q % kTileR;
+            if (g == 0 && busy && i < n && r < Rn) {
+                if (fwd && line + 1 < ny)
+                    pre[q] = adj_in<float, ADJ>(a, line + 1, i, P[((long)(line + 1) * Rn + r) * n + i]);
+                else if (!fwd)
+                    pre[q] = P[((long)line * Rn + r) * n + i];
+            }
+        }
+        float2 acc[kTileM][kTileR];
+#pragma unroll
+        for (int x = 0; x < kTileM; x++)
+#pragma unroll
+            for (int y = 0; y < kTileR; y++) acc[x][y] = make_float2(0, 0);
+        for (int ch = 0; ch < cpl; ch++, seq++) {
+            const int s = (int)(seq % a.nstage);
+            const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
+            if (!dead && !mbar_wait_bounded_cta(smem_u32(&full[s]), ph, kSweepWaitLimit)) {
+                dead = true;
+                atomicOr(a.status, 4);
+            }
+            const Cx *st = ring + (size_t)s * (a.stage_bytes / sizeof(Cx));
+            const int m0 = ch * a.rows_per_stage;
+            const int rows = min(a.rows_per_stage, n - m0);
+            if (busy) {
+#pragma unroll 2
+                for (int ml = g; ml < rows; ml += GM) {
+                    const float4 ga = *reinterpret_cast<const float4 *>(st + (long)ml * ldg + i0);
+                    const float4 gb = *reinterpret_cast<const float4 *>(st + (long)ml * ldg + i0 + 2);
+                    const float4 va = *reinterpret_cast<const float4 *>(v + (size_t)(m0 + ml) * RR + r0);
+                    const float4 vb = *reinterpret_cast<const float4 *>(v + (size_t)(m0 + ml) * RR + r0 + 2);
+                    const float2 gg[4] = {make_float2(ga.x, ga.y), make_float2(ga.z, ga.w), make_float2(gb.x, gb.y),
+                                          make_float2(gb.z, gb.w)};
+                    const float2 vv[4] = {make_float2(va.x, va.y), make_float2(va.z, va.w), make_float2(vb.x, vb.y),
+                                          make_float2(vb.z, vb.w)};
+#pragma unroll
+                    for (int x = 0; x < kTileM; x++)
+#pragma unroll
+                        for (int y = 0; y < kTileR; y++) acc[x][y] = cfma(gg[x], vv[y], acc[x][y]);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive_local(&empty[s]);
+        }
+        // partial tiles of groups 1..GM-1 to shared memory ([q][tile]: a warp's stores are contiguous)
+        if (GM > 1) {
+            if (g > 0) {
+#pragma unroll
+                for (int q = 0; q < NQ; q++) red[((size_t)(g - 1) * NQ + q) * TPG + tile] = acc[q / kTileR][q % kTileR];
+            }
+            consumer_barrier_n<CW>();
+        }
+        if (g == 0 && busy) {
+            const Cx cn = (fwd && line + 1 < ny) ? a.cmy[line + 1] : make_float2(0, 0);
+            const Cx cp = fwd ? make_float2(0, 0) : a.cpy[line];
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                const int x = q / kTileR, y = q % kTileR;
+                float2 sum = acc[x][y];
+#pragma unroll
+                for (int h = 1; h < GM; h++) {
+                    const float2 o = red[((size_t)(h - 1) * NQ + q) * TPG + tile];
+                    sum.x += o.x;
+                    sum.y += o.y;
+                }
+                const int i = i0 + x, r = r0 + y;
+                if (i >= n || r >= Rn) continue;
+                Cx out, vn;
+                bool last;
+                if (fwd) {
+                    out = sum;
+                    last = line + 1 == ny;
+                    vn = last ? out : cfms(cn, out, pre[q]);
+                } else {
+                    out = cfms(cp, sum, pre[q]);
+                    last = true;
+                    vn = out;
+                }
+                P[((long)line * Rn + r) * n + i] = last ? adj_out<float, ADJ>(a, line, i, out) : out;
+                vnext[(size_t)i * RR + r] = vn;
+            }
+        }
+        consumer_barrier_n<CW>();
+    }
+}
+
+// RR right-hand sides per CTA, one CTA per kz
+constexpr int kTiledWarps = 8;
+
+template <int RR, bool ADJ> static int sweep_tiled_rr(const SweepArgs &sa, cudaStream_t st) {
+    typedef float2 Cx;
+    SweepK<float> k;
+    k.n = sa.n;
+    k.ny = sa.ny;
+    k.ldg = sa.ldg;
+    k.nrhs = sa.R;
+    k.Gt = (const Cx *)sa.Gt;
+    k.cmy = (const Cx *)sa.cmy;
+    k.cpy = (const Cx *)sa.cpy;
+    k.planes = (Cx *)sa.planes;
+    k.dxy = (const Cx *)sa.dxy;
+    k.status = sa.status;
+    // groups: the largest power of two GM with tiles <= threads per group
+    constexpr int CT = kTiledWarps * 32;
+    const int tiles = ((sa.n + kTileM - 1) / kTileM) * (RR / kTileR);
+    int gm = 1;
+    while (gm < kTiledWarps && tiles <= CT / (gm * 2)) gm *= 2;
+    if (tiles > CT) return HELM3D_ERR_ARG;
+    const size_t vbytes = sizeof(Cx) * 2 * (size_t)sa.n * RR;
+    const size_t rbytes = sizeof(Cx) * (size_t)(gm - 1) * kTileM * kTileR * (CT / gm);
+    const size_t budget = device_info().smem_optin - vbytes - rbytes - 1024;
+    const size_t row_bytes = (size_t)sa.ldg * sizeof(Cx);
+    int rows = (int)((16 * 1024) / row_bytes);
+    if (rows < 1) rows = 1;
+    if (rows > sa.n) rows = sa.n;
+    k.rows_per_stage = rows;
+    k.stage_bytes = (uint32_t)(((size_t)rows * row_bytes + 127) & ~(size_t)127);
+    size_t ring_cap = budget < (size_t)200 * 1024 ? budget : (size_t)200 * 1024;
+    int nst = (int)(ring_cap / k.stage_bytes);
+    if (nst > 32) nst = 32;
+    if (nst < 2) return HELM3D_ERR_ARG;
+    k.nstage = nst;
+    const size_t smem = (size_t)nst * k.stage_bytes + vbytes + rbytes + 2 * nst * sizeof(uint64_t);
+    auto pick = [&](auto kern) -> int {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return HELM3D_ERR_CUDA;
+        kern<<<dim3((unsigned)sa.nz), (kTiledWarps + 1) * 32, smem, st>>>(k);
+        return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
+    };
+    switch (gm) {
+        case 1: return pick(sweep_tiled_kernel<RR, 1, ADJ, kTiledWarps>);
+        case 2: return pick(sweep_tiled_kernel<RR, 2, ADJ, kTiledWarps>);
+        case 4: return pick(sweep_tiled_kernel<RR, 4, ADJ, kTiledWarps>);
+        default: return pick(sweep_tiled_kernel<RR, 8, ADJ, kTiledWarps>);
+    }
+}
+
+template <bool ADJ> static int sweep_tiled(const SweepArgs &sa, cudaStream_t s) {
+    if (sa.R <= 4) return sweep_tiled_rr<4, ADJ>(sa, s);
+    if (sa.R <= 8) return sweep_tiled_rr<8, ADJ>(sa, s);
+    return sweep_tiled_rr<16, ADJ>(sa, s);
+}
+
 template <typename R, int G, int RR, bool ADJ> static int sweep_impl(const SweepArgs &sa, cudaStream_t st) {
     typedef cplx<R> Cx;
     SweepK<R> k;
@@ -256,6 +485,9 @@ template <typename R, int G> static int sweep_g(const SweepArgs &sa, cudaStream_
 
 int launch_sweep(bool c64, const SweepArgs &sa, cudaStream_t s) {
     if (sa.n < 1 || sa.n > kSweepMaxN || sa.R < 1 || sa.R > kMaxBatch) return HELM3D_ERR_ARG;
+    // complex64 batches of 3 or more: the register-tiled kernel (its 16-byte
+    // tile loads need ldg, the padded row length, to be a multiple of 4)
+    if (c64 && sa.R >= 3 && sa.ldg % 4 == 0) return sa.dxy ? sweep_tiled<true>(sa, s) : sweep_tiled<false>(sa, s);
     const int g = sa.n <= 64 ? 4 : (sa.n <= 128 ? 2 : 1);
     if (c64) {
         if (g == 4) return sweep_g<float, 4>(sa, s);
