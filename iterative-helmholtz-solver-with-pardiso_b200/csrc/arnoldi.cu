@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(kArnThreads) reorth_check_kernel(ArnState a, i
     int need = 0;
     if (p < a.B && !a.frozen[p]) {
         const double2 *h = a.h + (long)p * a.SH;
-        need = h[2 * a.M2].x < 0.5 * h[j + 1].x;
+        need = h[2 * a.M2].x < H3D_REORTH_ETA2 * h[j + 1].x;
     }
     need = __syncthreads_or(need);
     if (p == 0) {

@@ -111,6 +111,12 @@ struct SweepArgs {
 int launch_sweep(bool c64, const SweepArgs &a, cudaStream_t s);
 constexpr int kMaxBatch = 16;  // right-hand sides per preconditioner launch
 
+// Classical Gram-Schmidt takes a second pass when the first left less than
+// this fraction of ||w||^2 (0.5: Kahan's "twice is enough", eta = 1/sqrt 2)
+#ifndef H3D_REORTH_ETA2
+#define H3D_REORTH_ETA2 0.5
+#endif
+
 // 7-point PML operator y_r = A (xscale sc_r x_r) (adjoint: A^H), complex128.
 struct StencilArgs {
     int nx, ny, nz;

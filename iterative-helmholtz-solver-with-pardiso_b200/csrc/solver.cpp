@@ -723,7 +723,7 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, hel
                 for (int p = 0; p < B; p++) {
                     const Rhs &r = S[act[p]];
                     const double2 *h = hb.h + (size_t)p * SH;
-                    if (!r.frozen && h[2 * M2].x < 0.5 * h[j + 1].x) again = true;
+                    if (!r.frozen && h[2 * M2].x < H3D_REORTH_ETA2 * h[j + 1].x) again = true;
                 }
                 for (int p = 0; p < B; p++) {
                     Rhs &r = S[act[p]];
