@@ -328,6 +328,56 @@ def run_ours(args, rank, world, dist):
     return line, round(its64) if its64 else None
 
 
+# ------------------------------------------------------ kernel microbench
+def run_kernels(args):
+    """Per-kernel device times of one batched FGMRES(1) iteration (one
+    preconditioner apply and one operator apply for all 16 sources, plus the
+    Gram-Schmidt and residual kernels) on the headline workload, with the
+    algorithmic bytes and HBM fraction of each kernel family.  The solver
+    holds only two Krylov vectors per source (about 4 GB on the device at
+    128^3), which keeps profiler captures of these kernels small."""
+    import torch
+
+    import helm3d
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    p = workload(args.n, BATCH)
+    F = torch.from_numpy(np.stack([p.rhs(i) for i in range(BATCH)])).to(dev)
+    U = torch.empty_like(F)
+    grid = helm3d.grid_mode_n(p.nx, p.ny, p.nz, p.h, p.pml, p.omega)
+    o = helm3d.default_opts(precision=helm3d.PREC_C64, restart=1, tol=TOL, beta_prec=BETA_PREC, max_iter=1,
+                            device=0, z_transform=helm3d.ZT_PML_EIGEN)
+    s = helm3d.Solver(grid, torch.from_numpy(np.ascontiguousarray(p.s2)).to(dev), o)
+    for _ in range(args.warmup):
+        s.solve(F, nrhs=BATCH, u=U, allow_not_converged=True)
+    torch.cuda.synchronize()
+    s.profile(True)
+    for _ in range(args.steps):
+        s.solve(F, nrhs=BATCH, u=U, allow_not_converged=True)
+    prof = s.profile_read()
+    s.close()
+    N = p.nx * p.ny * p.nz
+    e = 8
+    nbytes = {
+        "sweep": 2.0 * p.nz * p.ny * p.nx * p.nx * e + 4.0 * N * e * BATCH,
+        "fft_fwd": (16.0 + e) * N * BATCH,
+        "fft_inv": (16.0 + e) * N * BATCH,
+    }
+    peak, peak_kind = read_peaks()
+    out = {"mode": "kernels", "workload": f"{p.nx}^3, {BATCH} sources, c64 preconditioner, PML eigenbasis",
+           "steps": args.steps, "peak_gbs": peak, "peak_source": peak_kind, "kernels": {}}
+    for k, (ms, n) in prof.items():
+        d = {"ms_total": round(ms, 4), "launches": int(n)}
+        if n and k in nbytes:
+            avg = ms / n / 1e3
+            d["bytes_per_launch"] = nbytes[k]
+            d["achieved_gbs"] = nbytes[k] / avg / 1e9
+            d["frac"] = d["achieved_gbs"] / peak
+        out["kernels"][k] = d
+    return out
+
+
 # ------------------------------------------------------------ CPU baseline
 def cpu_port_sample(n: int, iters: int | None, cores: int, budget_iters: int = 2):
     """Time the oracle port (SciPy SuperLU per kz + NumPy FFT + NumPy stencil,
@@ -428,10 +478,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", dest="n", type=int, default=128, help="grid points per axis")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels", action="store_true",
+                    help="per-kernel microbench: batched FGMRES(1) iterations instead of full solves")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.kernels:
+        print(json.dumps(run_kernels(args)))
+        return
     if args.impl == "reference":
         # the CPU reference runs on rank 0 only; the other ranks exit at once
         out = run_reference(args, rank)

@@ -211,6 +211,10 @@ int helm3d_create(const helm3d_grid *grid, const double *s2, const helm3d_opts *
     // HELM3D_GRAPH=0 keeps the host-driven restart cycle (no CUDA graphs)
     const char *genv = std::getenv("HELM3D_GRAPH");
     c->use_graphs = !(genv && genv[0] == '0');
+    // HELM3D_GS=cgs2 selects classical Gram-Schmidt with the conditional
+    // second pass for mode N instead of DCGS2
+    const char *gsenv = std::getenv("HELM3D_GS");
+    c->gs_lowsync = !(gsenv && std::strcmp(gsenv, "cgs2") == 0);
     auto t0 = std::chrono::steady_clock::now();
     if ((rc = ctx_setup_grid(c)) || (rc = ctx_setup_medium(c, s2, is_device_ptr(s2))) || (rc = ctx_factor(c)))
         return fail(rc);

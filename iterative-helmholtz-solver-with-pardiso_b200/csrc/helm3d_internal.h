@@ -165,18 +165,41 @@ struct ArnState {
     double2 *g;        // [B][m+1] rotated right-hand side (g[0] = beta on entry)
     double *est;       // [B][m] |g[j+1]| / ||f|| after step j
     double *nf, *tol;  // [B]
+    double *beta;      // [B] ||w'|| of the last update (DCGS2: the open column's scale)
     int *frozen, *k, *it, *max_iter;   // [B]
-    int *flags;        // [0] second Gram-Schmidt pass wanted, [1] second passes taken, [2] longest k, [3] error
+    int *flags;        // [kArnFlags]: [0] second Gram-Schmidt pass wanted, [1] second passes taken,
+                       // [2] longest k, [3] error, [4] last step run, [5] some p still active
     int m, B;
     double2 *h;        // Krylov scalars: [B][SH], h1 at 0, h2 at M2, norms at 2 M2, y at 3 M2
     int SH, M2;
     double *vs;        // basis scales [B][M2]
 };
+constexpr int kArnFlags = 8;
 // flags[0] = any unfrozen p with ||w||^2 after the first pass < 1/2 of before
 int launch_reorth_check(const ArnState &a, int j, cudaStream_t s);
 // column j of H (h1 + h2 when flags[0]), rotations, g, est, frozen, k, it,
 // vs[j + 1]; sets `next` (if has_next) to "some p is still unfrozen"
 int launch_givens(const ArnState &a, int j, bool has_next, cudaGraphConditionalHandle next, cudaStream_t s);
+// DCGS2 (low-synchronization Gram-Schmidt with delayed reorthogonalization,
+// flexible FGMRES): per step j one reduction (dots2) and one update pass
+// (update2) over the basis.  Krylov scalars per right-hand side: dots at h
+// (2 j + 2 slots), ||w'||^2 at 2 M2, update coefficients alpha at 4 M2 and
+// delta at 5 M2.
+int launch_dots2(const VecBatch &V, long ldv, const ScaleBatch &vs, int j, const VecBatch &w, long N, int R,
+                 const Reduce &red, double2 *out, long sOut, cudaStream_t s, const int *pred, const int *skip);
+int launch_update2(const VecBatch &V, long ldv, int j, const double2 *coef, long sCoef, int M2, const VecBatch &w,
+                   long N, int R, const Reduce &red, double2 *out, long sOut, cudaStream_t s, const int *pred,
+                   const int *skip);
+// reorthogonalization dots of the cycle's last tentative vector V_{jl+1},
+// jl = *jl on the device (tmax: the largest jl + 1)
+int launch_dots_tail(const VecBatch &V, long ldv, const ScaleBatch &vs, int tmax, const int *jl, long N, int R,
+                     const Reduce &red, double2 *out, long sOut, cudaStream_t s, const int *pred, const int *skip);
+// finalize column j - 1, write column j and the update coefficients
+int launch_lagged(const ArnState &a, int j, cudaStream_t s);
+// beta, vs[j + 1], flags[4..5] and the condition of step j + 1
+int launch_post(const ArnState &a, int j, bool has_next, cudaGraphConditionalHandle next, cudaStream_t s);
+// finalize the open column of the cycle's last step
+int launch_lagged_final(const ArnState &a, cudaStream_t s);
 // y = R^{-1} g (k x k per p, zero padded to m) into h at 3 M2; flags[2] = max k
 int launch_backsub(const ArnState &a, cudaStream_t s);
 // out[r].x = ||x_r||^2 over the box [x0,x1) x [y0,y1) x [z0,z1)
@@ -277,6 +300,7 @@ struct helm3d_ctx {
     };
     std::vector<CycleGraph> graphs;
     bool use_graphs = true;
+    bool gs_lowsync = true;                     // mode N: DCGS2 (HELM3D_GS=cgs2: classical CGS2)
     size_t f_cap = 0, u_cap = 0;                // staging capacities (vectors) of d_f, d_u
     double *d_vs = nullptr;
     double2 *d_h = nullptr;        // small device scalars

@@ -79,17 +79,126 @@ __global__ void __launch_bounds__(kRedThreads) dots_kernel(const double2 *__rest
     }
 }
 
+// Low-synchronization Gram-Schmidt (DCGS2, delayed reorthogonalization): one
+// pass over V_0 .. V_j and the new vector w gives, per right-hand side,
+//   slots 0 .. j       b_i = vs_i <V_i, w>      (i <= j)
+//   slots j+1 .. 2j    a_i = vs_i <V_i, V_j>    (i < j: the lagged second
+//                                                projection of V_j)
+//   slot 2j+1          g   = <V_j, V_j>
+// A right-hand side with skip[r] set writes zero partials and reads nothing.
+__global__ void __launch_bounds__(kRedThreads) dots2_kernel(const double2 *__restrict__ V, long ldv, long sV,
+                                                            const double *__restrict__ vs, long sVs, int j,
+                                                            const double2 *__restrict__ w, long sW, long N,
+                                                            double2 *__restrict__ partials, int cap,
+                                                            const int *pred, const int *skip) {
+    __shared__ double2 sh[(kRedThreads / 32) * (2 * kDotChunk + 2)];
+    if (pred && *pred == 0) return;
+    const int r = blockIdx.y;
+    partials += (long)r * gridDim.x * cap + (long)blockIdx.x * cap;
+    if (skip && skip[r]) {
+        for (int q = threadIdx.x; q < 2 * j + 2; q += blockDim.x) partials[q] = make_double2(0, 0);
+        return;
+    }
+    V += r * sV;
+    w += r * sW;
+    vs += r * sVs;
+    const double2 *__restrict__ vj = V + (long)j * ldv;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (int c0 = 0; c0 < j || c0 == 0; c0 += kDotChunk) {
+        // acc[q]: <V_{c0+q}, w>; acc[kDotChunk+q]: <V_{c0+q}, V_j>; then <V_j, w>, |V_j|^2
+        double2 acc[2 * kDotChunk + 2];
+#pragma unroll
+        for (int q = 0; q < 2 * kDotChunk + 2; q++) acc[q] = make_double2(0, 0);
+        const bool first = c0 == 0;
+        for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
+            const double2 wl = w[l], xl = vj[l];
+#pragma unroll
+            for (int q = 0; q < kDotChunk; q++)
+                if (c0 + q < j) {
+                    const double2 v = V[(c0 + q) * ldv + l];
+                    const double2 vc = make_double2(v.x, -v.y);
+                    acc[q] = cfma(vc, wl, acc[q]);
+                    acc[kDotChunk + q] = cfma(vc, xl, acc[kDotChunk + q]);
+                }
+            if (first) {
+                acc[2 * kDotChunk] = cfma(make_double2(xl.x, -xl.y), wl, acc[2 * kDotChunk]);
+                acc[2 * kDotChunk + 1].x += xl.x * xl.x + xl.y * xl.y;
+            }
+        }
+        block_sum<2 * kDotChunk + 2>(acc, sh);
+        if (threadIdx.x == 0) {
+            for (int q = 0; q < kDotChunk && c0 + q < j; q++) {
+                partials[c0 + q] = cscale(acc[q], vs[c0 + q]);
+                partials[j + 1 + c0 + q] = cscale(acc[kDotChunk + q], vs[c0 + q]);
+            }
+            if (first) {
+                partials[j] = cscale(acc[2 * kDotChunk], vs[j]);
+                partials[2 * j + 1] = acc[2 * kDotChunk + 1];
+            }
+        }
+    }
+}
+
+// The delayed reorthogonalization of the last tentative vector V_t of a
+// cycle, t = *jl + 1 (read on the device: the number of steps a graph ran
+// is decided on the device): slots 0 .. t-1 a_i = vs_i <V_i, V_t>, slot t
+// g = <V_t, V_t>.
+__global__ void __launch_bounds__(kRedThreads) dots_tail_kernel(const double2 *__restrict__ V, long ldv, long sV,
+                                                                const double *__restrict__ vs, long sVs,
+                                                                const int *jl, long N,
+                                                                double2 *__restrict__ partials, int cap,
+                                                                const int *pred, const int *skip) {
+    __shared__ double2 sh[(kRedThreads / 32) * (kDotChunk + 1)];
+    if (pred && *pred == 0) return;
+    const int t = *jl + 1;
+    const int r = blockIdx.y;
+    partials += (long)r * gridDim.x * cap + (long)blockIdx.x * cap;
+    if (skip && skip[r]) {
+        for (int q = threadIdx.x; q <= t; q += blockDim.x) partials[q] = make_double2(0, 0);
+        return;
+    }
+    V += r * sV;
+    vs += r * sVs;
+    const double2 *__restrict__ vt = V + (long)t * ldv;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (int c0 = 0; c0 < t; c0 += kDotChunk) {
+        double2 acc[kDotChunk + 1];
+#pragma unroll
+        for (int q = 0; q <= kDotChunk; q++) acc[q] = make_double2(0, 0);
+        const bool first = c0 == 0;
+        for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
+            const double2 xl = vt[l];
+#pragma unroll
+            for (int q = 0; q < kDotChunk; q++)
+                if (c0 + q < t) {
+                    const double2 v = V[(c0 + q) * ldv + l];
+                    acc[q] = cfma(make_double2(v.x, -v.y), xl, acc[q]);
+                }
+            if (first) acc[kDotChunk].x += xl.x * xl.x + xl.y * xl.y;
+        }
+        block_sum<kDotChunk + 1>(acc, sh);
+        if (threadIdx.x == 0) {
+            for (int q = 0; q < kDotChunk && c0 + q < t; q++) partials[c0 + q] = cscale(acc[q], vs[c0 + q]);
+            if (first) partials[t] = acc[kDotChunk];
+        }
+    }
+}
+
 // out[r][i] = sum_b partials[r][b][i]: one block of kFinalThreads per (i, r),
 // threads stride over the block partials, then a fixed shuffle tree
-// (deterministic: the order depends only on nblocks)
+// (deterministic: the order depends only on nblocks).  With nv_dev the
+// count is min(nv, *nv_dev + nv_add).
 constexpr int kFinalThreads = 128;
 __global__ void __launch_bounds__(kFinalThreads) reduce_partials_kernel(const double2 *__restrict__ partials,
                                                                         int nblocks, int cap, int nv,
                                                                         double2 *__restrict__ out, long sOut,
-                                                                        const int *pred) {
+                                                                        const int *pred,
+                                                                        const int *nv_dev = nullptr,
+                                                                        int nv_add = 0) {
     __shared__ double2 sh[kFinalThreads / 32];
     if (pred && *pred == 0) return;
     const int i = blockIdx.x, r = blockIdx.y;
+    if (nv_dev) nv = min(nv, *nv_dev + nv_add);
     if (i >= nv) return;
     partials += (long)r * nblocks * cap;
     double2 s = make_double2(0, 0);
@@ -137,6 +246,49 @@ __global__ void __launch_bounds__(kRedThreads) update_kernel(const double2 *__re
         block_sum<1>(nrm, sh);
         if (threadIdx.x == 0) partials[(long)r * gridDim.x * cap + (long)blockIdx.x * cap] = nrm[0];
     }
+}
+
+// The DCGS2 update pass: with alpha = coef[0 .. j-1], delta = coef[M2 .. M2+j]
+//   V_j <- V_j - sum_{i<j} alpha_i V_i                 (j > 0)
+//   w   <- w - sum_{i<j} delta_i V_i - delta_j V_j(old)
+// and ||w||^2 partials; skip[r] set: zero partials, nothing read or written.
+__global__ void __launch_bounds__(kRedThreads) update2_kernel(double2 *__restrict__ V, long ldv, long sV, int j,
+                                                              const double2 *__restrict__ coef, long sCoef, int M2,
+                                                              double2 *__restrict__ w, long sW, long N,
+                                                              double2 *__restrict__ partials, int cap,
+                                                              const int *pred, const int *skip) {
+    extern __shared__ double2 sc[];  // alpha[j], delta[j + 1]
+    __shared__ double2 sh[(kRedThreads / 32)];
+    if (pred && *pred == 0) return;
+    const int r = blockIdx.y;
+    if (skip && skip[r]) {
+        if (threadIdx.x == 0) partials[(long)r * gridDim.x * cap + (long)blockIdx.x * cap] = make_double2(0, 0);
+        return;
+    }
+    V += r * sV;
+    w += r * sW;
+    coef += r * sCoef;
+    double2 *alpha = sc, *delta = sc + j;
+    for (int i = threadIdx.x; i < j; i += blockDim.x) alpha[i] = coef[i];
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) delta[i] = coef[M2 + i];
+    __syncthreads();
+    double2 *__restrict__ vj = V + (long)j * ldv;
+    double2 nrm[1] = {make_double2(0, 0)};
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
+        double2 x = vj[l];
+        double2 acc = cfms(delta[j], x, w[l]);
+        for (int i = 0; i < j; i++) {
+            const double2 v = V[i * ldv + l];
+            x = cfms(alpha[i], v, x);
+            acc = cfms(delta[i], v, acc);
+        }
+        if (j > 0) vj[l] = x;
+        w[l] = acc;
+        nrm[0].x += acc.x * acc.x + acc.y * acc.y;
+    }
+    block_sum<1>(nrm, sh);
+    if (threadIdx.x == 0) partials[(long)r * gridDim.x * cap + (long)blockIdx.x * cap] = nrm[0];
 }
 
 // x += sum_i y[i] zs[i] Z_i  (i < *nzv_dev when given, else nzv)
@@ -255,6 +407,40 @@ int launch_update(const VecBatch &V, long ldv, const ScaleBatch &vs, int nv, con
         V.p, ldv, V.stride, vs.p, vs.stride, nv, coef, sCoef, w.p, w.stride, N, post, red.partials, red.cap, pred);
     if (post == 1)
         reduce_partials_kernel<<<dim3(1, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, 1, out, sOut, pred);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_dots2(const VecBatch &V, long ldv, const ScaleBatch &vs, int j, const VecBatch &w, long N, int R,
+                 const Reduce &red, double2 *out, long sOut, cudaStream_t s, const int *pred, const int *skip) {
+    const int nout = 2 * j + 2;
+    if (nout > red.cap || R > red.rmax) return HELM3D_ERR_ARG;
+    const int nb = red.nblocks;
+    dots2_kernel<<<dim3(nb, R), kRedThreads, 0, s>>>(V.p, ldv, V.stride, vs.p, vs.stride, j, w.p, w.stride, N,
+                                                     red.partials, red.cap, pred, skip);
+    reduce_partials_kernel<<<dim3(nout, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, nout, out, sOut,
+                                                                    pred);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_dots_tail(const VecBatch &V, long ldv, const ScaleBatch &vs, int tmax, const int *jl, long N, int R,
+                     const Reduce &red, double2 *out, long sOut, cudaStream_t s, const int *pred, const int *skip) {
+    if (tmax + 1 > red.cap || R > red.rmax) return HELM3D_ERR_ARG;
+    const int nb = red.nblocks;
+    dots_tail_kernel<<<dim3(nb, R), kRedThreads, 0, s>>>(V.p, ldv, V.stride, vs.p, vs.stride, jl, N, red.partials,
+                                                         red.cap, pred, skip);
+    reduce_partials_kernel<<<dim3(tmax + 1, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, tmax + 1, out,
+                                                                        sOut, pred, jl, 2);
+    return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+int launch_update2(const VecBatch &V, long ldv, int j, const double2 *coef, long sCoef, int M2, const VecBatch &w,
+                   long N, int R, const Reduce &red, double2 *out, long sOut, cudaStream_t s, const int *pred,
+                   const int *skip) {
+    if (R > red.rmax) return HELM3D_ERR_ARG;
+    const int nb = red.nblocks;
+    update2_kernel<<<dim3(nb, R), kRedThreads, sizeof(double2) * (2 * j + 1), s>>>(
+        V.p, ldv, V.stride, j, coef, sCoef, M2, w.p, w.stride, N, red.partials, red.cap, pred, skip);
+    reduce_partials_kernel<<<dim3(1, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, 1, out, sOut, pred);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 

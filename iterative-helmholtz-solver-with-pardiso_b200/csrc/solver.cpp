@@ -49,17 +49,18 @@ static Reduce reducer(helm3d_ctx *c) {
     return r;
 }
 
-// small per-right-hand-side device scalars: h1 | h2 | norms | y, each m+2 long
-static int scalars_per_rhs(int m) { return 4 * (m + 2); }
+// small per-right-hand-side device scalars, each region m+2 long:
+// h1 | h2 | norms | y | alpha | delta  (DCGS2 dots span h1 and h2)
+static int scalars_per_rhs(int m) { return 6 * (m + 2); }
 
 // bytes of the device Arnoldi state for R right-hand sides and restart m
 static size_t arn_bytes(int m, int R) {
     return sizeof(double2) * (size_t)R * ((size_t)(m + 1) * m + 2 * m + (m + 1)) +
-           sizeof(double) * (size_t)R * (m + 2) + sizeof(int) * ((size_t)4 * R + 4) + 256;
+           sizeof(double) * (size_t)R * (m + 3) + sizeof(int) * ((size_t)4 * R + kArnFlags) + 256;
 }
 
 // the state arrays of a batch of B (restart m) carved from c->d_arn:
-// doubles first (est, nf, tol), then ints (frozen, k, it, max_iter, flags)
+// doubles first (est, nf, tol, beta), then ints (frozen, k, it, max_iter, flags)
 static ArnState arn_state(helm3d_ctx *c, int m, int B) {
     ArnState a;
     const int R = c->r_alloc;
@@ -76,7 +77,8 @@ static ArnState arn_state(helm3d_ctx *c, int m, int B) {
     q += sizeof(double) * (size_t)R * m;
     a.nf = (double *)q;
     a.tol = a.nf + R;
-    q += sizeof(double) * (size_t)2 * R;
+    a.beta = a.tol + R;
+    q += sizeof(double) * (size_t)3 * R;
     a.frozen = (int *)q;
     a.k = a.frozen + R;
     a.it = a.k + R;
@@ -86,7 +88,7 @@ static ArnState arn_state(helm3d_ctx *c, int m, int B) {
     a.B = B;
     a.h = c->d_h;
     a.M2 = m + 2;
-    a.SH = 4 * (m + 2);
+    a.SH = scalars_per_rhs(m);
     a.vs = c->d_vs;
     return a;
 }
@@ -120,7 +122,7 @@ int ensure_krylov(helm3d_ctx *c, int m, int R) {
         total += bytes;
         return cuda_check(c, cudaMalloc(p, bytes), what);
     };
-    c->red_cap = std::max(m + 2, 8);
+    c->red_cap = std::max(2 * m + 4, 8);
     c->red_blocks = 2 * device_info().sm_count;
     int rc;
     if ((rc = get((void **)&c->d_V, vb * (m + 1) * R, "Krylov basis V")) ||
@@ -372,6 +374,11 @@ static void givens(zc a, zc b, zc &cs, zc &sn) {
     }
 }
 
+// Mode N (flexible) uses DCGS2, the low-synchronization Gram-Schmidt with
+// delayed reorthogonalization, unless HELM3D_GS=cgs2 selects classical
+// Gram-Schmidt with the conditional second pass.
+static bool lowsync(const helm3d_ctx *c) { return c->opts.mode == HELM3D_MODE_N && c->gs_lowsync; }
+
 // ------------------------------------------------ restart cycle as a graph
 // One Arnoldi step j of a batch of B, kernels only: the operator and
 // preconditioner applications, classical Gram-Schmidt with its norms, the
@@ -399,6 +406,19 @@ static int arnoldi_step(helm3d_ctx *c, int m, int B, int j, bool adjoint, const 
     } else {
         RC(apply_op(c, Vj, 1.0, vsj, w, B));
     }
+    if (lowsync(c)) {
+        // DCGS2: one reduction (w against V_0..V_j, the lagged second
+        // projection of V_j), the bookkeeping, one update pass
+        RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+            return launch_dots2(Vall, N, vsb, j, w, N, B, red, d_h1, SH, c->stream, nullptr, a.frozen);
+        }));
+        RC(timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_lagged(a, j, c->stream); }));
+        RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+            return launch_update2(Vall, N, j, Hd + 4 * M2, SH, M2, w, N, B, red, d_nrm, SH, c->stream, nullptr,
+                                  a.frozen);
+        }));
+        return timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_post(a, j, has_next, next, c->stream); });
+    }
     RC(timed(c, HELM3D_K_KRYLOV, 2,
              [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h1, SH, c->stream, true); }));
     RC(timed(c, HELM3D_K_KRYLOV, 2,
@@ -419,6 +439,15 @@ static int cycle_tail(helm3d_ctx *c, int m, int B, const ArnState &a) {
     const long ldV = (long)(m + 1) * N, ldZ = (long)m * N;
     const int M2 = m + 2, SH = scalars_per_rhs(m);
     double2 *d_y = c->d_h + 3 * M2;
+    if (lowsync(c)) {
+        // the open column of the last step (skipped when every right-hand
+        // side stopped inside the cycle)
+        RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+            return launch_dots_tail(VecBatch{c->d_V, ldV}, N, ScaleBatch{c->d_vs, M2}, m, a.flags + 4, N, B,
+                                    reducer(c), c->d_h, SH, c->stream, a.flags + 5, a.frozen);
+        }));
+        RC(timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_lagged_final(a, c->stream); }));
+    }
     RC(timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_backsub(a, c->stream); }));
     return timed(c, HELM3D_K_KRYLOV, 1, [&] {
         return c->opts.mode == HELM3D_MODE_N
@@ -642,12 +671,14 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, hel
         const VecBatch Vall{V, ldV};
         const ScaleBatch vsb{c->d_vs, M2};
         const int gi = (c->use_graphs && !c->prof && !o.verbose) ? cycle_graph(c, m, B, adjoint) : -1;
-        if (gi >= 0) {
-            // the whole cycle on the device: state in, one graph launch, state out
+        if (gi >= 0 || lowsync(c)) {
+            // the whole cycle on the device: state in, one graph launch (or
+            // the steps launched one by one, the host checking after each
+            // whether some right-hand side is still active), state out
             const ArnState a = arn_state(c, m, B);
             const int Ra = c->r_alloc;
             std::vector<double> dv((size_t)2 * Ra, 0.0);
-            std::vector<int> iv((size_t)4 * Ra + 4, 0);
+            std::vector<int> iv((size_t)4 * Ra + kArnFlags, 0);
             std::vector<double2> g0((size_t)B);
             for (int p = 0; p < B; p++) {
                 const Rhs &r = S[act[p]];
@@ -666,7 +697,22 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, hel
             RC(cuda_check(c, cudaMemcpy2DAsync(a.g, sizeof(double2) * (m + 1), g0.data(), sizeof(double2),
                                                sizeof(double2), B, cudaMemcpyHostToDevice, c->stream),
                           "cycle state"));
-            RC(cuda_check(c, cudaGraphLaunch(c->graphs[gi].exec, c->stream), "cycle graph"));
+            if (gi >= 0) {
+                RC(cuda_check(c, cudaGraphLaunch(c->graphs[gi].exec, c->stream), "cycle graph"));
+            } else {
+                RC(ensure_planes(c, B));
+                for (int j = 0; j < m; j++) {
+                    RC(arnoldi_step(c, m, B, j, adjoint, a, false, 0));
+                    int active = 0;
+                    RC(cuda_check(c, cudaMemcpyAsync(&active, a.flags + 5, sizeof(int), cudaMemcpyDeviceToHost,
+                                                     c->stream),
+                                  "active"));
+                    RC(cuda_check(c, cudaStreamSynchronize(c->stream), "step"));
+                    if (o.verbose) fprintf(stderr, "helm3d: step %d, %s\n", j + 1, active ? "active" : "done");
+                    if (!active) break;
+                }
+                RC(cycle_tail(c, m, B, a));
+            }
             std::vector<double> est((size_t)Ra * m);
             RC(cuda_check(c, cudaMemcpyAsync(iv.data(), a.frozen, sizeof(int) * iv.size(), cudaMemcpyDeviceToHost,
                                              c->stream),
@@ -679,7 +725,8 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, hel
             if (flags[3]) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
             const int kmax = flags[2];
             c->reorth += flags[1];
-            c->launches += kmax * c->graphs[gi].kernels_per_step + c->graphs[gi].tail_kernels;
+            if (gi >= 0)   // steps run = last step index + 1
+                c->launches += (flags[4] + 1) * c->graphs[gi].kernels_per_step + c->graphs[gi].tail_kernels;
             for (int p = 0; p < B; p++) {
                 Rhs &r = S[act[p]];
                 r.it = iv[2 * Ra + p];
