@@ -131,6 +131,19 @@ int helm3d_set_medium(helm3d_ctx *ctx, const double *s2);
  * Source/templates.h:59), which the reference calls once per source. */
 int helm3d_solve(helm3d_ctx *ctx, const double *f, double *u, int nrhs, helm3d_stats *stats);
 
+/* Solve n contexts at once: grids of different sizes, each with its own
+ * medium, options and factor, on one device.  Context i solves nrhs[i]
+ * right-hand sides f[i] -> u[i] (host or device pointers, laid out as for
+ * helm3d_solve).  The contexts iterate FGMRES in lockstep restart cycles,
+ * and each cycle of all of them is one CUDA graph whose independent branches
+ * (one per context) run side by side on the GPU, so that small grids that
+ * cannot fill it alone share it.  The work is ordered on the first context's
+ * stream; stats (n entries, or NULL) are per context.  A context may appear
+ * only once.  No counterpart in the reference, which solves one grid per
+ * run (Source/main.cpp:470). */
+int helm3d_solve_group(helm3d_ctx *const *ctxs, int n, const double *const *f, double *const *u, const int *nrhs,
+                       helm3d_stats *stats);
+
 /* The same system by BiCGStab with the reference's shadow residual 2 r0.
  * Replaces BCGSTAB (Source/BcGSTAB.cpp:6-666, Source/templates.h:60). */
 int helm3d_solve_bicgstab(helm3d_ctx *ctx, const double *f, double *u, helm3d_stats *stats);

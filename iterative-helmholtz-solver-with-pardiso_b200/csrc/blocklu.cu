@@ -123,8 +123,10 @@ template <typename R, int NP, int NPC> constexpr size_t factor_smem_bytes() {
            16 + sizeof(uint64_t) * 2 * kRing;
 }
 
-template <typename R, int NP, int NW, int CB, int C>
-__global__ void __launch_bounds__(NW * 32, 1) factor_kernel(FactorK<R> a) {
+// MB: CTAs per SM the register budget is planned for (2 lets two kz chains
+// share an SM and hide each other's pivot-step latency)
+template <typename R, int NP, int NW, int CB, int C, int MB>
+__global__ void __launch_bounds__(NW * 32, MB) factor_kernel(FactorK<R> a) {
     constexpr int RB = NP / 32;
     constexpr int NPC = NP / C;
     static_assert(NW * CB == NPC, "columns per CTA must equal warps x columns per warp");
@@ -366,11 +368,7 @@ __global__ void __launch_bounds__(NW * 32, 1) factor_kernel(FactorK<R> a) {
 }
 
 // ------------------------------------------------------------------ launch
-struct FactorCfg {
-    int np, nw, cb, c;
-};
-
-template <typename R, int NP, int NW, int CB, int C>
+template <typename R, int NP, int NW, int CB, int C, int MB>
 static int launch_cfg(const FactorArgs &fa, cudaStream_t st) {
     FactorK<R> k;
     k.n = fa.n;
@@ -386,7 +384,7 @@ static int launch_cfg(const FactorArgs &fa, cudaStream_t st) {
     k.kz2 = (const cplx<R> *)fa.kz2;
     k.status = fa.status;
     constexpr size_t smem = factor_smem_bytes<R, NP, NP / C>();
-    auto kern = factor_kernel<R, NP, NW, CB, C>;
+    auto kern = factor_kernel<R, NP, NW, CB, C, MB>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return HELM3D_ERR_CUDA;
     cudaLaunchConfig_t cfg = {};
@@ -405,40 +403,64 @@ static int launch_cfg(const FactorArgs &fa, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
-// padded block sizes and their thread/cluster shapes, smallest first
-static int factor_np(bool c64, int n) {
-    static const int np64[] = {32, 64, 96, 128, 192, 256};
-    static const int np128[] = {32, 64, 96, 128, 192, 256};
-    const int *t = c64 ? np64 : np128;
-    for (int q = 0; q < 6; q++)
-        if (n <= t[q]) return t[q];
-    return 0;
+// The launch shapes of the factor (padded block NP, warps NW, columns per
+// warp CB, cluster size C, CTAs per SM planned MB), smallest NP first; for a
+// block size n the autotuner times every shape of the smallest NP >= n (the
+// first is the default).
+typedef int (*FactorLaunch)(const FactorArgs &, cudaStream_t);
+struct FactorShape {
+    int np;
+    FactorLaunch fn;
+};
+static const FactorShape kShapes64[] = {
+    {32, launch_cfg<float, 32, 4, 8, 1, 1>},
+    {64, launch_cfg<float, 64, 8, 8, 1, 1>},
+    {96, launch_cfg<float, 96, 12, 8, 1, 1>},
+    {128, launch_cfg<float, 128, 16, 8, 1, 1>},
+    {128, launch_cfg<float, 128, 8, 8, 2, 1>},
+    {192, launch_cfg<float, 192, 12, 8, 2, 1>},
+    {224, launch_cfg<float, 224, 7, 8, 4, 1>},
+    {224, launch_cfg<float, 224, 7, 4, 8, 2>},
+    {256, launch_cfg<float, 256, 8, 8, 4, 1>},
+    {256, launch_cfg<float, 256, 8, 4, 8, 2>},
+};
+static const FactorShape kShapes128[] = {
+    {32, launch_cfg<double, 32, 8, 4, 1, 1>},
+    {64, launch_cfg<double, 64, 16, 4, 1, 1>},
+    {96, launch_cfg<double, 96, 12, 4, 2, 1>},
+    {128, launch_cfg<double, 128, 8, 4, 4, 1>},
+    {192, launch_cfg<double, 192, 12, 4, 4, 1>},
+    {224, launch_cfg<double, 224, 7, 4, 8, 1>},
+    {256, launch_cfg<double, 256, 8, 4, 8, 1>},
+};
+
+template <size_t K> static void shapes_for(const FactorShape (&t)[K], int n, int &first, int &count) {
+    first = -1;
+    count = 0;
+    for (size_t q = 0; q < K; q++) {
+        if (t[q].np < n) continue;
+        if (first < 0) first = (int)q;
+        if (t[q].np != t[first].np) break;
+        count++;
+    }
 }
 
-bool factor_supported(bool c64, int n) { return n >= 1 && factor_np(c64, n) != 0; }
+int factor_variants(bool c64, int n) {
+    int first, count;
+    if (c64) shapes_for(kShapes64, n, first, count);
+    else shapes_for(kShapes128, n, first, count);
+    return count;
+}
 
-int launch_factor(bool c64, const FactorArgs &fa, cudaStream_t s) {
-    const int np = factor_np(c64, fa.n);
-    if (c64) {
-        switch (np) {
-            case 32: return launch_cfg<float, 32, 4, 8, 1>(fa, s);
-            case 64: return launch_cfg<float, 64, 8, 8, 1>(fa, s);
-            case 96: return launch_cfg<float, 96, 12, 8, 1>(fa, s);
-            case 128: return launch_cfg<float, 128, 16, 8, 1>(fa, s);
-            case 192: return launch_cfg<float, 192, 12, 8, 2>(fa, s);
-            case 256: return launch_cfg<float, 256, 8, 8, 4>(fa, s);
-        }
-    } else {
-        switch (np) {
-            case 32: return launch_cfg<double, 32, 8, 4, 1>(fa, s);
-            case 64: return launch_cfg<double, 64, 16, 4, 1>(fa, s);
-            case 96: return launch_cfg<double, 96, 12, 4, 2>(fa, s);
-            case 128: return launch_cfg<double, 128, 8, 4, 4>(fa, s);
-            case 192: return launch_cfg<double, 192, 12, 4, 4>(fa, s);
-            case 256: return launch_cfg<double, 256, 8, 4, 8>(fa, s);
-        }
-    }
-    return HELM3D_ERR_ARG;
+bool factor_supported(bool c64, int n) { return n >= 1 && factor_variants(c64, n) > 0; }
+
+int launch_factor(bool c64, const FactorArgs &fa, cudaStream_t s, int variant) {
+    int first, count;
+    if (c64) shapes_for(kShapes64, fa.n, first, count);
+    else shapes_for(kShapes128, fa.n, first, count);
+    if (count == 0) return HELM3D_ERR_ARG;
+    if (variant < 0 || variant >= count) variant = 0;
+    return (c64 ? kShapes64 : kShapes128)[first + variant].fn(fa, s);
 }
 
 }  // namespace h3d

@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <memory>
 #include <new>
 #include <vector>
 
@@ -270,6 +271,95 @@ static int solve_common(helm3d_ctx *c, const double *f, double *u, int nrhs, hel
 
 int helm3d_solve(helm3d_ctx *c, const double *f, double *u, int nrhs, helm3d_stats *st) {
     return solve_common(c, f, u, nrhs, st, 0);
+}
+
+int helm3d_solve_group(helm3d_ctx *const *ctxs, int n, const double *const *f, double *const *u, const int *nrhs,
+                       helm3d_stats *stats) {
+    if (!ctxs || n < 1 || !f || !u || !nrhs) return HELM3D_ERR_ARG;
+    for (int i = 0; i < n; i++) {
+        helm3d_ctx *c = ctxs[i];
+        if (!c) return HELM3D_ERR_ARG;
+        if (!f[i] || !u[i] || nrhs[i] < 1) return set_error(c, HELM3D_ERR_ARG, "solve_group: bad vector arguments");
+        if (c->device != ctxs[0]->device) return set_error(c, HELM3D_ERR_ARG, "solve_group: contexts on two devices");
+        for (int q = 0; q < i; q++)
+            if (ctxs[q] == c) return set_error(c, HELM3D_ERR_ARG, "solve_group: a context appears twice");
+    }
+    cudaSetDevice(ctxs[0]->device);
+    // every context's work (staging included) on the first context's stream
+    // for the call
+    struct Guard {
+        std::vector<helm3d_ctx *> cs;
+        std::vector<cudaStream_t> saved;
+        ~Guard() {
+            for (size_t i = 0; i < cs.size(); i++) cs[i]->stream = saved[i];
+        }
+    } guard;
+    for (int i = 0; i < n; i++) {
+        guard.cs.push_back(ctxs[i]);
+        guard.saved.push_back(ctxs[i]->stream);
+        ctxs[i]->stream = ctxs[0]->stream;
+        if (stats) {
+            helm3d_stats &s = stats[i];
+            s.iterations = 0;
+            s.restarts = 0;
+            s.ms_solve = 0;
+            s.relres = 0;
+            s.relres_phys = 0;
+            s.history_len = 0;
+            s.status = HELM3D_OK;
+        }
+    }
+    // batch per context, each sized after the earlier contexts' workspace
+    std::vector<int> Bc(n);
+    int rounds = 0;
+    for (int i = 0; i < n; i++) {
+        helm3d_ctx *c = ctxs[i];
+        const bool staged = !is_device_ptr(f[i]) || !is_device_ptr(u[i]);
+        Bc[i] = batch_size(c, nrhs[i], staged);
+        int rc = ensure_krylov(c, std::max(1, c->opts.restart), Bc[i]);
+        if (rc) return rc;
+        rounds = std::max(rounds, (nrhs[i] + Bc[i] - 1) / Bc[i]);
+    }
+    int worst = HELM3D_OK;
+    for (int t = 0; t < rounds; t++) {
+        std::vector<helm3d_ctx *> cs;
+        std::vector<const double2 *> fd;
+        std::vector<double2 *> ud;
+        std::vector<int> Rs;
+        std::vector<helm3d_stats *> sts;
+        std::vector<std::unique_ptr<VecArg>> fa, ua;
+        std::vector<double *> uh;
+        std::vector<size_t> counts;
+        for (int i = 0; i < n; i++) {
+            const int r0 = t * Bc[i];
+            if (r0 >= nrhs[i]) continue;
+            helm3d_ctx *c = ctxs[i];
+            const int R = std::min(Bc[i], nrhs[i] - r0);
+            const size_t count = (size_t)R * c->N;
+            const double *fr = f[i] + 2 * (size_t)r0 * c->N;
+            double *ur = u[i] + 2 * (size_t)r0 * c->N;
+            fa.emplace_back(new VecArg(c, fr, count, true, &c->d_f, &c->f_cap));
+            if (fa.back()->rc) return fa.back()->rc;
+            ua.emplace_back(new VecArg(c, ur, count, false, &c->d_u, &c->u_cap));
+            if (ua.back()->rc) return ua.back()->rc;
+            cs.push_back(c);
+            fd.push_back(fa.back()->dev);
+            ud.push_back(ua.back()->dev);
+            Rs.push_back(R);
+            sts.push_back(stats ? &stats[i] : nullptr);
+            uh.push_back(ur);
+            counts.push_back(count);
+        }
+        int rc = fgmres_group(cs.data(), (int)cs.size(), fd.data(), ud.data(), Rs.data(), sts.data());
+        if (rc && rc != HELM3D_ERR_NOT_CONVERGED) return rc;
+        if (rc) worst = rc;
+        for (size_t q = 0; q < cs.size(); q++) {
+            if (sts[q] && rc) sts[q]->status = rc;
+            const int rc2 = ua[q]->copy_out(uh[q], counts[q]);
+            if (rc2) return rc2;
+        }
+    }
+    return worst;
 }
 
 int helm3d_solve_bicgstab(helm3d_ctx *c, const double *f, double *u, helm3d_stats *st) {

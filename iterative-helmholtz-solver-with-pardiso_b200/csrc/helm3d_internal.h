@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <complex>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -94,7 +95,9 @@ struct FactorArgs {
     const void *kz2;          // cplx<P>[nz]: complex shift of mode k (-kz^2 or lambda_k)
     int *status;              // device flag: bit 0 = zero pivot
 };
-int launch_factor(bool c64, const FactorArgs &a, cudaStream_t s);
+// variant: one of the factor_variants(c64, n) launch shapes (0: the default)
+int launch_factor(bool c64, const FactorArgs &a, cudaStream_t s, int variant = 0);
+int factor_variants(bool c64, int n);
 bool factor_supported(bool c64, int n);
 
 // Forward/backward block sweep over y-lines for every kz and all R
@@ -107,8 +110,13 @@ struct SweepArgs {
     int R;
     const void *dxy;          // null: S^{-1}; else S^{-H} with the [2][ny][n] alpha_x alpha_y table
     int *status;              // device flag: bit 2 = a bounded wait expired
+    int stage_kb = 16;        // bulk-copy stage of G^T rows (KB, about)
+    int ring_kb = 200;        // shared-memory ring of stages (KB, at most)
 };
 int launch_sweep(bool c64, const SweepArgs &a, cudaStream_t s);
+// the sweep's launch variants (stage and ring sizes) the autotuner times
+constexpr int kSweepVariants = 6;
+void sweep_variant(int v, int &stage_kb, int &ring_kb);
 constexpr int kMaxBatch = 16;  // right-hand sides per preconditioner launch
 
 // Classical Gram-Schmidt takes a second pass when the first left less than
@@ -130,6 +138,7 @@ struct StencilArgs {
     VecBatch y;
     VecBatch f;               // if f.p: y = f - A x
     int R;
+    int zchunk = 16;          // z points per thread (autotuned: 8, 16, 32, 64)
 };
 int launch_stencil(const StencilArgs &a, bool adjoint, cudaStream_t s);
 
@@ -228,6 +237,17 @@ int launch_grad_accum(const VecBatch &lam, const VecBatch &u, int R, double w2, 
 
 Dev &device_info();
 
+// ------------------------------------------------------------- autotuner
+// The fastest of nvariants launch shapes of a kernel family for a problem
+// shape: launch(v) runs variant v once on the context's stream; the choice is
+// cached per (family, shape) for the process (and in HELM3D_TUNE_CACHE).
+// Not for use inside a stream capture.
+bool tune_enabled();
+constexpr int kStencilVariants = 4;   // z chunk 16, 8, 32, 64
+constexpr int kReduceVariants = 3;    // reduction blocks 2, 1, 4 per SM
+int stencil_zchunk(int v);
+int reduce_blocks(int v);
+
 }  // namespace h3d
 
 // ---------------------------------------------------------------- context
@@ -301,6 +321,12 @@ struct helm3d_ctx {
     std::vector<CycleGraph> graphs;
     bool use_graphs = true;
     bool gs_lowsync = true;                     // mode N: DCGS2 (HELM3D_GS=cgs2: classical CGS2)
+    // autotuned launch variants: the factor's, and the sweep's (forward,
+    // adjoint) and stencil's of the current solve's batch (reduction blocks:
+    // red_blocks)
+    int tv_factor = 0;
+    int tv_sweep[2] = {0, 0};
+    int tv_stencil = 0;
     size_t f_cap = 0, u_cap = 0;                // staging capacities (vectors) of d_f, d_u
     double *d_vs = nullptr;
     double2 *d_h = nullptr;        // small device scalars
@@ -334,6 +360,11 @@ template <class F> int timed(helm3d_ctx *c, int kind, int kernels, F &&f) {
     return rc;
 }
 
+int tune_pick(helm3d_ctx *c, const char *family, const std::string &shape, int nvariants,
+              const std::function<int(int)> &launch);
+// tune the solve-time kernels (sweep, stencil, reductions) of a batch of R
+// (and the adjoint forms) on the context's own buffers, before any capture
+int tune_solve(helm3d_ctx *c, int R, bool adjoint);
 int ctx_setup_grid(helm3d_ctx *c);                                   // grid/option tables, allocations
 int ctx_setup_medium(helm3d_ctx *c, const double *s2, bool s2_on_device);  // medium tables
 int ctx_factor(helm3d_ctx *c);
@@ -347,6 +378,11 @@ int apply_prec_adjoint(helm3d_ctx *c, const VecBatch &x, double xscale, const Sc
                        int R);
 // FGMRES on R right-hand sides f + r N -> u + r N (device), iterated in lockstep
 int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, helm3d_stats *st);
+// FGMRES on n contexts at once (R[i] <= kMaxBatch right-hand sides of device
+// vectors f[i] -> u[i] each): every restart cycle of every context in one
+// graph launch on the first context's stream
+int fgmres_group(helm3d_ctx *const *cs, int n, const double2 *const *f, double2 *const *u, const int *R,
+                 helm3d_stats *const *st);
 int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st);
 int ensure_krylov(helm3d_ctx *c, int m, int R);
 int set_error(helm3d_ctx *c, int code, const std::string &msg);

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
@@ -506,7 +507,26 @@ int ctx_factor(helm3d_ctx *c) {
     a.base2d = c->d_base2d;
     a.kz2 = c->d_kz2;
     a.status = c->d_status;
-    rc = timed(c, HELM3D_K_FACTOR, 1, [&] { return launch_factor(c->c64, a, c->stream); });
+    const int nv = factor_variants(c->c64, a.n);
+    if (nv > 1) {
+        // the launch shapes of this block size, timed once per process; the
+        // device status (set-up flags included) is kept across the tuning runs
+        char shape[96];
+        std::snprintf(shape, sizeof(shape), "%d|%d|%d|%d", c->c64 ? 64 : 128, a.n, a.ny, a.nz);
+        int st0 = 0;
+        rc = cuda_check(c, cudaMemcpyAsync(&st0, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+                        "status");
+        if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "status");
+        if (rc) return rc;
+        c->tv_factor = tune_pick(c, "FACTOR", shape, nv, [&](int v) { return launch_factor(c->c64, a, c->stream, v); });
+        rc = cuda_check(c, cudaMemcpyAsync(c->d_status, &st0, sizeof(int), cudaMemcpyHostToDevice, c->stream),
+                        "status");
+        if (!rc) rc = cuda_check(c, cudaStreamSynchronize(c->stream), "status");
+        if (rc) return rc;
+    } else {
+        c->tv_factor = 0;
+    }
+    rc = timed(c, HELM3D_K_FACTOR, 1, [&] { return launch_factor(c->c64, a, c->stream, c->tv_factor); });
     if (rc) return set_error(c, rc, std::string("factor launch failed: ") + cudaGetErrorString(cudaGetLastError()));
     int st = 0;
     rc = cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");

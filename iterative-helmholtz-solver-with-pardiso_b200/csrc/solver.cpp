@@ -25,7 +25,10 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <memory>
 
 #include "helm3d_internal.h"
 
@@ -123,13 +126,16 @@ int ensure_krylov(helm3d_ctx *c, int m, int R) {
         return cuda_check(c, cudaMalloc(p, bytes), what);
     };
     c->red_cap = std::max(2 * m + 4, 8);
-    c->red_blocks = 2 * device_info().sm_count;
+    c->red_blocks = reduce_blocks(0);
+    // partials for the largest reduction grid the autotuner may pick
+    int red_max = 0;
+    for (int v = 0; v < kReduceVariants; v++) red_max = std::max(red_max, reduce_blocks(v));
     int rc;
     if ((rc = get((void **)&c->d_V, vb * (m + 1) * R, "Krylov basis V")) ||
         (c->opts.mode == HELM3D_MODE_N && (rc = get((void **)&c->d_Z, vb * m * R, "Krylov basis Z"))) ||
         (rc = get((void **)&c->d_vs, sizeof(double) * (m + 2) * R, "basis scales")) ||
         (rc = get((void **)&c->d_h, sizeof(double2) * scalars_per_rhs(m) * R, "Krylov scalars")) ||
-        (rc = get((void **)&c->d_partials, sizeof(double2) * c->red_cap * c->red_blocks * R, "partials")) ||
+        (rc = get((void **)&c->d_partials, sizeof(double2) * c->red_cap * red_max * R, "partials")) ||
         (rc = get((void **)&c->d_Fw, vb * R, "packed right-hand sides")) ||
         (rc = get((void **)&c->d_Uw, vb * R, "packed iterates")) ||
         (rc = get(&c->d_arn, arn_bytes(m, R), "Arnoldi state"))) {
@@ -187,6 +193,7 @@ static SweepArgs sweep_args(helm3d_ctx *c, int R, bool adjoint) {
     s.R = R;
     s.dxy = adjoint ? c->d_dxy : nullptr;
     s.status = c->d_status;
+    sweep_variant(c->tv_sweep[adjoint ? 1 : 0], s.stage_kb, s.ring_kb);
     return s;
 }
 
@@ -262,6 +269,7 @@ static StencilArgs stencil_args(helm3d_ctx *c, const VecBatch &x, double xscale,
     a.y = y;
     a.f = f;
     a.R = R;
+    a.zchunk = stencil_zchunk(c->tv_stencil);
     return a;
 }
 
@@ -458,31 +466,27 @@ static int cycle_tail(helm3d_ctx *c, int m, int B, const ArnState &a) {
     });
 }
 
-// The cycle graph of a batch of B: m conditional (IF) nodes in sequence, the
-// body of node j holding step j, then the tail.  Step 0 always runs; the
-// Givens kernel of step j sets the condition of step j + 1.  Built once per
-// (B, adjoint) and kept until the workspace moves.  Returns the index in
-// c->graphs, or -1 when graphs are unavailable (the caller falls back to
-// the host-driven cycle).
-static int cycle_graph(helm3d_ctx *c, int m, int B, bool adjoint) {
-    for (size_t q = 0; q < c->graphs.size(); q++)
-        if (c->graphs[q].B == B && c->graphs[q].adjoint == adjoint) return (int)q;
-    if (ensure_planes(c, B)) return -1;   // every allocation before the capture
+// Adds the restart cycle of context c (a batch of B) to graph G as one more
+// chain of root nodes: m conditional (IF) nodes in sequence, the body of
+// node j holding step j, then the tail.  Step 0 always runs; the bookkeeping
+// kernel of step j sets the condition of step j + 1.  The chain's kernels
+// are recorded on c's launch count per step (per_step) and at the tail.
+// Every allocation happens before the captures.
+static bool add_cycle(cudaGraph_t G, helm3d_ctx *c, int m, int B, bool adjoint, long long &per_step,
+                      long long &tail) {
+    if (ensure_planes(c, B)) return false;
     const ArnState a = arn_state(c, m, B);
     cudaStream_t cap = nullptr;
     if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
-        return -1;
+        return false;
     }
     cudaStream_t saved = c->stream;
     const bool prof = c->prof;
     const long long launches0 = c->launches;
     c->stream = cap;
     c->prof = false;
-    cudaGraph_t G = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    long long per_step = 0, tail = 0;
-    bool ok = cudaGraphCreate(&G, 0) == cudaSuccess;
+    bool ok = true;
     std::vector<cudaGraphConditionalHandle> hs(m);
     for (int j = 0; ok && j < m; j++)
         ok = cudaGraphConditionalHandleCreate(&hs[j], G, j == 0 ? 1u : 0u, cudaGraphCondAssignDefault) == cudaSuccess;
@@ -517,12 +521,27 @@ static int cycle_graph(helm3d_ctx *c, int m, int B, bool adjoint) {
             tail = c->launches - l0;
         }
     }
-    if (ok) ok = cudaGraphInstantiate(&exec, G, 0) == cudaSuccess;
-    if (G) cudaGraphDestroy(G);
     cudaStreamDestroy(cap);
     c->stream = saved;
     c->prof = prof;
     c->launches = launches0;
+    if (!ok) cudaGetLastError();
+    return ok;
+}
+
+// The cycle graph of one context for a batch of B, built once per
+// (B, adjoint) and kept until the workspace moves.  Returns the index in
+// c->graphs, or -1 when graphs are unavailable (the caller then launches the
+// steps itself).
+static int cycle_graph(helm3d_ctx *c, int m, int B, bool adjoint) {
+    for (size_t q = 0; q < c->graphs.size(); q++)
+        if (c->graphs[q].B == B && c->graphs[q].adjoint == adjoint) return (int)q;
+    cudaGraph_t G = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long per_step = 0, tail = 0;
+    bool ok = cudaGraphCreate(&G, 0) == cudaSuccess && add_cycle(G, c, m, B, adjoint, per_step, tail);
+    if (ok) ok = cudaGraphInstantiate(&exec, G, 0) == cudaSuccess;
+    if (G) cudaGraphDestroy(G);
     if (!ok) {
         cudaGetLastError();
         if (exec) cudaGraphExecDestroy(exec);
@@ -530,6 +549,55 @@ static int cycle_graph(helm3d_ctx *c, int m, int B, bool adjoint) {
     }
     c->graphs.push_back({B, adjoint, exec, per_step, tail});
     return (int)c->graphs.size() - 1;
+}
+
+// ------------------------------------------------------------- autotuning
+int tune_solve(helm3d_ctx *c, int R, bool adjoint) {
+    const bool any_forced = std::getenv("HELM3D_FORCE_SWEEP") || std::getenv("HELM3D_FORCE_STENCIL") ||
+                            std::getenv("HELM3D_FORCE_REDUCE");
+    if (!tune_enabled() && !any_forced) {
+        c->tv_sweep[0] = c->tv_sweep[1] = 0;
+        c->tv_stencil = 0;
+        c->red_blocks = reduce_blocks(0);
+        return HELM3D_OK;
+    }
+    const helm3d_grid &g = c->grid;
+    const int m = c->m_alloc;
+    const long N = c->N, ldV = (long)(m + 1) * N;
+    char shape[128];
+    // the sweep, in place on zeroed planes of R right-hand sides
+    RC(cuda_check(c, cudaMemsetAsync(c->d_planes, 0, (c->c64 ? 8 : 16) * (size_t)N * R, c->stream), "tune planes"));
+    const int adj = adjoint ? 1 : 0;
+    std::snprintf(shape, sizeof(shape), "%d|%d|%d|%d|%d|%d", c->c64 ? 64 : 128, g.nx, g.ny, g.nz, R, adj);
+    const SweepArgs s0 = sweep_args(c, R, adjoint);
+    c->tv_sweep[adj] = tune_pick(c, "SWEEP", shape, kSweepVariants, [&](int v) {
+        SweepArgs t = s0;
+        sweep_variant(v, t.stage_kb, t.ring_kb);
+        return launch_sweep(c->c64, t, c->stream);
+    });
+    if (c->opts.mode == HELM3D_MODE_N) {
+        // the stencil from V_0 into V_1 of every right-hand side
+        std::snprintf(shape, sizeof(shape), "%d|%d|%d|%d", g.nx, g.ny, g.nz, R);
+        StencilArgs a0 = stencil_args(c, VecBatch{c->d_V, ldV}, 1.0, kNoScale, VecBatch{c->d_V + N, ldV},
+                                      VecBatch{nullptr, 0}, R);
+        c->tv_stencil = tune_pick(c, "STENCIL", shape, kStencilVariants, [&](int v) {
+            StencilArgs t = a0;
+            t.zchunk = stencil_zchunk(v);
+            return launch_stencil(t, adjoint, c->stream);
+        });
+    }
+    // the Gram-Schmidt reduction at mid-cycle depth (read-only on V)
+    const int j = std::min(m - 1, std::max(0, m / 2));
+    std::snprintf(shape, sizeof(shape), "%ld|%d|%d", N, R, j);
+    const int rv = tune_pick(c, "REDUCE", shape, kReduceVariants, [&](int v) {
+        Reduce red = reducer(c);
+        red.nblocks = reduce_blocks(v);
+        return launch_dots2(VecBatch{c->d_V, ldV}, N, ScaleBatch{c->d_vs, m + 2}, j,
+                            VecBatch{c->d_V + (size_t)(j + 1) * N, ldV}, N, R, red, c->d_h, scalars_per_rhs(m),
+                            c->stream, nullptr, nullptr);
+    });
+    c->red_blocks = reduce_blocks(rv);
+    return HELM3D_OK;
 }
 
 // --------------------------------------------------------------- FGMRES
@@ -549,49 +617,50 @@ struct Rhs {
 };
 }  // namespace
 
-int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, helm3d_stats *st) {
-    const helm3d_opts &o = c->opts;
-    const bool flexible = (o.mode == HELM3D_MODE_N);
-    if (adjoint && !flexible) return set_error(c, HELM3D_ERR_ARG, "adjoint solve is mode N only");
-    RC(check_batch(c, R));
-    const int m = std::max(1, o.restart);
-    RC(ensure_krylov(c, m, R));
-    const long N = c->N;
-    const size_t vb = sizeof(double2) * (size_t)N;
-    const long ldV = (long)(m + 1) * N, ldZ = (long)m * N;   // per right-hand side basis strides
-    const int M2 = m + 2, SH = scalars_per_rhs(m);
-    double2 *V = c->d_V, *Z = c->d_Z, *Fw = c->d_Fw, *Uw = c->d_Uw, *Hd = c->d_h;
-    double2 *d_h1 = Hd, *d_h2 = Hd + M2, *d_nrm = Hd + 2 * M2, *d_y = Hd + 3 * M2;
-    Pinned hb((size_t)SH * R);
-    if (!hb.h) return set_error(c, HELM3D_ERR_OOM, "pinned host buffer");
-    const Reduce red = reducer(c);
-    const double tol = o.tol;
+// One FGMRES solve of a lockstep batch of R right-hand sides on one context,
+// as a sequence of restart cycles: begin(); then, while the batch is not
+// done, cycle_begin() (true residual, retirement, the cycle's batch B), the
+// cycle itself (a graph launch, the steps launched one by one with device
+// bookkeeping, or the host-driven cycle) and cycle_end(); then finish().  A
+// group of contexts runs the cycles of all its contexts as one graph launch.
+struct FgmresRun {
+    helm3d_ctx *c;
+    const double2 *f;
+    double2 *u;
+    int R;
+    bool adjoint;
+    helm3d_stats *st;
+    int m = 1, M2 = 3, SH = 0;
+    long N = 0, ldV = 0, ldZ = 0;
+    size_t vb = 0;
+    bool flexible = false;
+    double2 *hbuf = nullptr;     // pinned mirror of the Krylov scalars
+    std::vector<Rhs> S;
+    std::vector<int> act;        // packed position p -> right-hand side
+    bool x_zero = true;
+    int B = 0;                   // batch of the current cycle
+    std::vector<double> vs0;
+    std::vector<double2> ybuf;
+    std::vector<int> iv;         // device cycle state of the current cycle (host side)
+    std::vector<double> dv, est;
+    std::vector<double2> g0;
 
-    cudaEventRecord(c->ev0, c->stream);
-    RC(cuda_check(c, cudaMemcpyAsync(Fw, f, vb * R, cudaMemcpyDeviceToDevice, c->stream), "f copy"));
-    RC(cuda_check(c, cudaMemsetAsync(Uw, 0, vb * R, c->stream), "x0"));
-    RC(cuda_check(c, cudaMemsetAsync(u, 0, vb * R, c->stream), "u0"));
-    RC(norms(c, VecBatch{Fw, N}, R, false, d_nrm, SH));
-    RC(fetch(c, Hd, (size_t)SH * R, hb.h, "norms of f"));
-    std::vector<Rhs> S(R);
-    std::vector<int> act;   // packed position p -> right-hand side
-    for (int r = 0; r < R; r++) {
-        Rhs &q = S[r];
-        q.orig = r;
-        q.nf = std::sqrt(hb.h[(size_t)r * SH + 2 * M2].x);
-        if (!std::isfinite(q.nf)) return set_error(c, HELM3D_ERR_NONFINITE, "right-hand side has NaN/Inf");
-        q.H.assign((size_t)(m + 1) * m, zc(0, 0));
-        q.cs.assign(m, zc(0, 0));
-        q.sn.assign(m, zc(0, 0));
-        q.gv.assign(m + 1, zc(0, 0));
-        act.push_back(r);
+    FgmresRun(helm3d_ctx *c_, const double2 *f_, double2 *u_, int R_, bool adj, helm3d_stats *st_)
+        : c(c_), f(f_), u(u_), R(R_), adjoint(adj), st(st_) {}
+    ~FgmresRun() {
+        if (hbuf) cudaFreeHost(hbuf);
     }
-    if (st) st->history_len = 0;
+    bool done() const { return act.empty(); }
+    bool device_cycle() const { return lowsync(c) || graphs_usable(); }
+    bool graphs_usable() const { return c->use_graphs && !c->prof && !c->opts.verbose; }
+
+    int fetch_scalars(int n, const char *what) { return fetch(c, c->d_h, (size_t)SH * n, hbuf, what); }
 
     // Drop the finished right-hand sides from the packed batch: their iterate
     // goes to u, the rest move down (iterate, right-hand side, and V_0 when
     // it holds the current residual).
-    auto retire = [&](bool move_v0) -> int {
+    int retire(bool move_v0) {
+        double2 *V = c->d_V, *Fw = c->d_Fw, *Uw = c->d_Uw;
         size_t q = 0;
         for (size_t p = 0; p < act.size(); p++) {
             Rhs &r = S[act[p]];
@@ -615,47 +684,95 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, hel
         }
         act.resize(q);
         return HELM3D_OK;
-    };
-    for (int r : act)
-        if (S[r].nf == 0.0) {
-            S[r].done = true;
-            S[r].relres = S[r].relres_phys = 0;
-        }
-    RC(retire(false));
+    }
 
-    bool x_zero = true;
-    std::vector<double> vs0(R);
-    std::vector<double2> ybuf((size_t)M2 * R);
-    while (!act.empty()) {
+    int begin() {
+        const helm3d_opts &o = c->opts;
+        flexible = (o.mode == HELM3D_MODE_N);
+        if (adjoint && !flexible) return set_error(c, HELM3D_ERR_ARG, "adjoint solve is mode N only");
+        RC(check_batch(c, R));
+        m = std::max(1, o.restart);
+        RC(ensure_krylov(c, m, R));
+        RC(ensure_planes(c, R));
+        RC(tune_solve(c, R, adjoint));
+        N = c->N;
+        vb = sizeof(double2) * (size_t)N;
+        ldV = (long)(m + 1) * N;
+        ldZ = (long)m * N;
+        M2 = m + 2;
+        SH = scalars_per_rhs(m);
+        if (cudaMallocHost((void **)&hbuf, sizeof(double2) * (size_t)SH * R) != cudaSuccess) {
+            cudaGetLastError();
+            hbuf = nullptr;
+            return set_error(c, HELM3D_ERR_OOM, "pinned host buffer");
+        }
+        cudaEventRecord(c->ev0, c->stream);
+        RC(cuda_check(c, cudaMemcpyAsync(c->d_Fw, f, vb * R, cudaMemcpyDeviceToDevice, c->stream), "f copy"));
+        RC(cuda_check(c, cudaMemsetAsync(c->d_Uw, 0, vb * R, c->stream), "x0"));
+        RC(cuda_check(c, cudaMemsetAsync(u, 0, vb * R, c->stream), "u0"));
+        RC(norms(c, VecBatch{c->d_Fw, N}, R, false, c->d_h + 2 * M2, SH));
+        RC(fetch_scalars(R, "norms of f"));
+        S.assign(R, Rhs());
+        act.clear();
+        for (int r = 0; r < R; r++) {
+            Rhs &q = S[r];
+            q.orig = r;
+            q.nf = std::sqrt(hbuf[(size_t)r * SH + 2 * M2].x);
+            if (!std::isfinite(q.nf)) return set_error(c, HELM3D_ERR_NONFINITE, "right-hand side has NaN/Inf");
+            q.H.assign((size_t)(m + 1) * m, zc(0, 0));
+            q.cs.assign(m, zc(0, 0));
+            q.sn.assign(m, zc(0, 0));
+            q.gv.assign(m + 1, zc(0, 0));
+            act.push_back(r);
+        }
+        if (st) st->history_len = 0;
+        for (int r : act)
+            if (S[r].nf == 0.0) {
+                S[r].done = true;
+                S[r].relres = S[r].relres_phys = 0;
+            }
+        RC(retire(false));
+        x_zero = true;
+        vs0.assign(R, 0.0);
+        ybuf.assign((size_t)M2 * R, make_double2(0, 0));
+        return HELM3D_OK;
+    }
+
+    // r0 = f - A x0 into V_0 of every active right-hand side, its norms, the
+    // stop test and retirement; B = 0 when the batch is done
+    int cycle_begin() {
+        const helm3d_opts &o = c->opts;
+        B = 0;
+        if (act.empty()) return HELM3D_OK;
+        double2 *V = c->d_V;
         const int A = (int)act.size();
-        // r0 = f - A x0 into V_0 of every active right-hand side, with its norms
         const VecBatch V0{V, ldV};
         if (x_zero) {
-            RC(cuda_check(c, cudaMemcpy2DAsync(V, sizeof(double2) * ldV, Fw, vb, vb, A, cudaMemcpyDeviceToDevice,
-                                               c->stream),
+            RC(cuda_check(c, cudaMemcpy2DAsync(V, sizeof(double2) * ldV, c->d_Fw, vb, vb, A,
+                                               cudaMemcpyDeviceToDevice, c->stream),
                           "r0"));
         } else {
-            RC(residual(c, VecBatch{Fw, N}, VecBatch{Uw, N}, V0, A, adjoint));
+            RC(residual(c, VecBatch{c->d_Fw, N}, VecBatch{c->d_Uw, N}, V0, A, adjoint));
         }
-        RC(norms(c, V0, A, true, d_nrm, SH));
-        RC(fetch(c, Hd, (size_t)SH * A, hb.h, "residual norms"));
+        RC(norms(c, V0, A, true, c->d_h + 2 * M2, SH));
+        RC(fetch_scalars(A, "residual norms"));
         bool any_done = false;
         for (int p = 0; p < A; p++) {
             Rhs &r = S[act[p]];
-            const double b2 = hb.h[(size_t)p * SH + 2 * M2].x, p2 = hb.h[(size_t)p * SH + 2 * M2 + 1].x;
+            const double b2 = hbuf[(size_t)p * SH + 2 * M2].x, p2 = hbuf[(size_t)p * SH + 2 * M2 + 1].x;
             r.beta = std::sqrt(b2);
             if (!std::isfinite(r.beta)) return set_error(c, HELM3D_ERR_NONFINITE, "residual is NaN/Inf");
             r.relres = r.beta / r.nf;
             r.relres_phys = std::sqrt(p2) / r.nf;   // relative to ||f|| as the reference (:591-592)
-            if (r.relres <= tol || r.it >= o.max_iter) {
+            if (r.relres <= o.tol || r.it >= o.max_iter) {
                 r.done = true;
-                r.status = (r.relres <= tol || o.max_iter == 0) ? HELM3D_OK : HELM3D_ERR_NOT_CONVERGED;
+                r.status = (r.relres <= o.tol || o.max_iter == 0) ? HELM3D_OK : HELM3D_ERR_NOT_CONVERGED;
                 any_done = true;
             }
         }
         if (any_done) RC(retire(true));
-        if (act.empty()) break;
-        const int B = (int)act.size();
+        if (act.empty()) return HELM3D_OK;
+        B = (int)act.size();
         for (int p = 0; p < B; p++) {
             Rhs &r = S[act[p]];
             vs0[p] = 1.0 / r.beta;
@@ -665,215 +782,375 @@ int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, hel
             r.frozen = false;
             r.k = 0;
         }
-        RC(cuda_check(c, cudaMemcpy2DAsync(c->d_vs, sizeof(double) * M2, vs0.data(), sizeof(double), sizeof(double), B,
-                                           cudaMemcpyHostToDevice, c->stream),
-                      "vs0"));
-        const VecBatch Vall{V, ldV};
-        const ScaleBatch vsb{c->d_vs, M2};
-        const int gi = (c->use_graphs && !c->prof && !o.verbose) ? cycle_graph(c, m, B, adjoint) : -1;
-        if (gi >= 0 || lowsync(c)) {
-            // the whole cycle on the device: state in, one graph launch (or
-            // the steps launched one by one, the host checking after each
-            // whether some right-hand side is still active), state out
-            const ArnState a = arn_state(c, m, B);
-            const int Ra = c->r_alloc;
-            std::vector<double> dv((size_t)2 * Ra, 0.0);
-            std::vector<int> iv((size_t)4 * Ra + kArnFlags, 0);
-            std::vector<double2> g0((size_t)B);
-            for (int p = 0; p < B; p++) {
-                const Rhs &r = S[act[p]];
-                dv[p] = r.nf;
-                dv[Ra + p] = tol;
-                iv[2 * Ra + p] = r.it;
-                iv[3 * Ra + p] = o.max_iter;
-                g0[p] = make_double2(r.beta, 0.0);
-            }
-            RC(cuda_check(c, cudaMemcpyAsync(a.nf, dv.data(), sizeof(double) * dv.size(), cudaMemcpyHostToDevice,
-                                             c->stream),
-                          "cycle state"));
-            RC(cuda_check(c, cudaMemcpyAsync(a.frozen, iv.data(), sizeof(int) * iv.size(), cudaMemcpyHostToDevice,
-                                             c->stream),
-                          "cycle state"));
-            RC(cuda_check(c, cudaMemcpy2DAsync(a.g, sizeof(double2) * (m + 1), g0.data(), sizeof(double2),
-                                               sizeof(double2), B, cudaMemcpyHostToDevice, c->stream),
-                          "cycle state"));
-            if (gi >= 0) {
-                RC(cuda_check(c, cudaGraphLaunch(c->graphs[gi].exec, c->stream), "cycle graph"));
-            } else {
-                RC(ensure_planes(c, B));
-                for (int j = 0; j < m; j++) {
-                    RC(arnoldi_step(c, m, B, j, adjoint, a, false, 0));
-                    int active = 0;
-                    RC(cuda_check(c, cudaMemcpyAsync(&active, a.flags + 5, sizeof(int), cudaMemcpyDeviceToHost,
-                                                     c->stream),
-                                  "active"));
-                    RC(cuda_check(c, cudaStreamSynchronize(c->stream), "step"));
-                    if (o.verbose) fprintf(stderr, "helm3d: step %d, %s\n", j + 1, active ? "active" : "done");
-                    if (!active) break;
-                }
-                RC(cycle_tail(c, m, B, a));
-            }
-            std::vector<double> est((size_t)Ra * m);
-            RC(cuda_check(c, cudaMemcpyAsync(iv.data(), a.frozen, sizeof(int) * iv.size(), cudaMemcpyDeviceToHost,
-                                             c->stream),
-                          "cycle result"));
-            RC(cuda_check(c, cudaMemcpyAsync(est.data(), a.est, sizeof(double) * est.size(), cudaMemcpyDeviceToHost,
-                                             c->stream),
-                          "cycle result"));
-            RC(cuda_check(c, cudaStreamSynchronize(c->stream), "cycle"));
-            const int *flags = iv.data() + 4 * Ra;
-            if (flags[3]) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
-            const int kmax = flags[2];
-            c->reorth += flags[1];
-            if (gi >= 0)   // steps run = last step index + 1
-                c->launches += (flags[4] + 1) * c->graphs[gi].kernels_per_step + c->graphs[gi].tail_kernels;
-            for (int p = 0; p < B; p++) {
-                Rhs &r = S[act[p]];
-                r.it = iv[2 * Ra + p];
-                r.k = iv[Ra + p];
-            }
-            for (int j = 0; j < kmax; j++) {
-                double e = 0;
-                for (int p = 0; p < B; p++)
-                    if (S[act[p]].k > j) e = std::max(e, est[(size_t)p * m + j]);
-                if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = e;
-            }
-        } else {
-            for (int j = 0; j < m; j++) {
-                const VecBatch Vj{V + (size_t)j * N, ldV}, w{V + (size_t)(j + 1) * N, ldV};
-                const ScaleBatch vsj{c->d_vs + j, M2};
-                if (flexible) {
-                    const VecBatch zj{Z + (size_t)j * N, ldZ};
-                    if (adjoint) {
-                        // A^H M^{-H} = (M^{-1} A)^H: the adjoint of the forward
-                        // preconditioned operator, with the same singular values
-                        RC(apply_prec_adjoint(c, Vj, 1.0, vsj, zj, B));
-                        RC(apply_op_adjoint(c, zj, 1.0, kNoScale, w, B));
-                    } else {
-                        RC(apply_prec(c, Vj, 1.0, vsj, zj, B));
-                        RC(apply_op(c, zj, 1.0, kNoScale, w, B));
-                    }
-                } else {
-                    RC(apply_op(c, Vj, 1.0, vsj, w, B));
-                }
-                // Classical Gram-Schmidt, repeated only when needed ("twice is
-                // enough"): h1 = V^H w with ||w||^2 from the same pass, w -= V h1
-                // with ||w||^2 after; a second pass runs when the norm of some
-                // right-hand side dropped below 1/sqrt(2) of its value.
-                RC(timed(c, HELM3D_K_KRYLOV, 2,
-                         [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h1, SH, c->stream, true); }));
-                RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
-                    return launch_update(Vall, N, vsb, j + 1, d_h1, SH, w, N, B, 1, red, d_nrm, SH, c->stream);
-                }));
-                RC(fetch(c, Hd, (size_t)SH * B, hb.h, "Arnoldi coefficients"));
-                bool again = false;
-                for (int p = 0; p < B; p++) {
-                    const Rhs &r = S[act[p]];
-                    const double2 *h = hb.h + (size_t)p * SH;
-                    if (!r.frozen && h[2 * M2].x < H3D_REORTH_ETA2 * h[j + 1].x) again = true;
-                }
-                for (int p = 0; p < B; p++) {
-                    Rhs &r = S[act[p]];
-                    const double2 *h = hb.h + (size_t)p * SH;
-                    for (int i = 0; i <= j; i++) r.H[(size_t)i * m + j] = zc(h[i].x, h[i].y);
-                }
-                if (again) {
-                    RC(timed(c, HELM3D_K_KRYLOV, 2,
-                             [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h2, SH, c->stream); }));
-                    RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
-                        return launch_update(Vall, N, vsb, j + 1, d_h2, SH, w, N, B, 1, red, d_nrm, SH, c->stream);
-                    }));
-                    RC(fetch(c, Hd, (size_t)SH * B, hb.h, "Arnoldi second pass"));
-                    for (int p = 0; p < B; p++) {
-                        Rhs &r = S[act[p]];
-                        const double2 *h = hb.h + (size_t)p * SH + M2;
-                        for (int i = 0; i <= j; i++) r.H[(size_t)i * m + j] += zc(h[i].x, h[i].y);
-                    }
-                    c->reorth++;
-                }
-                double est_max = 0;
-                bool all_frozen = true;
-                for (int p = 0; p < B; p++) {
-                    Rhs &r = S[act[p]];
-                    if (r.frozen) continue;
-                    const double hn = std::sqrt(std::max(0.0, hb.h[(size_t)p * SH + 2 * M2].x));
-                    if (!std::isfinite(hn)) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
-                    std::vector<zc> &H = r.H;
-                    H[(size_t)(j + 1) * m + j] = hn;
-                    for (int i = 0; i < j; i++) {
-                        const zc a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
-                        H[(size_t)i * m + j] = r.cs[i] * a + r.sn[i] * b;
-                        H[(size_t)(i + 1) * m + j] = -std::conj(r.sn[i]) * a + r.cs[i] * b;
-                    }
-                    const zc a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
-                    givens(a, b, r.cs[j], r.sn[j]);
-                    H[(size_t)j * m + j] = r.cs[j] * a + r.sn[j] * b;
-                    H[(size_t)(j + 1) * m + j] = 0.0;
-                    r.gv[j + 1] = -std::conj(r.sn[j]) * r.gv[j];
-                    r.gv[j] = r.cs[j] * r.gv[j];
-                    r.it++;
-                    r.k = j + 1;
-                    const double est = std::abs(r.gv[j + 1]) / r.nf;
-                    est_max = std::max(est_max, est);
-                    if (hn == 0.0 || est <= tol || r.it >= o.max_iter) r.frozen = true;
-                    else all_frozen = false;
-                }
-                if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = est_max;
-                if (o.verbose) fprintf(stderr, "helm3d: step %d  max est relres %.3e over %d rhs\n", j + 1, est_max, B);
-                if (all_frozen) break;
-                RC(timed(c, HELM3D_K_KRYLOV, 1,
-                         [&] { return launch_set_scale(d_nrm, SH, c->d_vs, M2, j + 1, B, c->stream); }));
-            }
-            // y = H^{-1} g (upper triangular k x k) per right-hand side, zero
-            // padded to the longest; x += basis * y
-            int kmax = 0;
-            for (int p = 0; p < B; p++) kmax = std::max(kmax, S[act[p]].k);
-            for (int p = 0; p < B; p++) {
-                const Rhs &r = S[act[p]];
-                double2 *y = ybuf.data() + (size_t)p * M2;
-                std::vector<zc> yz(r.k);
-                for (int i = r.k - 1; i >= 0; i--) {
-                    zc s = r.gv[i];
-                    for (int q = i + 1; q < r.k; q++) s -= r.H[(size_t)i * m + q] * yz[q];
-                    yz[i] = s / r.H[(size_t)i * m + i];
-                }
-                for (int i = 0; i < kmax; i++) y[i] = i < r.k ? make_double2(yz[i].real(), yz[i].imag()) : make_double2(0, 0);
-            }
-            if (kmax > 0) {
-                RC(cuda_check(c, cudaMemcpy2DAsync(d_y, sizeof(double2) * SH, ybuf.data(), sizeof(double2) * M2,
-                                                   sizeof(double2) * kmax, B, cudaMemcpyHostToDevice, c->stream),
-                              "y"));
-                RC(timed(c, HELM3D_K_KRYLOV, 1, [&] {
-                    return flexible ? launch_combine(VecBatch{Z, ldZ}, N, kNoScale, kmax, d_y, SH, VecBatch{Uw, N}, N, B,
-                                                     c->stream)
-                                    : launch_combine(Vall, N, vsb, kmax, d_y, SH, VecBatch{Uw, N}, N, B, c->stream);
-                }));
-            }
+        return cuda_check(c, cudaMemcpy2DAsync(c->d_vs, sizeof(double) * M2, vs0.data(), sizeof(double),
+                                               sizeof(double), B, cudaMemcpyHostToDevice, c->stream),
+                          "vs0");
+    }
+
+    // the device cycle state of the batch in (before the graph or the steps)
+    int upload_state() {
+        const helm3d_opts &o = c->opts;
+        const ArnState a = arn_state(c, m, B);
+        const int Ra = c->r_alloc;
+        dv.assign((size_t)2 * Ra, 0.0);
+        iv.assign((size_t)4 * Ra + kArnFlags, 0);
+        g0.assign((size_t)B, make_double2(0, 0));
+        for (int p = 0; p < B; p++) {
+            const Rhs &r = S[act[p]];
+            dv[p] = r.nf;
+            dv[Ra + p] = o.tol;
+            iv[2 * Ra + p] = r.it;
+            iv[3 * Ra + p] = o.max_iter;
+            g0[p] = make_double2(r.beta, 0.0);
         }
+        RC(cuda_check(c, cudaMemcpyAsync(a.nf, dv.data(), sizeof(double) * dv.size(), cudaMemcpyHostToDevice,
+                                         c->stream),
+                      "cycle state"));
+        RC(cuda_check(c, cudaMemcpyAsync(a.frozen, iv.data(), sizeof(int) * iv.size(), cudaMemcpyHostToDevice,
+                                         c->stream),
+                      "cycle state"));
+        return cuda_check(c, cudaMemcpy2DAsync(a.g, sizeof(double2) * (m + 1), g0.data(), sizeof(double2),
+                                               sizeof(double2), B, cudaMemcpyHostToDevice, c->stream),
+                          "cycle state");
+    }
+
+    // a device cycle without a graph: the steps one by one, the host checking
+    // after each whether some right-hand side is still active
+    int run_steps() {
+        const ArnState a = arn_state(c, m, B);
+        for (int j = 0; j < m; j++) {
+            RC(arnoldi_step(c, m, B, j, adjoint, a, false, 0));
+            int active = 0;
+            RC(cuda_check(c, cudaMemcpyAsync(&active, a.flags + 5, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+                          "active"));
+            RC(cuda_check(c, cudaStreamSynchronize(c->stream), "step"));
+            if (c->opts.verbose) fprintf(stderr, "helm3d: step %d, %s\n", j + 1, active ? "active" : "done");
+            if (!active) break;
+        }
+        return cycle_tail(c, m, B, a);
+    }
+
+    // the device cycle state out; per_step / tail: kernels of a graph launch
+    // (counted here), or -1 when the steps were launched (already counted)
+    int cycle_end_device(long long per_step, long long tail) {
+        const ArnState a = arn_state(c, m, B);
+        const int Ra = c->r_alloc;
+        est.assign((size_t)Ra * m, 0.0);
+        RC(cuda_check(c, cudaMemcpyAsync(iv.data(), a.frozen, sizeof(int) * iv.size(), cudaMemcpyDeviceToHost,
+                                         c->stream),
+                      "cycle result"));
+        RC(cuda_check(c, cudaMemcpyAsync(est.data(), a.est, sizeof(double) * est.size(), cudaMemcpyDeviceToHost,
+                                         c->stream),
+                      "cycle result"));
+        RC(cuda_check(c, cudaStreamSynchronize(c->stream), "cycle"));
+        const int *flags = iv.data() + 4 * Ra;
+        if (flags[3]) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
+        const int kmax = flags[2];
+        c->reorth += flags[1];
+        if (per_step >= 0) c->launches += (flags[4] + 1) * per_step + tail;   // steps run = last step index + 1
+        for (int p = 0; p < B; p++) {
+            Rhs &r = S[act[p]];
+            r.it = iv[2 * Ra + p];
+            r.k = iv[Ra + p];
+        }
+        for (int j = 0; j < kmax; j++) {
+            double e = 0;
+            for (int p = 0; p < B; p++)
+                if (S[act[p]].k > j) e = std::max(e, est[(size_t)p * m + j]);
+            if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = e;
+        }
+        return cycle_done();
+    }
+
+    int cycle_done() {
         x_zero = false;
         for (int p = 0; p < B; p++) S[act[p]].restarts++;
+        return HELM3D_OK;
     }
-    if (!flexible) {
-        // u = L0^{-1} w for every right-hand side (in place: the forward
-        // transform reads all of u before the inverse writes it)
-        RC(apply_prec(c, VecBatch{u, N}, 1.0, kNoScale, VecBatch{u, N}, R));
+
+    // the host-driven cycle (classical Gram-Schmidt, host Givens): mode R
+    // without graphs, or HELM3D_GS=cgs2 without graphs
+    int run_host_cycle();
+
+    int finish() {
+        if (!flexible) {
+            // u = L0^{-1} w for every right-hand side (in place: the forward
+            // transform reads all of u before the inverse writes it)
+            RC(apply_prec(c, VecBatch{u, N}, 1.0, kNoScale, VecBatch{u, N}, R));
+        }
+        cudaEventRecord(c->ev1, c->stream);
+        RC(check_status(c));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        int status = HELM3D_OK;
+        for (const Rhs &r : S) {
+            if (r.status) status = r.status;
+            if (st) {
+                st->iterations += r.it;
+                st->restarts += r.restarts;
+                st->relres = std::max(st->relres, r.relres);
+                st->relres_phys = std::max(st->relres_phys, r.relres_phys);
+            }
+        }
+        if (st) st->ms_solve += ms;
+        return status;
     }
-    cudaEventRecord(c->ev1, c->stream);
-    RC(check_status(c));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    int status = HELM3D_OK;
-    for (const Rhs &r : S) {
-        if (r.status) status = r.status;
-        if (st) {
-            st->iterations += r.it;
-            st->restarts += r.restarts;
-            st->relres = std::max(st->relres, r.relres);
-            st->relres_phys = std::max(st->relres_phys, r.relres_phys);
+};
+
+int FgmresRun::run_host_cycle() {
+    const helm3d_opts &o = c->opts;
+    const double tol = o.tol;
+    double2 *V = c->d_V, *Z = c->d_Z, *Uw = c->d_Uw, *Hd = c->d_h;
+    double2 *d_h1 = Hd, *d_h2 = Hd + M2, *d_nrm = Hd + 2 * M2, *d_y = Hd + 3 * M2;
+    const Reduce red = reducer(c);
+    const VecBatch Vall{V, ldV};
+    const ScaleBatch vsb{c->d_vs, M2};
+    for (int j = 0; j < m; j++) {
+        const VecBatch Vj{V + (size_t)j * N, ldV}, w{V + (size_t)(j + 1) * N, ldV};
+        const ScaleBatch vsj{c->d_vs + j, M2};
+        if (flexible) {
+            const VecBatch zj{Z + (size_t)j * N, ldZ};
+            if (adjoint) {
+                // A^H M^{-H} = (M^{-1} A)^H: the adjoint of the forward
+                // preconditioned operator, with the same singular values
+                RC(apply_prec_adjoint(c, Vj, 1.0, vsj, zj, B));
+                RC(apply_op_adjoint(c, zj, 1.0, kNoScale, w, B));
+            } else {
+                RC(apply_prec(c, Vj, 1.0, vsj, zj, B));
+                RC(apply_op(c, zj, 1.0, kNoScale, w, B));
+            }
+        } else {
+            RC(apply_op(c, Vj, 1.0, vsj, w, B));
+        }
+        // Classical Gram-Schmidt, repeated only when needed ("twice is
+        // enough"): h1 = V^H w with ||w||^2 from the same pass, w -= V h1
+        // with ||w||^2 after; a second pass runs when the norm of some
+        // right-hand side dropped below 1/sqrt(2) of its value.
+        RC(timed(c, HELM3D_K_KRYLOV, 2,
+                 [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h1, SH, c->stream, true); }));
+        RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+            return launch_update(Vall, N, vsb, j + 1, d_h1, SH, w, N, B, 1, red, d_nrm, SH, c->stream);
+        }));
+        RC(fetch_scalars(B, "Arnoldi coefficients"));
+        bool again = false;
+        for (int p = 0; p < B; p++) {
+            const Rhs &r = S[act[p]];
+            const double2 *h = hbuf + (size_t)p * SH;
+            if (!r.frozen && h[2 * M2].x < H3D_REORTH_ETA2 * h[j + 1].x) again = true;
+        }
+        for (int p = 0; p < B; p++) {
+            Rhs &r = S[act[p]];
+            const double2 *h = hbuf + (size_t)p * SH;
+            for (int i = 0; i <= j; i++) r.H[(size_t)i * m + j] = zc(h[i].x, h[i].y);
+        }
+        if (again) {
+            RC(timed(c, HELM3D_K_KRYLOV, 2,
+                     [&] { return launch_dots(Vall, N, vsb, j + 1, w, N, B, red, d_h2, SH, c->stream); }));
+            RC(timed(c, HELM3D_K_KRYLOV, 2, [&] {
+                return launch_update(Vall, N, vsb, j + 1, d_h2, SH, w, N, B, 1, red, d_nrm, SH, c->stream);
+            }));
+            RC(fetch_scalars(B, "Arnoldi second pass"));
+            for (int p = 0; p < B; p++) {
+                Rhs &r = S[act[p]];
+                const double2 *h = hbuf + (size_t)p * SH + M2;
+                for (int i = 0; i <= j; i++) r.H[(size_t)i * m + j] += zc(h[i].x, h[i].y);
+            }
+            c->reorth++;
+        }
+        double est_max = 0;
+        bool all_frozen = true;
+        for (int p = 0; p < B; p++) {
+            Rhs &r = S[act[p]];
+            if (r.frozen) continue;
+            const double hn = std::sqrt(std::max(0.0, hbuf[(size_t)p * SH + 2 * M2].x));
+            if (!std::isfinite(hn)) return set_error(c, HELM3D_ERR_NONFINITE, "Arnoldi norm is NaN/Inf");
+            std::vector<zc> &H = r.H;
+            H[(size_t)(j + 1) * m + j] = hn;
+            for (int i = 0; i < j; i++) {
+                const zc a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
+                H[(size_t)i * m + j] = r.cs[i] * a + r.sn[i] * b;
+                H[(size_t)(i + 1) * m + j] = -std::conj(r.sn[i]) * a + r.cs[i] * b;
+            }
+            const zc a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
+            givens(a, b, r.cs[j], r.sn[j]);
+            H[(size_t)j * m + j] = r.cs[j] * a + r.sn[j] * b;
+            H[(size_t)(j + 1) * m + j] = 0.0;
+            r.gv[j + 1] = -std::conj(r.sn[j]) * r.gv[j];
+            r.gv[j] = r.cs[j] * r.gv[j];
+            r.it++;
+            r.k = j + 1;
+            const double est = std::abs(r.gv[j + 1]) / r.nf;
+            est_max = std::max(est_max, est);
+            if (hn == 0.0 || est <= tol || r.it >= o.max_iter) r.frozen = true;
+            else all_frozen = false;
+        }
+        if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = est_max;
+        if (o.verbose) fprintf(stderr, "helm3d: step %d  max est relres %.3e over %d rhs\n", j + 1, est_max, B);
+        if (all_frozen) break;
+        RC(timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_set_scale(d_nrm, SH, c->d_vs, M2, j + 1, B, c->stream); }));
+    }
+    // y = H^{-1} g (upper triangular k x k) per right-hand side, zero
+    // padded to the longest; x += basis * y
+    int kmax = 0;
+    for (int p = 0; p < B; p++) kmax = std::max(kmax, S[act[p]].k);
+    for (int p = 0; p < B; p++) {
+        const Rhs &r = S[act[p]];
+        double2 *y = ybuf.data() + (size_t)p * M2;
+        std::vector<zc> yz(r.k);
+        for (int i = r.k - 1; i >= 0; i--) {
+            zc s = r.gv[i];
+            for (int q = i + 1; q < r.k; q++) s -= r.H[(size_t)i * m + q] * yz[q];
+            yz[i] = s / r.H[(size_t)i * m + i];
+        }
+        for (int i = 0; i < kmax; i++) y[i] = i < r.k ? make_double2(yz[i].real(), yz[i].imag()) : make_double2(0, 0);
+    }
+    if (kmax > 0) {
+        RC(cuda_check(c, cudaMemcpy2DAsync(d_y, sizeof(double2) * SH, ybuf.data(), sizeof(double2) * M2,
+                                           sizeof(double2) * kmax, B, cudaMemcpyHostToDevice, c->stream),
+                      "y"));
+        RC(timed(c, HELM3D_K_KRYLOV, 1, [&] {
+            return flexible ? launch_combine(VecBatch{Z, ldZ}, N, kNoScale, kmax, d_y, SH, VecBatch{Uw, N}, N, B,
+                                             c->stream)
+                            : launch_combine(Vall, N, vsb, kmax, d_y, SH, VecBatch{Uw, N}, N, B, c->stream);
+        }));
+    }
+    return cycle_done();
+}
+
+int fgmres(helm3d_ctx *c, const double2 *f, double2 *u, int R, bool adjoint, helm3d_stats *st) {
+    FgmresRun run(c, f, u, R, adjoint, st);
+    RC(run.begin());
+    while (!run.done()) {
+        RC(run.cycle_begin());
+        if (run.B == 0) break;
+        const int gi = run.graphs_usable() ? cycle_graph(c, run.m, run.B, adjoint) : -1;
+        if (gi >= 0) {
+            RC(run.upload_state());
+            RC(cuda_check(c, cudaGraphLaunch(c->graphs[gi].exec, c->stream), "cycle graph"));
+            RC(run.cycle_end_device(c->graphs[gi].kernels_per_step, c->graphs[gi].tail_kernels));
+        } else if (lowsync(c)) {
+            RC(run.upload_state());
+            RC(run.run_steps());
+            RC(run.cycle_end_device(-1, 0));
+        } else {
+            RC(run.run_host_cycle());
         }
     }
-    if (st) st->ms_solve += ms;
-    return status;
+    return run.finish();
+}
+
+// ------------------------------------------------- groups of contexts
+// A group graph: the cycles of several contexts (each with its batch size)
+// as independent chains of one graph, so that the kernels of grids of
+// different sizes run side by side on the GPU.
+namespace {
+struct GroupGraph {
+    std::vector<int> key;                  // batch per context (0: not in the cycle)
+    cudaGraphExec_t exec = nullptr;
+    std::vector<long long> per_step, tail;
+};
+struct StreamGuard {
+    std::vector<helm3d_ctx *> cs;
+    std::vector<cudaStream_t> saved;
+    ~StreamGuard() {
+        for (size_t i = 0; i < cs.size(); i++) cs[i]->stream = saved[i];
+    }
+};
+}  // namespace
+
+int fgmres_group(helm3d_ctx *const *cs, int n, const double2 *const *f, double2 *const *u, const int *R,
+                 helm3d_stats *const *st) {
+    // one stream for the call: the group graph and every context's set-up
+    // and read-back work are ordered on it
+    StreamGuard guard;
+    cudaStream_t gs = cs[0]->stream;
+    for (int i = 0; i < n; i++) {
+        guard.cs.push_back(cs[i]);
+        guard.saved.push_back(cs[i]->stream);
+        cs[i]->stream = gs;
+    }
+    std::vector<std::unique_ptr<FgmresRun>> runs;
+    for (int i = 0; i < n; i++) {
+        runs.emplace_back(new FgmresRun(cs[i], f[i], u[i], R[i], false, st[i]));
+        RC(runs.back()->begin());
+    }
+    std::vector<GroupGraph> graphs;
+    struct Cleanup {
+        std::vector<GroupGraph> *g;
+        ~Cleanup() {
+            for (auto &x : *g)
+                if (x.exec) cudaGraphExecDestroy(x.exec);
+        }
+    } cleanup{&graphs};
+    bool use_group = true;
+    for (int i = 0; i < n; i++) use_group = use_group && runs[i]->graphs_usable();
+    for (;;) {
+        std::vector<int> key(n, 0);
+        bool any = false;
+        for (int i = 0; i < n; i++) {
+            if (runs[i]->done()) continue;
+            RC(runs[i]->cycle_begin());
+            key[i] = runs[i]->B;
+            any = any || key[i] > 0;
+        }
+        if (!any) break;
+        int gi = -1;
+        if (use_group) {
+            for (size_t q = 0; q < graphs.size(); q++)
+                if (graphs[q].key == key) gi = (int)q;
+            if (gi < 0) {
+                GroupGraph g;
+                g.key = key;
+                g.per_step.assign(n, 0);
+                g.tail.assign(n, 0);
+                cudaGraph_t G = nullptr;
+                bool ok = cudaGraphCreate(&G, 0) == cudaSuccess;
+                for (int i = 0; ok && i < n; i++)
+                    if (key[i] > 0) ok = add_cycle(G, cs[i], runs[i]->m, key[i], false, g.per_step[i], g.tail[i]);
+                if (ok) ok = cudaGraphInstantiate(&g.exec, G, 0) == cudaSuccess;
+                if (G) cudaGraphDestroy(G);
+                if (ok) {
+                    graphs.push_back(g);
+                    gi = (int)graphs.size() - 1;
+                } else {
+                    cudaGetLastError();
+                    use_group = false;   // the contexts' own cycles from here on
+                }
+            }
+        }
+        if (gi >= 0) {
+            for (int i = 0; i < n; i++)
+                if (key[i] > 0) RC(runs[i]->upload_state());
+            RC(cuda_check(cs[0], cudaGraphLaunch(graphs[gi].exec, gs), "group cycle graph"));
+            for (int i = 0; i < n; i++)
+                if (key[i] > 0) RC(runs[i]->cycle_end_device(graphs[gi].per_step[i], graphs[gi].tail[i]));
+            continue;
+        }
+        for (int i = 0; i < n; i++) {
+            if (key[i] == 0) continue;
+            FgmresRun &run = *runs[i];
+            helm3d_ctx *c = cs[i];
+            const int g1 = run.graphs_usable() ? cycle_graph(c, run.m, run.B, false) : -1;
+            if (g1 >= 0) {
+                RC(run.upload_state());
+                RC(cuda_check(c, cudaGraphLaunch(c->graphs[g1].exec, c->stream), "cycle graph"));
+                RC(run.cycle_end_device(c->graphs[g1].kernels_per_step, c->graphs[g1].tail_kernels));
+            } else if (lowsync(c)) {
+                RC(run.upload_state());
+                RC(run.run_steps());
+                RC(run.cycle_end_device(-1, 0));
+            } else {
+                RC(run.run_host_cycle());
+            }
+        }
+    }
+    int worst = HELM3D_OK;
+    for (int i = 0; i < n; i++) {
+        const int rc = runs[i]->finish();
+        if (rc && rc != HELM3D_ERR_NOT_CONVERGED) return rc;
+        if (rc) worst = rc;
+    }
+    return worst;
 }
 
 // -------------------------------------------------------------- BiCGStab

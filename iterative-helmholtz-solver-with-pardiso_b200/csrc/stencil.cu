@@ -13,17 +13,17 @@
 
 namespace h3d {
 
-constexpr int kStX = 32, kStY = 8, kStZ = 16;
+constexpr int kStX = 32, kStY = 8;
 
 template <bool ADJ>
 __global__ void __launch_bounds__(kStX *kStY) stencil_kernel(StencilArgs a) {
     const int i = blockIdx.x * kStX + threadIdx.x;
     const int j = blockIdx.y * kStY + threadIdx.y;
     if (i >= a.nx || j >= a.ny) return;
-    const int nzc = (a.nz + kStZ - 1) / kStZ;
+    const int nzc = (a.nz + a.zchunk - 1) / a.zchunk;
     const int r = blockIdx.z / nzc;
-    const int k0 = (blockIdx.z - r * nzc) * kStZ;
-    const int k1 = min(a.nz, k0 + kStZ);
+    const int k0 = (blockIdx.z - r * nzc) * a.zchunk;
+    const int k1 = min(a.nz, k0 + a.zchunk);
     const long plane = (long)a.nx * a.ny;
     const long col = (long)j * a.nx + i;
     const double2 *x = a.x.p + r * a.x.stride;
@@ -97,7 +97,8 @@ __global__ void __launch_bounds__(kStX *kStY) stencil_kernel(StencilArgs a) {
 
 int launch_stencil(const StencilArgs &a, bool adjoint, cudaStream_t s) {
     dim3 block(kStX, kStY);
-    dim3 grid((a.nx + kStX - 1) / kStX, (a.ny + kStY - 1) / kStY, ((a.nz + kStZ - 1) / kStZ) * a.R);
+    if (a.zchunk < 1) return HELM3D_ERR_ARG;
+    dim3 grid((a.nx + kStX - 1) / kStX, (a.ny + kStY - 1) / kStY, ((a.nz + a.zchunk - 1) / a.zchunk) * a.R);
     if (adjoint) stencil_kernel<true><<<grid, block, 0, s>>>(a);
     else stencil_kernel<false><<<grid, block, 0, s>>>(a);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;

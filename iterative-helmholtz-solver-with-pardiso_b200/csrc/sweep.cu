@@ -405,12 +405,13 @@ template <int RR, bool ADJ> static int sweep_tiled_rr(const SweepArgs &sa, cudaS
     const size_t rbytes = sizeof(Cx) * (size_t)(gm - 1) * kTileM * kTileR * (CT / gm);
     const size_t budget = device_info().smem_optin - vbytes - rbytes - 1024;
     const size_t row_bytes = (size_t)sa.ldg * sizeof(Cx);
-    int rows = (int)((16 * 1024) / row_bytes);
+    int rows = (int)(((size_t)sa.stage_kb * 1024) / row_bytes);
     if (rows < 1) rows = 1;
     if (rows > sa.n) rows = sa.n;
     k.rows_per_stage = rows;
     k.stage_bytes = (uint32_t)(((size_t)rows * row_bytes + 127) & ~(size_t)127);
-    size_t ring_cap = budget < (size_t)200 * 1024 ? budget : (size_t)200 * 1024;
+    const size_t ring_max = (size_t)sa.ring_kb * 1024;
+    size_t ring_cap = budget < ring_max ? budget : ring_max;
     int nst = (int)(ring_cap / k.stage_bytes);
     if (nst > 32) nst = 32;
     if (nst < 2) return HELM3D_ERR_ARG;
@@ -451,14 +452,16 @@ template <typename R, int G, int RR, bool ADJ> static int sweep_impl(const Sweep
     k.status = sa.status;
     const size_t vbytes = sizeof(Cx) * 2 * (size_t)sa.n * RR;
     const size_t budget = device_info().smem_optin - vbytes - 1024;
-    // ~16 KB stages, as many as fit the rest of shared memory (at most ~200 KB)
+    // stages of about stage_kb, as many as fit the rest of shared memory
+    // (at most ring_kb)
     const size_t row_bytes = (size_t)sa.ldg * sizeof(Cx);
-    int rows = (int)((16 * 1024) / row_bytes);
+    int rows = (int)(((size_t)sa.stage_kb * 1024) / row_bytes);
     if (rows < 1) rows = 1;
     if (rows > sa.n) rows = sa.n;
     k.rows_per_stage = rows;
     k.stage_bytes = (uint32_t)(((size_t)rows * row_bytes + 127) & ~(size_t)127);
-    size_t ring_cap = budget < (size_t)200 * 1024 ? budget : (size_t)200 * 1024;
+    const size_t ring_max = (size_t)sa.ring_kb * 1024;
+    size_t ring_cap = budget < ring_max ? budget : ring_max;
     int nst = (int)(ring_cap / k.stage_bytes);
     if (nst > 32) nst = 32;
     if (nst < 2) return HELM3D_ERR_ARG;
@@ -481,6 +484,14 @@ template <typename R, int G, bool ADJ> static int sweep_rr(const SweepArgs &sa, 
 
 template <typename R, int G> static int sweep_g(const SweepArgs &sa, cudaStream_t s) {
     return sa.dxy ? sweep_rr<R, G, true>(sa, s) : sweep_rr<R, G, false>(sa, s);
+}
+
+void sweep_variant(int v, int &stage_kb, int &ring_kb) {
+    static const int kStage[kSweepVariants] = {16, 8, 32, 16, 8, 32};
+    static const int kRingKb[kSweepVariants] = {200, 200, 200, 100, 100, 100};
+    if (v < 0 || v >= kSweepVariants) v = 0;
+    stage_kb = kStage[v];
+    ring_kb = kRingKb[v];
 }
 
 int launch_sweep(bool c64, const SweepArgs &sa, cudaStream_t s) {

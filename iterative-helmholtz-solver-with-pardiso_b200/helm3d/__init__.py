@@ -60,6 +60,8 @@ _sig = {
     "helm3d_create": (ctypes.c_int, [ctypes.POINTER(Grid), _vp, ctypes.POINTER(Opts), ctypes.POINTER(_vp)]),
     "helm3d_set_medium": (ctypes.c_int, [_vp, _vp]),
     "helm3d_solve": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.POINTER(Stats)]),
+    "helm3d_solve_group": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp),
+                                          ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(Stats)]),
     "helm3d_solve_bicgstab": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(Stats)]),
     "helm3d_solve_adjoint": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(Stats)]),
     "helm3d_apply_op": (ctypes.c_int, [_vp, _vp, _vp]),
@@ -280,6 +282,33 @@ class Solver:
     @property
     def kernel_launches(self) -> int:
         return int(lib.helm3d_kernel_launches(self.h))
+
+
+def solve_group(solvers, fs, nrhs=None, us=None, allow_not_converged=False):
+    """Solve several Solvers (grids of different sizes) at once: one lockstep
+    FGMRES whose restart cycles run as one CUDA graph over all the grids.
+    fs[i]: right-hand sides of solvers[i] (NumPy arrays or torch CUDA
+    tensors, (nrhs_i, nz, ny, nx) or (nz, ny, nx)).  Returns the solutions,
+    each shaped like its right-hand sides, and sets each solver's last_stats."""
+    n = len(solvers)
+    fs = [_c128(f) for f in fs]
+    if nrhs is None:
+        nrhs = [int(f.shape[0]) if len(f.shape) == 4 else 1 for f in fs]
+    if us is None:
+        us = [f.new_empty(f.shape) if hasattr(f, "data_ptr") else np.empty(f.shape, dtype=np.complex128)
+              for f in fs]
+    hs = (_vp * n)(*[s.h for s in solvers])
+    fp = (_vp * n)(*[_ptr(f) for f in fs])
+    up = (_vp * n)(*[_ptr(u) for u in us])
+    ks = (ctypes.c_int * n)(*nrhs)
+    st = (Stats * n)()
+    rc = lib.helm3d_solve_group(hs, n, fp, up, ks, st)
+    if rc != OK and not (allow_not_converged and rc == ERR_NOT_CONVERGED):
+        msgs = "; ".join((lib.helm3d_last_error(s.h) or b"").decode() for s in solvers)
+        raise Helm3dError(rc, f"solve_group: {msgs}")
+    for s, x in zip(solvers, st):
+        s.last_stats = x
+    return us
 
 
 def grid_mode_n(nx, ny, nz, h, pml, omega) -> Grid:
