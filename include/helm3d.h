@@ -168,6 +168,14 @@ int helm3d_apply_prec(helm3d_ctx *ctx, const double *x, double *y);
  * adjoint. */
 int helm3d_apply_prec_adjoint(helm3d_ctx *ctx, const double *x, double *y);
 
+/* y_r = M^{-1} x_r (adjoint != 0: M^{-H} x_r, mode N) for nrhs <= 16
+ * vectors stored one after another (nrhs * nx*ny*nz complex each, host or
+ * device pointers), as one batched preconditioner apply: each factor block
+ * read from memory serves every vector.  Batched form of
+ * Solve3DSparseUsingFT_CSR (Source/functions.cpp:5837-6061), which the
+ * reference applies to one vector at a time. */
+int helm3d_apply_prec_batch(helm3d_ctx *ctx, const double *x, double *y, int nrhs, int adjoint);
+
 /* The same y = M^{-1} x for callers that cannot allocate device memory at
  * the point of use (inside an allocator or pool callback, with free memory
  * held by a caching allocator, or on a path that must avoid cudaMalloc's

@@ -405,6 +405,30 @@ int helm3d_apply_op_adjoint(helm3d_ctx *c, const double *x, double *y) { return 
 int helm3d_apply_prec(helm3d_ctx *c, const double *x, double *y) { return apply_common(c, x, y, 2); }
 int helm3d_apply_prec_adjoint(helm3d_ctx *c, const double *x, double *y) { return apply_common(c, x, y, 3); }
 
+int helm3d_apply_prec_batch(helm3d_ctx *c, const double *x, double *y, int nrhs, int adjoint) {
+    if (!c || !x || !y) return HELM3D_ERR_ARG;
+    if (nrhs < 1 || nrhs > kMaxBatch) return set_error(c, HELM3D_ERR_ARG, "apply_prec_batch: nrhs must be 1..16");
+    if (adjoint && c->opts.mode != HELM3D_MODE_N)
+        return set_error(c, HELM3D_ERR_ARG, "adjoint preconditioner is mode N only");
+    cudaSetDevice(c->device);
+    const size_t cnt = (size_t)c->N * nrhs;
+    VecArg xa(c, x, cnt, true, &c->d_f, &c->f_cap);
+    if (xa.rc) return xa.rc;
+    VecArg ya(c, y, cnt, false, &c->d_u, &c->u_cap);
+    if (ya.rc) return ya.rc;
+    // the sweep shape: forced (HELM3D_FORCE_SWEEP), else the one the last
+    // solve of this context was tuned to
+    const int forced = tune_forced("SWEEP");
+    if (forced >= 0) c->tv_sweep[adjoint ? 1 : 0] = forced < kSweepVariants ? forced : 0;
+    const VecBatch xb{xa.dev, c->N}, yb{ya.dev, c->N};
+    const ScaleBatch one{nullptr, 0};
+    int rc = adjoint ? apply_prec_adjoint(c, xb, 1.0, one, yb, nrhs) : apply_prec(c, xb, 1.0, one, yb, nrhs);
+    if (rc) return rc;
+    rc = ya.copy_out(y, cnt);
+    if (rc) return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "apply_prec_batch");
+}
+
 int helm3d_misfit_grad(helm3d_ctx *c, const double *f, int nsrc, const long long *recv, int nrecv, const double *data,
                        double *grad, double *misfit, helm3d_stats *st) {
     if (!c) return HELM3D_ERR_ARG;

@@ -112,11 +112,15 @@ struct SweepArgs {
     int *status;              // device flag: bit 2 = a bounded wait expired
     int stage_kb = 16;        // bulk-copy stage of G^T rows (KB, about)
     int ring_kb = 200;        // shared-memory ring of stages (KB, at most)
+    int tc_mc = 0;            // complex64, n <= 128: the tensor-core sweep with G^T chunks of tc_mc rows (16, 32)
 };
 int launch_sweep(bool c64, const SweepArgs &a, cudaStream_t s);
-// the sweep's launch variants (stage and ring sizes) the autotuner times
-constexpr int kSweepVariants = 6;
-void sweep_variant(int v, int &stage_kb, int &ring_kb);
+// the sweep's launch variants the autotuner times: stage and ring sizes of
+// the CUDA-core kernels (0-5), the tensor-core kernel's chunk (6, 7)
+constexpr int kSweepVariants = 8;
+void sweep_variant(int v, SweepArgs &a);
+bool sweep_tc_supported(int n);
+int launch_sweep_tc(const SweepArgs &a, int mc, cudaStream_t s);
 constexpr int kMaxBatch = 16;  // right-hand sides per preconditioner launch
 
 // Classical Gram-Schmidt takes a second pass when the first left less than
@@ -243,6 +247,8 @@ Dev &device_info();
 // cached per (family, shape) for the process (and in HELM3D_TUNE_CACHE).
 // Not for use inside a stream capture.
 bool tune_enabled();
+// HELM3D_FORCE_<family> as an integer, or -1 when unset
+int tune_forced(const char *family);
 constexpr int kStencilVariants = 4;   // z chunk 16, 8, 32, 64
 constexpr int kReduceVariants = 3;    // reduction blocks 2, 1, 4 per SM
 int stencil_zchunk(int v);

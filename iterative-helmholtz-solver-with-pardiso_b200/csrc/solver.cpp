@@ -193,7 +193,7 @@ static SweepArgs sweep_args(helm3d_ctx *c, int R, bool adjoint) {
     s.R = R;
     s.dxy = adjoint ? c->d_dxy : nullptr;
     s.status = c->d_status;
-    sweep_variant(c->tv_sweep[adjoint ? 1 : 0], s.stage_kb, s.ring_kb);
+    sweep_variant(c->tv_sweep[adjoint ? 1 : 0], s);
     return s;
 }
 
@@ -572,7 +572,7 @@ int tune_solve(helm3d_ctx *c, int R, bool adjoint) {
     const SweepArgs s0 = sweep_args(c, R, adjoint);
     c->tv_sweep[adj] = tune_pick(c, "SWEEP", shape, kSweepVariants, [&](int v) {
         SweepArgs t = s0;
-        sweep_variant(v, t.stage_kb, t.ring_kb);
+        sweep_variant(v, t);
         return launch_sweep(c->c64, t, c->stream);
     });
     if (c->opts.mode == HELM3D_MODE_N) {

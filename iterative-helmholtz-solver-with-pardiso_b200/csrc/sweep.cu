@@ -486,16 +486,20 @@ template <typename R, int G> static int sweep_g(const SweepArgs &sa, cudaStream_
     return sa.dxy ? sweep_rr<R, G, true>(sa, s) : sweep_rr<R, G, false>(sa, s);
 }
 
-void sweep_variant(int v, int &stage_kb, int &ring_kb) {
-    static const int kStage[kSweepVariants] = {16, 8, 32, 16, 8, 32};
-    static const int kRingKb[kSweepVariants] = {200, 200, 200, 100, 100, 100};
+void sweep_variant(int v, SweepArgs &a) {
+    static const int kStage[kSweepVariants] = {16, 8, 32, 16, 8, 32, 16, 16};
+    static const int kRingKb[kSweepVariants] = {200, 200, 200, 100, 100, 100, 200, 200};
+    static const int kTcMc[kSweepVariants] = {0, 0, 0, 0, 0, 0, 32, 16};
     if (v < 0 || v >= kSweepVariants) v = 0;
-    stage_kb = kStage[v];
-    ring_kb = kRingKb[v];
+    a.stage_kb = kStage[v];
+    a.ring_kb = kRingKb[v];
+    a.tc_mc = kTcMc[v];
 }
 
 int launch_sweep(bool c64, const SweepArgs &sa, cudaStream_t s) {
     if (sa.n < 1 || sa.n > kSweepMaxN || sa.R < 1 || sa.R > kMaxBatch) return HELM3D_ERR_ARG;
+    // the tensor-core kernel where it applies (complex64, one row block)
+    if (c64 && sa.tc_mc && sweep_tc_supported(sa.n)) return launch_sweep_tc(sa, sa.tc_mc, s);
     // complex64 batches of 3 or more: the register-tiled kernel (its 16-byte
     // tile loads need ldg, the padded row length, to be a multiple of 4)
     if (c64 && sa.R >= 3 && sa.ldg % 4 == 0) return sa.dxy ? sweep_tiled<true>(sa, s) : sweep_tiled<false>(sa, s);

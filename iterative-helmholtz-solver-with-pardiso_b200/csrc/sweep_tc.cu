@@ -1,0 +1,385 @@
+// sweep_tc.cu -- the block sweep of sweep.cu for complex64 batches of
+// right-hand sides on the 5th-generation tensor cores (tcgen05, kind::tf32,
+// FP32-class products by 3xTF32: a_hi b_hi + a_hi b_lo + a_lo b_hi).
+// Same recurrence (the per-kz 2D solve replacing PARDISO phase 33,
+// Source/functions.cpp:5959, and DirSolveFastDiagStruct,
+// Source/HODLR/BinaryTreesHODLR.cpp:2971-3018):
+//   forward   y_0 = G_0 f_0,   y_j = G_j (f_j - cmy[j] y_{j-1})
+//   backward  x_{ny-1} = y_{ny-1},   x_j = y_j - cpy[j] G_j x_{j+1}
+// One CTA per kz, all RR (8 or 16, padded) right-hand sides at once: each
+// line is the real GEMM
+//   D[i][2r + c] = sum_K A[i][K] B[2r + c][K],   K = 2m + c'  (m < n, c' = re/im)
+// with A = G_j (row i, complex interleaved along K: the natural layout of
+// G) and B the real form of the line's input v (B[2r][2m] = Re v[m][r],
+// B[2r][2m+1] = -Im v, B[2r+1][2m] = Im v, B[2r+1][2m+1] = Re v), so that
+// D[i][2r] + i D[i][2r+1] = (G_j v)[i][r].  M = 128 (rows i, n <= 128),
+// N = 2 RR, K = 2 n padded to the chunk.
+//
+// Roles (10 warps):
+//   * warp 8, one lane: streams G_j^T (rows m, i contiguous, as the factor
+//     stores it) chunk by chunk (MC rows m) into a ring of shared-memory
+//     stages with 1D bulk copies, as far ahead as the ring allows;
+//   * warps 0-7: convert each chunk -- thread i reads G^T[m][i] for half of
+//     the chunk's m, splits it into tf32 hi + lo and stores both into TMEM
+//     (lane i, column K), one of three chunk buffers; at the end of a line
+//     they read D from TMEM (warp w: lanes 32 (w % 4) + [0, 32), the columns
+//     of half the right-hand sides), finish the line (y or x into the
+//     planes), write the next line's v to shared memory and from it the
+//     next B (hi and lo, canonical no-swizzle K-major layout, 16-byte units
+//     in address order so that the stores of a warp are contiguous);
+//   * warp 9, one lane: issues the MMAs of a line (A from TMEM, B from
+//     shared memory) chunk by chunk as the buffers fill, and commits them to
+//     the buffer-free barriers and, after the last chunk, to the
+//     accumulator-ready barrier.
+// G^T chunks of the next line are converted while the current line's MMAs
+// run; the dependence chain per line is MMAs -> epilogue -> B.  Every wait is
+// bounded; on expiry bit 2 of *status is set and the kernel runs on without
+// waiting (results then invalid), waits (bounded) for its own MMAs and bulk
+// copies, frees its TMEM and returns.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "cplx.cuh"
+#include "helm3d_internal.h"
+#include "ptx.cuh"
+#include "tcgen05.cuh"
+
+namespace h3d {
+
+constexpr int kTcConsumerWarps = 8;
+constexpr int kTcThreads = (kTcConsumerWarps + 2) * 32;
+constexpr int kTcMaxN = 128;           // MMA M: one row block
+constexpr int kTcBuf = 3;              // TMEM A chunk buffers
+constexpr int kTcLook = kTcBuf - 1;    // chunks of the next line converted before a line's epilogue
+constexpr uint32_t kTcCols = 512;      // TMEM columns: D at 0, buffer b at 128 (b + 1)
+constexpr uint32_t kTcWaitLimit = 1u << 22;
+
+struct SweepTcK {
+    int n, ny, ldg, nrhs;
+    int npad;            // n rounded up to the chunk (K = 2 npad)
+    int cpl;             // chunks per line
+    int nstage;          // bulk-copy ring depth
+    uint32_t stage_bytes;
+    const float2 *Gt;
+    const float2 *cmy, *cpy;
+    float2 *planes;
+    const float2 *dxy;   // adjoint scaling table (see sweep.cu), or null
+    int *status;
+};
+
+__device__ __forceinline__ void tc_consumer_barrier() {
+    asm volatile("bar.sync 1, %0;" ::"n"(kTcConsumerWarps * 32) : "memory");
+}
+
+template <bool ADJ> __device__ __forceinline__ float2 tc_adj_in(const SweepTcK &a, int line, int i, float2 f) {
+    if (!ADJ) return f;
+    return cmul(a.dxy[(long)line * a.n + i], make_float2(f.x, -f.y));
+}
+template <bool ADJ> __device__ __forceinline__ float2 tc_adj_out(const SweepTcK &a, int line, int i, float2 x) {
+    if (!ADJ) return x;
+    return cmul(make_float2(x.x, -x.y), a.dxy[(long)(a.ny + line) * a.n + i]);
+}
+
+// G^T rows of chunk `seq` of the chain (forward lines 0..ny-1, then
+// backward lines ny-2..0, MC rows m per chunk)
+template <int MC>
+__device__ __forceinline__ const float2 *tc_stage_src(const SweepTcK &a, int kz, long seq, int *rows) {
+    const long t = seq / a.cpl;
+    const int c = (int)(seq - t * a.cpl);
+    const int line = t < a.ny ? (int)t : (int)(2 * a.ny - 2 - t);
+    const int m0 = c * MC;
+    *rows = min(MC, a.n - m0);
+    return a.Gt + (((long)kz * a.ny + line) * a.n + m0) * (long)a.ldg;
+}
+
+template <int RR, int MC, bool ADJ>
+__global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
+    constexpr int NR = 2 * RR;        // B rows = D columns
+    constexpr int KC = 2 * MC;        // K per chunk (TMEM columns of hi, and of lo)
+    constexpr int RH = RR / 2;        // right-hand sides per warpgroup in the epilogue
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const int n = a.n, ny = a.ny, ldg = a.ldg, Rn = a.nrhs, npad = a.npad, cpl = a.cpl;
+    const int Kp = 2 * npad;
+    const int kz = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nsteps = 2 * ny - 1;
+    const long nseq = (long)nsteps * cpl;
+
+    unsigned char *ring = smem_raw;
+    float *Bhi = reinterpret_cast<float *>(smem_raw + (size_t)a.nstage * a.stage_bytes);
+    float *Blo = Bhi + (size_t)NR * Kp;
+    const int vld = npad + 2;         // padded row of vst (bank spread across right-hand sides)
+    float2 *vst = reinterpret_cast<float2 *>(Blo + (size_t)NR * Kp);   // [RR][vld]
+    uint64_t *raw_full = reinterpret_cast<uint64_t *>(vst + (size_t)RR * vld);
+    uint64_t *raw_empty = raw_full + a.nstage;
+    uint64_t *a_full = raw_empty + a.nstage;
+    uint64_t *a_empty = a_full + kTcBuf;
+    uint64_t *b_full = a_empty + kTcBuf;
+    uint64_t *d_full = b_full + 1;
+    uint64_t *fin = d_full + 1;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(fin + 1);
+    float2 *P = a.planes + (long)kz * ny * Rn * n;   // line j, rhs r, row i at ((j*Rn + r)*n + i)
+
+    if (warp == 0) tmem_alloc(tslot, kTcCols);
+    if (tid == 0) {
+        for (int s = 0; s < a.nstage; s++) {
+            mbar_init(&raw_full[s], 1);
+            mbar_init(&raw_empty[s], kTcConsumerWarps);
+        }
+        for (int b = 0; b < kTcBuf; b++) {
+            mbar_init(&a_full[b], kTcConsumerWarps);
+            mbar_init(&a_empty[b], 1);
+        }
+        mbar_init(b_full, kTcConsumerWarps);
+        mbar_init(d_full, 1);
+        mbar_init(fin, 1);
+        fence_mbar_init_cluster();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    bool dead = false;
+    auto fail = [&]() {
+        if (!dead) atomicOr(a.status, 4);
+        dead = true;
+    };
+    auto wait = [&](uint64_t *bar, uint32_t parity) {
+        if (!dead && !mbar_wait_bounded_cta(smem_u32(bar), parity, kTcWaitLimit)) fail();
+    };
+
+    if (warp == kTcConsumerWarps) {
+        // ---------------------------------------------------- producer
+        if (lane == 0) {
+            for (long seq = 0; seq < nseq; seq++) {
+                const int s = (int)(seq % a.nstage);
+                if (seq >= a.nstage) wait(&raw_empty[s], (uint32_t)(((seq / a.nstage) & 1) ^ 1));
+                int rows;
+                const float2 *src = tc_stage_src<MC>(a, kz, seq, &rows);
+                const uint32_t bytes = (uint32_t)rows * ldg * 8u;
+                mbar_expect_tx(&raw_full[s], bytes);
+                bulk_g2s(ring + (size_t)s * a.stage_bytes, src, bytes, &raw_full[s]);
+            }
+            // the copies still in flight land before the CTA exits
+            const long first = nseq > a.nstage ? nseq - a.nstage : 0;
+            for (long seq = first; seq < nseq; seq++)
+                mbar_wait_bounded_cta(smem_u32(&raw_full[seq % a.nstage]), (uint32_t)((seq / a.nstage) & 1),
+                                      kTcWaitLimit);
+        }
+    } else if (warp == kTcConsumerWarps + 1) {
+        // --------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = umma_idesc_tf32(NR);
+            const uint32_t sbo = (uint32_t)(Kp / 4) * 128u;
+            const uint32_t bhi = smem_u32(Bhi), blo = smem_u32(Blo);
+            for (int t = 0; t < nsteps; t++) {
+                wait(b_full, (uint32_t)(t & 1));
+                tc_fence_after();
+                for (int c = 0; c < cpl; c++) {
+                    const long seq = (long)t * cpl + c;
+                    const int b = (int)(seq % kTcBuf);
+                    wait(&a_full[b], (uint32_t)((seq / kTcBuf) & 1));
+                    tc_fence_after();
+                    const uint32_t ahi = tmem + 128u * (uint32_t)(b + 1), alo = ahi + (uint32_t)KC;
+#pragma unroll
+                    for (int ks = 0; ks < KC / 8; ks++) {
+                        const uint32_t koff = (uint32_t)((c * KC + ks * 8) / 4) * 128u;
+                        const uint64_t dh = umma_desc(bhi + koff, 128, sbo), dl = umma_desc(blo + koff, 128, sbo);
+                        umma_tf32_ts(tmem, ahi + (uint32_t)(ks * 8), dh, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+                        umma_tf32_ts(tmem, ahi + (uint32_t)(ks * 8), dl, idesc, 1u);
+                        umma_tf32_ts(tmem, alo + (uint32_t)(ks * 8), dh, idesc, 1u);
+                    }
+                    umma_commit(&a_empty[b]);
+                }
+                umma_commit(d_full);
+            }
+            // every MMA of this CTA complete before the TMEM is freed
+            umma_commit(fin);
+            mbar_wait_bounded_cta(smem_u32(fin), 0u, kTcWaitLimit);
+        }
+    } else {
+        // ------------------------------------------ converters / epilogue
+        const int q = warp & 3, wg = warp >> 2;
+        const int i = 32 * q + lane;                      // TMEM lane = row of G_j and of D
+        const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
+
+        // B (hi, lo) of the next line from vst; 16-byte units u in address
+        // order: row & 7, then the K quad, then the 8-row group
+        auto build_b = [&]() {
+            const int kq_n = Kp / 4;
+            const int units = NR * kq_n;
+            for (int u = tid; u < units; u += kTcConsumerWarps * 32) {
+                const int rlo = u & 7, rest = u >> 3;
+                const int kq = rest % kq_n, rg = rest / kq_n;
+                const int row = rg * 8 + rlo, r = row >> 1;
+                const float4 vv = *reinterpret_cast<const float4 *>(vst + (size_t)r * vld + 2 * kq);
+                float4 e;
+                if ((row & 1) == 0) e = make_float4(vv.x, -vv.y, vv.z, -vv.w);   // (Re v, -Im v)
+                else e = make_float4(vv.y, vv.x, vv.w, vv.z);                   // (Im v, Re v)
+                float4 h, l;
+                tf32_split_f(e.x, h.x, l.x);
+                tf32_split_f(e.y, h.y, l.y);
+                tf32_split_f(e.z, h.z, l.z);
+                tf32_split_f(e.w, h.w, l.w);
+                reinterpret_cast<float4 *>(Bhi)[u] = h;
+                reinterpret_cast<float4 *>(Blo)[u] = l;
+            }
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_local(b_full);
+        };
+
+        // one chunk of G^T rows into TMEM buffer seq % kTcBuf (hi and lo)
+        auto convert = [&](long seq) {
+            const int s = (int)(seq % a.nstage);
+            const int b = (int)(seq % kTcBuf);
+            wait(&raw_full[s], (uint32_t)((seq / a.nstage) & 1));
+            if (seq >= kTcBuf) wait(&a_empty[b], (uint32_t)(((seq / kTcBuf) & 1) ^ 1));
+            tc_fence_after();
+            const int c = (int)(seq % cpl);
+            const int rows = min(MC, n - c * MC);
+            const float2 *raw = reinterpret_cast<const float2 *>(ring + (size_t)s * a.stage_bytes);
+            float hv[MC], lv[MC];
+#pragma unroll
+            for (int k = 0; k < MC / 2; k++) {
+                const int ml = wg * (MC / 2) + k;
+                float2 g = make_float2(0.f, 0.f);
+                if (i < n && ml < rows) g = raw[(size_t)ml * ldg + i];
+                tf32_split_f(g.x, hv[2 * k], lv[2 * k]);
+                tf32_split_f(g.y, hv[2 * k + 1], lv[2 * k + 1]);
+            }
+            const uint32_t col = 128u * (uint32_t)(b + 1) + (uint32_t)(wg * MC);
+            if constexpr (MC == 32) {
+                tmem_st32(trow + col, hv);
+                tmem_st32(trow + col + KC, lv);
+            } else {
+                tmem_st16(trow + col, hv);
+                tmem_st16(trow + col + KC, lv);
+            }
+            tmem_wait_st();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive_local(&raw_empty[s]);
+                mbar_arrive_local(&a_full[b]);
+            }
+        };
+
+        // line 0's input: f_0 for every right-hand side
+        for (int e = tid; e < RR * npad; e += kTcConsumerWarps * 32) {
+            const int r = e / npad, m = e - r * npad;
+            vst[(size_t)r * vld + m] =
+                (r < Rn && m < n) ? tc_adj_in<ADJ>(a, 0, m, P[(long)r * n + m]) : make_float2(0.f, 0.f);
+        }
+        tc_consumer_barrier();
+        build_b();
+
+        long conv = 0;
+        for (int t = 0; t < nsteps; t++) {
+            const long target = min(nseq, (long)(t + 1) * cpl + kTcLook);
+            while (conv < target) convert(conv++);
+            const bool fwd = t < ny;
+            const int line = fwd ? t : 2 * ny - 2 - t;
+            const bool last_fwd = fwd && line + 1 == ny;
+            // what finishing the line needs besides G v
+            float2 pre[RH];
+#pragma unroll
+            for (int k = 0; k < RH; k++) {
+                const int r = wg * RH + k;
+                pre[k] = make_float2(0.f, 0.f);
+                if (i < n && r < Rn) {
+                    if (fwd && !last_fwd) pre[k] = tc_adj_in<ADJ>(a, line + 1, i, P[((long)(line + 1) * Rn + r) * n + i]);
+                    else if (!fwd) pre[k] = P[((long)line * Rn + r) * n + i];
+                }
+            }
+            const float2 cn = (fwd && !last_fwd) ? a.cmy[line + 1] : make_float2(0.f, 0.f);
+            const float2 cp = fwd ? make_float2(0.f, 0.f) : a.cpy[line];
+            wait(d_full, (uint32_t)(t & 1));
+            tc_fence_after();
+            float d[RR];
+            if constexpr (RR == 16) tmem_ld16_nowait(trow + (uint32_t)(wg * RR), d);
+            else tmem_ld8_nowait(trow + (uint32_t)(wg * RR), d);
+            tmem_wait_ld(d);
+            tc_fence_before();
+#pragma unroll
+            for (int k = 0; k < RH; k++) {
+                const int r = wg * RH + k;
+                const float2 acc = make_float2(d[2 * k], d[2 * k + 1]);
+                float2 out, vn;
+                bool fin_x;   // out is this line's final x
+                if (fwd) {
+                    out = acc;                                        // y_line
+                    fin_x = last_fwd;
+                    vn = fin_x ? out : cfms(cn, out, pre[k]);         // f_{line+1} - cmy y_line, or x_{ny-1}
+                } else {
+                    out = cfms(cp, acc, pre[k]);                      // x_line = y_line - cpy G x_{line+1}
+                    fin_x = true;
+                    vn = out;
+                }
+                const bool valid = i < n && r < Rn;
+                if (valid) P[((long)line * Rn + r) * n + i] = fin_x ? tc_adj_out<ADJ>(a, line, i, out) : out;
+                if (i < npad) vst[(size_t)r * vld + i] = valid ? vn : make_float2(0.f, 0.f);
+            }
+            if (t + 1 < nsteps) {
+                tc_consumer_barrier();
+                build_b();
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, kTcCols);
+}
+
+// ------------------------------------------------------------------- host
+bool sweep_tc_supported(int n) { return n >= 1 && n <= kTcMaxN; }
+
+template <int RR, int MC, bool ADJ> static int sweep_tc_impl(const SweepArgs &sa, cudaStream_t st) {
+    SweepTcK k;
+    k.n = sa.n;
+    k.ny = sa.ny;
+    k.ldg = sa.ldg;
+    k.nrhs = sa.R;
+    k.npad = ((sa.n + MC - 1) / MC) * MC;
+    k.cpl = k.npad / MC;
+    k.Gt = (const float2 *)sa.Gt;
+    k.cmy = (const float2 *)sa.cmy;
+    k.cpy = (const float2 *)sa.cpy;
+    k.planes = (float2 *)sa.planes;
+    k.dxy = (const float2 *)sa.dxy;
+    k.status = sa.status;
+    k.stage_bytes = (uint32_t)((((size_t)MC * sa.ldg * 8) + 127) & ~(size_t)127);
+    const size_t bbytes = 2 * sizeof(float) * (size_t)(2 * RR) * (2 * k.npad);
+    const size_t vbytes = sizeof(float2) * (size_t)RR * (k.npad + 2);
+    const size_t fixed = bbytes + vbytes + sizeof(uint64_t) * (2 * kTcBuf + 3) + 16;
+    const size_t optin = device_info().smem_optin;
+    if (fixed + 2 * (size_t)k.stage_bytes + 2 * sizeof(uint64_t) * 2 > optin) return HELM3D_ERR_ARG;
+    int nst = (int)((optin - fixed) / (k.stage_bytes + 2 * sizeof(uint64_t)));
+    const int ring_cap = (int)(((size_t)sa.ring_kb * 1024) / k.stage_bytes);
+    if (nst > ring_cap) nst = ring_cap;
+    if (nst > 8) nst = 8;
+    if (nst < 2) return HELM3D_ERR_ARG;
+    k.nstage = nst;
+    const size_t smem = (size_t)nst * k.stage_bytes + bbytes + vbytes + sizeof(uint64_t) * (2 * nst + 2 * kTcBuf + 3) +
+                        16;
+    auto kern = sweep_tc_kernel<RR, MC, ADJ>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return HELM3D_ERR_CUDA;
+    kern<<<dim3((unsigned)sa.nz), kTcThreads, smem, st>>>(k);
+    return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
+template <int MC, bool ADJ> static int sweep_tc_rr(const SweepArgs &sa, cudaStream_t s) {
+    if (sa.R <= 8) return sweep_tc_impl<8, MC, ADJ>(sa, s);
+    return sweep_tc_impl<16, MC, ADJ>(sa, s);
+}
+
+int launch_sweep_tc(const SweepArgs &sa, int mc, cudaStream_t s) {
+    if (!sweep_tc_supported(sa.n) || sa.R < 1 || sa.R > 16) return HELM3D_ERR_ARG;
+    if (mc == 16) return sa.dxy ? sweep_tc_rr<16, true>(sa, s) : sweep_tc_rr<16, false>(sa, s);
+    return sa.dxy ? sweep_tc_rr<32, true>(sa, s) : sweep_tc_rr<32, false>(sa, s);
+}
+
+}  // namespace h3d

@@ -37,92 +37,13 @@
 #include "cplx.cuh"
 #include "helm3d_internal.h"
 #include "ptx.cuh"
+#include "tcgen05.cuh"
 
 namespace h3d {
 
 constexpr int kZcThreads = 256;
 constexpr int kZcM = 128;                  // tile positions (MMA M)
 constexpr uint32_t kZcWaitLimit = 1u << 22;
-
-// ------------------------------------------------------------- tf32 split
-__host__ __device__ inline float tf32_round(float f) {
-    uint32_t u;
-#ifdef __CUDA_ARCH__
-    u = __float_as_uint(f);
-#else
-    std::memcpy(&u, &f, 4);
-#endif
-    u = (u + 0x1000u) & 0xFFFFE000u;
-#ifdef __CUDA_ARCH__
-    return __uint_as_float(u);
-#else
-    float r;
-    std::memcpy(&r, &u, 4);
-    return r;
-#endif
-}
-
-// hi + lo ~ v to ~2^-21 relative, both exact tf32 values
-__host__ __device__ inline void tf32_split(double v, float &hi, float &lo) {
-    hi = tf32_round((float)v);
-    lo = tf32_round((float)(v - (double)hi));
-}
-
-// ------------------------------------------------------------ tcgen05 PTX
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    // start address, LBO, SBO (all >> 4), version 1 (sm_100), no swizzle
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
-}
-
-// kind::tf32, fp32 accumulator, A and B K-major, M = 128
-__host__ __device__ constexpr uint32_t umma_idesc_tf32(int n) {
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kZcM >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-        :
-        : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t *bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// 16 consecutive fp32 columns of this warp's 32 TMEM lanes (lane = thread);
-// the values may be used only after tmem_wait_ld()
-__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, float *v) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]),
-          "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
-        : "r"(taddr));
-}
-// waits for this thread's outstanding TMEM loads; the 32 registers they fill
-// pass through the statement so that no use of them is scheduled before it
-__device__ __forceinline__ void tmem_wait_ld(float (&v)[32]) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]),
-                   "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]),
-                   "+f"(v[15]), "+f"(v[16]), "+f"(v[17]), "+f"(v[18]), "+f"(v[19]), "+f"(v[20]), "+f"(v[21]),
-                   "+f"(v[22]), "+f"(v[23]), "+f"(v[24]), "+f"(v[25]), "+f"(v[26]), "+f"(v[27]), "+f"(v[28]),
-                   "+f"(v[29]), "+f"(v[30]), "+f"(v[31])
-                 :
-                 : "memory");
-}
 
 // -------------------------------------------------------------- the kernel
 struct ZtcArgs {
@@ -140,12 +61,6 @@ struct ZtcArgs {
     uint32_t tmem_cols;
     int *status;
 };
-
-// byte offset of element (row, kk) in a no-swizzle K-major operand with KC
-// columns (see the file comment)
-__host__ __device__ inline uint32_t canon_off(int row, int kk, int KC) {
-    return (uint32_t)((row >> 3) * (KC / 4) * 128 + (kk >> 2) * 128 + (row & 7) * 16 + (kk & 3) * 4);
-}
 
 __device__ __forceinline__ long zc_plane_index(const PlaneLayout &L, int r, int k, long w) {
     const long j = w / L.nx, i = w - j * L.nx;
@@ -304,7 +219,7 @@ __global__ void __launch_bounds__(kZcThreads, 1) ztc_kernel(ZtcArgs a) {
                 const uint32_t blo = bs + bbytes / 2;
                 for (int part = 0; part * 256 < N; part++) {
                     const int n_part = N - part * 256 < 256 ? N - part * 256 : 256;
-                    const uint32_t idesc = umma_idesc_tf32(n_part);
+                    const uint32_t idesc = umma_idesc_tf32(n_part, kZcM);
                     const uint32_t brow = (uint32_t)(part * 256 / 8) * sbo;   // row offset of this part
                     const uint32_t td = tmem + (uint32_t)(part * 256);
 #pragma unroll

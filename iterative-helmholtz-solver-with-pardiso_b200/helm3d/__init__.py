@@ -65,6 +65,7 @@ _sig = {
     "helm3d_solve_bicgstab": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(Stats)]),
     "helm3d_solve_adjoint": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(Stats)]),
     "helm3d_apply_op": (ctypes.c_int, [_vp, _vp, _vp]),
+    "helm3d_apply_prec_batch": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int]),
     "helm3d_apply_op_adjoint": (ctypes.c_int, [_vp, _vp, _vp]),
     "helm3d_apply_prec": (ctypes.c_int, [_vp, _vp, _vp]),
     "helm3d_apply_prec_adjoint": (ctypes.c_int, [_vp, _vp, _vp]),
@@ -217,6 +218,16 @@ class Solver:
 
     def apply_prec_adjoint(self, x):
         return self._apply(lib.helm3d_apply_prec_adjoint, x, "apply_prec_adjoint")
+
+    def apply_prec_batch(self, X, adjoint=False):
+        """M^{-1} (or M^{-H}) of each of the nrhs <= 16 vectors X[r] (shape
+        (nrhs, nz, ny, nx)) in one batched apply."""
+        X = _c128(X)
+        Y = X.new_empty(X.shape) if hasattr(X, "data_ptr") else np.empty(X.shape, dtype=np.complex128)
+        rc = lib.helm3d_apply_prec_batch(self.h, _ptr(X), _ptr(Y), int(X.shape[0]), 1 if adjoint else 0)
+        if rc != OK:
+            self._err(rc, "apply_prec_batch")
+        return Y
 
     def misfit_grad(self, f, recv, data, nsrc: int | None = None, grad=None, allow_not_converged=False):
         """(J, dJ/ds2) for J = 1/2 sum_s ||u_s[recv] - data_s||^2, A u_s = f_s.
