@@ -56,7 +56,7 @@ ITERS_128 = 513
 def workload(n: int, nsrc: int = 1):
     """The 128^3 heterogeneous medium recipe at size n with nsrc seeded
     sources (the medium does not depend on nsrc; source 0 is the same)."""
-    from oracle import media
+    from helm3d import media
     p = media.layered_medium(n, n, n, 10.0, 12, 2024, ppw=8.0, n_sources=nsrc)
     p.meta["config"] = "C2"
     return p
@@ -378,6 +378,207 @@ def run_kernels(args):
     return out
 
 
+# ------------------------------------------------- the other configurations
+def _solver(helm3d, p, s2, prec, zt, restart=RESTART, tol=TOL, stream=None):
+    g = helm3d.grid_mode_n(p.nx, p.ny, p.nz, p.h, p.pml, p.omega)
+    o = helm3d.default_opts(precision=prec, restart=restart, tol=tol, beta_prec=BETA_PREC, max_iter=20000,
+                            device=0, z_transform=zt)
+    s = helm3d.Solver(g, s2, o)
+    if stream is not None:
+        s.set_stream(stream)
+    return s
+
+
+def _events_ms(stream, fn, steps):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_large(args, n: int, restart: int, label: str):
+    """One n^3 heterogeneous medium (the 128^3 recipe at size n): time per
+    source-solve of the batched complex64 preconditioner (16 sources, PML
+    eigenbasis), of one source with it, and of the plain complex128 FFT-z path
+    with one source; each step includes set-up and factor.  The complex64
+    solutions' error is measured against the complex128 solution."""
+    import torch
+
+    import helm3d
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    p = helm3d_media().layered_medium(n, n, n, 10.0, 12 if n < 200 else 16, 2024, ppw=8.0, n_sources=BATCH)
+    F = torch.from_numpy(np.stack([p.rhs(i) for i in range(BATCH)])).to(dev)
+    s2 = torch.from_numpy(np.ascontiguousarray(p.s2)).to(dev)
+    U = torch.empty_like(F)
+    out = {"mode": label, "workload": f"{n}^3 heterogeneous medium (1500->3000 m/s depth gradient, three +-20 % "
+                                      f"anomalies), PML {p.pml}, 8 ppw; FGMRES({restart}) to {TOL}; each step "
+                                      f"= set-up + factor + solve", "n": n}
+    res = {}
+    for name, prec, zt, nrhs in (("batched16_c64_eigen", helm3d.PREC_C64, helm3d.ZT_PML_EIGEN, BATCH),
+                                 ("single_c64_eigen", helm3d.PREC_C64, helm3d.ZT_PML_EIGEN, 1),
+                                 ("fp64_plain", helm3d.PREC_C128, helm3d.ZT_FFT, 1)):
+        s = _solver(helm3d, p, s2, prec, zt, restart=restart, stream=stream)
+
+        def step():
+            s.set_medium(s2)
+            s.solve(F[:nrhs], nrhs=nrhs, u=U[:nrhs], allow_not_converged=True)
+        for _ in range(args.warmup):
+            step()
+        ms = _events_ms(stream, step, args.steps)
+        st = s.last_stats
+        res[name] = {"s_per_solve": ms / 1e3 / nrhs, "ms_per_step": ms, "sources": nrhs,
+                     "iterations_per_source": st.iterations / nrhs, "relres": st.relres}
+        if name == "batched16_c64_eigen":
+            Ub = U.clone()
+        s.close()
+    u64 = U[0]
+    res["batched16_c64_eigen"]["relerr_vs_fp64"] = float(torch.linalg.vector_norm(Ub[0] - u64) /
+                                                         torch.linalg.vector_norm(u64))
+    out["results"] = res
+    out["speedup_batched_vs_fp64_plain"] = res["fp64_plain"]["s_per_solve"] / res["batched16_c64_eigen"]["s_per_solve"]
+    out["speedup_single_vs_fp64_plain"] = res["fp64_plain"]["s_per_solve"] / res["single_c64_eigen"]["s_per_solve"]
+    return out
+
+
+def run_group(args):
+    """16 sources on a 96^3 medium plus 8 uneven grids with one source each,
+    every grid its own medium: set-up and factor of all nine contexts, then
+    one grouped FGMRES (restart cycles of all grids in one CUDA graph),
+    against the same contexts solved one after another."""
+    import torch
+
+    import helm3d
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    probs = helm3d_media().config_c4()
+    Fs = [torch.from_numpy(np.stack([p.rhs(i) for i in range(len(p.sources))])).to(dev) for p in probs]
+    S2 = [torch.from_numpy(np.ascontiguousarray(p.s2)).to(dev) for p in probs]
+    Us = [torch.empty_like(f) for f in Fs]
+    ss = [_solver(helm3d, p, s2, helm3d.PREC_C64, helm3d.ZT_PML_EIGEN, stream=stream) for p, s2 in zip(probs, S2)]
+    nsol = sum(int(f.shape[0]) for f in Fs)
+
+    def setup():
+        for s, s2 in zip(ss, S2):
+            s.set_medium(s2)
+
+    def grouped():
+        setup()
+        helm3d.solve_group(ss, Fs, us=Us, allow_not_converged=True)
+
+    def one_by_one():
+        setup()
+        for s, f, u in zip(ss, Fs, Us):
+            s.solve(f, nrhs=int(f.shape[0]), u=u, allow_not_converged=True)
+
+    out = {"mode": "group", "workload": "16 sources on 96^3 + 8 uneven grids (" +
+           ", ".join(f"{p.nx}x{p.ny}x{p.nz}" for p in probs[1:]) + "), one source each, own media, PML 8; "
+           f"c64 preconditioner (PML eigenbasis), FGMRES({RESTART}) to {TOL}; step = set-up + factor of all "
+           "grids + solve", "solves_per_step": nsol}
+    for name, fn in (("grouped", grouped), ("one_by_one", one_by_one)):
+        for _ in range(args.warmup):
+            fn()
+        ms = _events_ms(stream, fn, args.steps)
+        out[name] = {"ms_per_step": ms, "s_per_solve": ms / 1e3 / nsol,
+                     "iterations": [s.last_stats.iterations for s in ss],
+                     "relres_max": max(s.last_stats.relres for s in ss)}
+    for s in ss:
+        s.close()
+    return out
+
+
+def run_gradient(args):
+    """The misfit gradient on the 200^3 configuration (PML 16, 8 sources,
+    50 x 50 receivers at the top of the interior, data from a model with
+    +-10 % anomalies, gradient at the smooth starting model): time of one
+    helm3d_misfit_grad (forward solves, adjoint solves, gradient kernel; the
+    factor of the starting model is set-up), and central finite differences
+    of the misfit on 20 seeded interior cells.  J(s2 +- d e_c) is evaluated
+    exactly from the base solutions by the rank-one update of A (Sherman-
+    Morrison: u' = u - k w u_c / (1 + k w_c), w = A^{-1} e_c, k = omega^2
+    (1 + i beta) d), one extra solve per cell and no refactorization, so
+    that the difference is free of the solver's tolerance."""
+    import torch
+
+    import helm3d
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    start, true, recv = helm3d_media().config_c5(n=args.n if args.n != 128 else 200)
+    ns = len(true.sources)
+    F = torch.from_numpy(np.stack([true.rhs(i) for i in range(ns)])).to(dev)
+    rec = torch.from_numpy(recv).to(dev)
+    tol = 1e-10
+    # data from the true model
+    st_ = _solver(helm3d, true, torch.from_numpy(np.ascontiguousarray(true.s2)).to(dev), helm3d.PREC_C64,
+                  helm3d.ZT_PML_EIGEN, restart=30, tol=tol, stream=stream)
+    Ut = st_.solve(F, nrhs=ns)
+    data = Ut.reshape(ns, -1)[:, rec].contiguous()
+    st_.close()
+    del Ut
+    s2 = torch.from_numpy(np.ascontiguousarray(start.s2)).to(dev)
+    s = _solver(helm3d, start, s2, helm3d.PREC_C64, helm3d.ZT_PML_EIGEN, restart=30, tol=tol, stream=stream)
+    for _ in range(args.warmup):
+        s.misfit_grad(F, rec, data)
+    box = {}
+
+    def grad_step():
+        box["J"], box["g"] = s.misfit_grad(F, rec, data)
+    ms = _events_ms(stream, grad_step, args.steps)
+    its = s.last_stats.iterations
+    J, g = box["J"], box["g"].reshape(-1)
+    # base solutions and the finite differences
+    U = s.solve(F, nrhs=ns).reshape(ns, -1)
+    rng = helm3d_media().SplitMix64(77)
+    nz, ny, nx = start.shape
+    pm = start.pml + 4
+    cells = []
+    while len(cells) < 20:
+        i, j, k = (rng.randint(pm, nx - 1 - pm), rng.randint(pm, ny // 2), rng.randint(pm, nz - 1 - pm))
+        cells.append((k * ny + j) * nx + i)
+    E = torch.zeros((len(cells), nz * ny * nx), dtype=torch.complex128, device=dev)
+    for q, c in enumerate(cells):
+        E[q, c] = 1.0
+    W = torch.empty_like(E)
+    for q0 in range(0, len(cells), BATCH):
+        q1 = min(len(cells), q0 + BATCH)
+        s.solve(E[q0:q1], nrhs=q1 - q0, u=W[q0:q1])
+    resid = U[:, rec] - data                                   # (ns, nrecv)
+    kap0 = start.omega ** 2 * complex(1.0, start.beta_phys)
+    fd, ad = [], []
+    for q, c in enumerate(cells):
+        delta = 1e-3 * float(s2.reshape(-1)[c])
+        dJ = []
+        for sgn in (1.0, -1.0):
+            kap = kap0 * sgn * delta
+            wc = W[q, c]
+            du = -kap * W[q, rec][None, :] * (U[:, c][:, None] / (1.0 + kap * wc))   # P (u' - u)
+            dJ.append(float((torch.real(torch.conj(resid) * du)).sum() + 0.5 * (du.abs() ** 2).sum()))
+        fd.append((dJ[0] - dJ[1]) / (2 * delta))
+        ad.append(float(g[c]))
+    fd, ad = np.array(fd), np.array(ad)
+    relerr = np.abs(fd - ad) / np.maximum(np.abs(fd), 1e-300)
+    s.close()
+    return {"mode": "gradient", "workload": f"{nx}^3 (PML {start.pml}), {ns} sources, {len(recv)} receivers; "
+            f"gradient of 0.5||P u - d||^2 w.r.t. s^2 at the smooth starting model; c64 preconditioner, "
+            f"FGMRES(30) to {tol}", "ms_per_gradient": ms, "iterations": its, "misfit": J,
+            "fd_cells": len(cells), "fd_relerr_max": float(relerr.max()), "fd_relerr_median": float(np.median(relerr)),
+            "fd_step": "1e-3 s^2 at the cell (central)"}
+
+
+def helm3d_media():
+    from helm3d import media
+    return media
+
+
 # ------------------------------------------------------------ CPU baseline
 def cpu_port_sample(n: int, iters: int | None, cores: int, budget_iters: int = 2):
     """Time the oracle port (SciPy SuperLU per kz + NumPy FFT + NumPy stencil,
@@ -480,12 +681,27 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels", action="store_true",
                     help="per-kernel microbench: batched FGMRES(1) iterations instead of full solves")
+    ap.add_argument("--workload", default="headline", choices=["headline", "c3", "c4", "c5", "n200"],
+                    help="c3: 160^3 mixed precision, FGMRES(30); c4: 96^3 x 16 sources + 8 uneven grids as one "
+                         "group; c5: 200^3 misfit gradient with finite-difference check; n200: 200^3 batched "
+                         "complex64 vs plain complex128")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.kernels:
         print(json.dumps(run_kernels(args)))
+        return
+    if args.workload != "headline" and args.impl == "ours":
+        if args.workload == "c3":
+            out = run_large(args, 160, 30, "c3")
+        elif args.workload == "n200":
+            out = run_large(args, 200, RESTART, "n200")
+        elif args.workload == "c4":
+            out = run_group(args)
+        else:
+            out = run_gradient(args)
+        print(json.dumps(out))
         return
     if args.impl == "reference":
         # the CPU reference runs on rank 0 only; the other ranks exit at once

@@ -97,7 +97,7 @@ template <int RB, int CB, typename Cx> __device__ __forceinline__ Cx sel_row(con
 }
 
 template <typename R> struct Smem {
-    cplx<R> *sGT, *ringcol, *ringpv;
+    cplx<R> *sGT, *ringcol, *ringpv, *pinvs;
     int *ringr, *perm, *rinv;
     uint64_t *full, *empty;
 };
@@ -108,7 +108,8 @@ __device__ __forceinline__ Smem<R> carve(unsigned char *raw) {
     s.sGT = reinterpret_cast<cplx<R> *>(raw);
     s.ringcol = s.sGT + NPC * NP;
     s.ringpv = s.ringcol + kRing * NP;
-    s.ringr = reinterpret_cast<int *>(s.ringpv + kRing);
+    s.pinvs = s.ringpv + kRing;
+    s.ringr = reinterpret_cast<int *>(s.pinvs + NP);
     s.perm = s.ringr + kRing;
     s.rinv = s.perm + NP;
     uintptr_t b = reinterpret_cast<uintptr_t>(s.rinv + NP);
@@ -119,7 +120,7 @@ __device__ __forceinline__ Smem<R> carve(unsigned char *raw) {
 }
 
 template <typename R, int NP, int NPC> constexpr size_t factor_smem_bytes() {
-    return sizeof(cplx<R>) * ((size_t)NPC * NP + (size_t)kRing * NP + kRing) + sizeof(int) * (kRing + 2 * NP) +
+    return sizeof(cplx<R>) * ((size_t)NPC * NP + (size_t)kRing * NP + kRing + NP) + sizeof(int) * (kRing + 2 * NP) +
            16 + sizeof(uint64_t) * 2 * kRing;
 }
 
@@ -285,22 +286,29 @@ __global__ void __launch_bounds__(NW * 32, MB) factor_kernel(FactorK<R> a) {
             } else {
                 pinv = cinv(pv);
             }
+            if (threadIdx.x == 0) sm.pinvs[k] = pinv;
             const int rl = r & 31, ar = r >> 5;
             Cx prow[CB];
 #pragma unroll
             for (int b = 0; b < CB; b++) prow[b] = cmul(shfl_c(sel_row<RB, CB>(S, ar, b), rl), pinv);
+            // The pivot row is left unscaled (it holds pv times the
+            // normalized row, and 1 in column k) and divided by pv when G is
+            // written out, so that every other element takes one complex FMA
+            // with the column entry zeroed in the pivot row.
+#pragma unroll
+            for (int ra = 0; ra < RB; ra++) colk[ra] = csel((lane + 32 * ra) == r, mkc<R>(0, 0), colk[ra]);
             // element update of column slot b for step k
             auto update_col = [&](int b) {
-                const bool isk = (col0 + b) == k;
+                if ((col0 + b) == k) {
 #pragma unroll
-                for (int ra = 0; ra < RB; ra++) {
-                    const bool isr = (lane + 32 * ra) == r;
-                    Cx v;
-                    if (isr) v = isk ? pinv : prow[b];
-                    else if (isk) v = mkc<R>(-(colk[ra].x * pinv.x - colk[ra].y * pinv.y),
-                                             -(colk[ra].x * pinv.y + colk[ra].y * pinv.x));
-                    else v = cfms(colk[ra], prow[b], S[ra][b]);
-                    S[ra][b] = v;
+                    for (int ra = 0; ra < RB; ra++) {
+                        const Cx e = mkc<R>(-(colk[ra].x * pinv.x - colk[ra].y * pinv.y),
+                                            -(colk[ra].x * pinv.y + colk[ra].y * pinv.x));
+                        S[ra][b] = csel((lane + 32 * ra) == r, mkc<R>(1, 0), e);
+                    }
+                } else {
+#pragma unroll
+                    for (int ra = 0; ra < RB; ra++) S[ra][b] = cfms(colk[ra], prow[b], S[ra][b]);
                 }
             };
             if (lane == rl) used |= 1u << ar;
@@ -343,16 +351,19 @@ __global__ void __launch_bounds__(NW * 32, MB) factor_kernel(FactorK<R> a) {
         for (int ra = 0; ra < RB; ra++) {
             const int i = lane + 32 * ra;
             const int ri = sm.rinv[i];
+            // row i was the pivot of step ri: divide by its pivot
+            const Cx sc = (ri >= 0 && ri < n) ? sm.pinvs[ri] : mkc<R>(1, 0);
 #pragma unroll
             for (int b = 0; b < CB; b++) {
                 const int j = col0 + b;
                 const int pj = j < n ? sm.perm[j] : j;
                 if (!H3D_OK_IDX(pj >= 0 && pj < NP && ri >= 0 && ri < NP)) continue;
+                const Cx g = cmul(S[ra][b], sc);
                 if constexpr (C == 1) {
-                    sm.sGT[pj * NP + ri] = S[ra][b];
+                    sm.sGT[pj * NP + ri] = g;
                 } else {
                     const int q = pj / NPC;
-                    st_cluster_c(mapa_u32(smem_u32(&sm.sGT[(pj % NPC) * NP + ri]), (uint32_t)q), S[ra][b]);
+                    st_cluster_c(mapa_u32(smem_u32(&sm.sGT[(pj % NPC) * NP + ri]), (uint32_t)q), g);
                 }
             }
         }

@@ -40,6 +40,12 @@ __host__ __device__ inline void tf32_split_f(float v, float &hi, float &lo) {
     hi = tf32_round(v);
     lo = tf32_round(v - hi);
 }
+// the same split with lo left in FP32: v - hi is exact, and the tensor core
+// reads only its tf32 part, which drops less than 2^-21 |v|
+__host__ __device__ inline void tf32_split_fast(float v, float &hi, float &lo) {
+    hi = tf32_round(v);
+    lo = v - hi;
+}
 
 // byte offset of element (row, kk) in a no-swizzle K-major operand whose
 // rows hold KC elements (8-row groups SBO = KC / 4 * 128 bytes apart)
