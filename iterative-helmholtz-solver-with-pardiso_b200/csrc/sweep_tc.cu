@@ -15,27 +15,30 @@
 // D[i][2r] + i D[i][2r+1] = (G_j v)[i][r].  M = 128 (rows i, n <= 128),
 // N = 2 RR, K = 2 n padded to the chunk.
 //
-// Roles (10 warps):
-//   * warp 8, one lane: streams G_j^T (rows m, i contiguous, as the factor
+// Roles (14 warps):
+//   * warp 12, one lane: streams G_j^T (rows m, i contiguous, as the factor
 //     stores it) chunk by chunk (MC rows m) into a ring of shared-memory
 //     stages with 1D bulk copies, as far ahead as the ring allows;
-//   * warps 0-7: convert each chunk -- thread i reads G^T[m][i] for half of
-//     the chunk's m, splits it into tf32 hi + lo and stores both into TMEM
-//     (lane i, column K), one of three chunk buffers; at the end of a line
-//     they read D from TMEM (warp w: lanes 32 (w % 4) + [0, 32), the columns
-//     of half the right-hand sides), finish the line (y or x into the
-//     planes), write the next line's v to shared memory and from it the
-//     next B (hi and lo, canonical no-swizzle K-major layout, 16-byte units
-//     in address order so that the stores of a warp are contiguous);
-//   * warp 9, one lane: issues the MMAs of a line (A from TMEM, B from
+//   * warps 0-3 (converters): thread i of warp i / 32 reads G^T[m][i] for
+//     every m of the chunk, splits it into tf32 hi + lo and stores both into
+//     TMEM (lane i, column K), one of three chunk buffers, running ahead of
+//     the MMAs as far as the buffers allow;
+//   * warps 4-11 (epilogue): at the end of a line read D from TMEM (warp
+//     4 + e: lanes 32 (e % 4) + [0, 32), the columns of half the right-hand
+//     sides), finish the line (y or x into the planes), write the next
+//     line's v to shared memory and from it the next B (hi and lo, canonical
+//     no-swizzle K-major layout, 16-byte units in address order so that the
+//     stores of a warp are contiguous);
+//   * warp 13, one lane: issues the MMAs of a line (A from TMEM, B from
 //     shared memory) chunk by chunk as the buffers fill, and commits them to
 //     the buffer-free barriers and, after the last chunk, to the
 //     accumulator-ready barrier.
-// G^T chunks of the next line are converted while the current line's MMAs
-// run; the dependence chain per line is MMAs -> epilogue -> B.  Every wait is
-// bounded; on expiry bit 2 of *status is set and the kernel runs on without
-// waiting (results then invalid), waits (bounded) for its own MMAs and bulk
-// copies, frees its TMEM and returns.
+// The dependence chain per line is MMAs -> epilogue -> B; the conversion of
+// the next chunks and the bulk copies run beside it.  Ring positions advance
+// by counters (no integer division in the loops).  Every wait is bounded; on
+// expiry bit 2 of *status is set and the kernel runs on without waiting
+// (results then invalid), waits (bounded) for its own MMAs and bulk copies,
+// frees its TMEM and returns.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -47,12 +50,14 @@
 
 namespace h3d {
 
-constexpr int kTcConsumerWarps = 8;
-constexpr int kTcThreads = (kTcConsumerWarps + 2) * 32;
-constexpr int kTcMaxN = 128;           // MMA M: one row block
-constexpr int kTcBuf = 3;              // TMEM A chunk buffers
-constexpr int kTcLook = kTcBuf - 1;    // chunks of the next line converted before a line's epilogue
-constexpr uint32_t kTcCols = 512;      // TMEM columns: D at 0, buffer b at 128 (b + 1)
+constexpr int kTcConvWarps = 4;          // warps 0-3: G^T chunks -> TMEM
+constexpr int kTcEpiWarps = 8;           // warps 4-11: finish each line, build the next B
+constexpr int kTcProducerWarp = kTcConvWarps + kTcEpiWarps;
+constexpr int kTcMmaWarp = kTcProducerWarp + 1;
+constexpr int kTcThreads = (kTcMmaWarp + 1) * 32;
+constexpr int kTcMaxN = 128;             // MMA M: one row block
+constexpr int kTcBuf = 3;                // TMEM A chunk buffers
+constexpr uint32_t kTcCols = 512;        // TMEM columns: D at 0, buffer b at 128 (b + 1)
 constexpr uint32_t kTcWaitLimit = 1u << 22;
 
 struct SweepTcK {
@@ -68,8 +73,8 @@ struct SweepTcK {
     int *status;
 };
 
-__device__ __forceinline__ void tc_consumer_barrier() {
-    asm volatile("bar.sync 1, %0;" ::"n"(kTcConsumerWarps * 32) : "memory");
+__device__ __forceinline__ void tc_epilogue_barrier() {
+    asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");
 }
 
 template <bool ADJ> __device__ __forceinline__ float2 tc_adj_in(const SweepTcK &a, int line, int i, float2 f) {
@@ -81,23 +86,25 @@ template <bool ADJ> __device__ __forceinline__ float2 tc_adj_out(const SweepTcK 
     return cmul(make_float2(x.x, -x.y), a.dxy[(long)(a.ny + line) * a.n + i]);
 }
 
-// G^T rows of chunk `seq` of the chain (forward lines 0..ny-1, then
-// backward lines ny-2..0, MC rows m per chunk)
-template <int MC>
-__device__ __forceinline__ const float2 *tc_stage_src(const SweepTcK &a, int kz, long seq, int *rows) {
-    const long t = seq / a.cpl;
-    const int c = (int)(seq - t * a.cpl);
-    const int line = t < a.ny ? (int)t : (int)(2 * a.ny - 2 - t);
-    const int m0 = c * MC;
-    *rows = min(MC, a.n - m0);
-    return a.Gt + (((long)kz * a.ny + line) * a.n + m0) * (long)a.ldg;
-}
+// A position in a ring of `size` slots: the slot, and the parity of the
+// current pass over the ring (the phase an mbarrier of the slot completes
+// on this use).  Advanced by one per use, without divisions.
+struct RingPos {
+    int slot = 0;
+    uint32_t phase = 0;
+    __device__ __forceinline__ void next(int size) {
+        if (++slot == size) {
+            slot = 0;
+            phase ^= 1u;
+        }
+    }
+};
 
 template <int RR, int MC, bool ADJ>
 __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
     constexpr int NR = 2 * RR;        // B rows = D columns
     constexpr int KC = 2 * MC;        // K per chunk (TMEM columns of hi, and of lo)
-    constexpr int RH = RR / 2;        // right-hand sides per warpgroup in the epilogue
+    constexpr int RH = RR / 2;        // right-hand sides per epilogue warp
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const int n = a.n, ny = a.ny, ldg = a.ldg, Rn = a.nrhs, npad = a.npad, cpl = a.cpl;
     const int Kp = 2 * npad;
@@ -125,13 +132,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
     if (tid == 0) {
         for (int s = 0; s < a.nstage; s++) {
             mbar_init(&raw_full[s], 1);
-            mbar_init(&raw_empty[s], kTcConsumerWarps);
+            mbar_init(&raw_empty[s], kTcConvWarps);
         }
         for (int b = 0; b < kTcBuf; b++) {
-            mbar_init(&a_full[b], kTcConsumerWarps);
+            mbar_init(&a_full[b], kTcConvWarps);
             mbar_init(&a_empty[b], 1);
         }
-        mbar_init(b_full, kTcConsumerWarps);
+        mbar_init(b_full, kTcEpiWarps);
         mbar_init(d_full, 1);
         mbar_init(fin, 1);
         fence_mbar_init_cluster();
@@ -149,37 +156,53 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
         if (!dead && !mbar_wait_bounded_cta(smem_u32(bar), parity, kTcWaitLimit)) fail();
     };
 
-    if (warp == kTcConsumerWarps) {
+    if (warp == kTcProducerWarp) {
         // ---------------------------------------------------- producer
         if (lane == 0) {
+            // G^T rows of chunk c of step t: forward lines 0..ny-1, then
+            // backward lines ny-2..0, MC rows m per chunk
+            RingPos rp;
+            int t = 0, c = 0;
             for (long seq = 0; seq < nseq; seq++) {
-                const int s = (int)(seq % a.nstage);
-                if (seq >= a.nstage) wait(&raw_empty[s], (uint32_t)(((seq / a.nstage) & 1) ^ 1));
-                int rows;
-                const float2 *src = tc_stage_src<MC>(a, kz, seq, &rows);
+                if (seq >= a.nstage) wait(&raw_empty[rp.slot], rp.phase ^ 1u);
+                const int line = t < ny ? t : 2 * ny - 2 - t;
+                const int m0 = c * MC;
+                const int rows = min(MC, n - m0);
+                const float2 *src = a.Gt + (((long)kz * ny + line) * n + m0) * (long)ldg;
                 const uint32_t bytes = (uint32_t)rows * ldg * 8u;
-                mbar_expect_tx(&raw_full[s], bytes);
-                bulk_g2s(ring + (size_t)s * a.stage_bytes, src, bytes, &raw_full[s]);
+                mbar_expect_tx(&raw_full[rp.slot], bytes);
+                bulk_g2s(ring + (size_t)rp.slot * a.stage_bytes, src, bytes, &raw_full[rp.slot]);
+                rp.next(a.nstage);
+                if (++c == cpl) {
+                    c = 0;
+                    t++;
+                }
             }
-            // the copies still in flight land before the CTA exits
-            const long first = nseq > a.nstage ? nseq - a.nstage : 0;
-            for (long seq = first; seq < nseq; seq++)
-                mbar_wait_bounded_cta(smem_u32(&raw_full[seq % a.nstage]), (uint32_t)((seq / a.nstage) & 1),
-                                      kTcWaitLimit);
+            // the copies still in flight land before the CTA exits: the
+            // last use of every slot (rp is one past the final use)
+            for (int k = 0; k < a.nstage && k < nseq; k++) {
+                int sl = rp.slot - 1 - k;
+                uint32_t ph = rp.phase;
+                if (sl < 0) {
+                    sl += a.nstage;
+                    ph ^= 1u;
+                }
+                mbar_wait_bounded_cta(smem_u32(&raw_full[sl]), ph, kTcWaitLimit);
+            }
         }
-    } else if (warp == kTcConsumerWarps + 1) {
+    } else if (warp == kTcMmaWarp) {
         // --------------------------------------------------- MMA issuer
         if (lane == 0) {
             const uint32_t idesc = umma_idesc_tf32(NR);
             const uint32_t sbo = (uint32_t)(Kp / 4) * 128u;
             const uint32_t bhi = smem_u32(Bhi), blo = smem_u32(Blo);
+            RingPos bp;
             for (int t = 0; t < nsteps; t++) {
                 wait(b_full, (uint32_t)(t & 1));
                 tc_fence_after();
                 for (int c = 0; c < cpl; c++) {
-                    const long seq = (long)t * cpl + c;
-                    const int b = (int)(seq % kTcBuf);
-                    wait(&a_full[b], (uint32_t)((seq / kTcBuf) & 1));
+                    const int b = bp.slot;
+                    wait(&a_full[b], bp.phase);
                     tc_fence_after();
                     const uint32_t ahi = tmem + 128u * (uint32_t)(b + 1), alo = ahi + (uint32_t)KC;
 #pragma unroll
@@ -191,6 +214,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                         umma_tf32_ts(tmem, alo + (uint32_t)(ks * 8), dh, idesc, 1u);
                     }
                     umma_commit(&a_empty[b]);
+                    bp.next(kTcBuf);
                 }
                 umma_commit(d_full);
             }
@@ -198,30 +222,80 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             umma_commit(fin);
             mbar_wait_bounded_cta(smem_u32(fin), 0u, kTcWaitLimit);
         }
+    } else if (warp < kTcConvWarps) {
+        // --------------------------------------------------- converters
+        // warp q: TMEM lanes 32 q + [0, 32) = rows i of G_j, every m of the chunk
+        const int q = warp;
+        const int i = 32 * q + lane;
+        const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
+        RingPos rp, bp;
+        int c = 0;
+        for (long seq = 0; seq < nseq; seq++) {
+            const int s = rp.slot, b = bp.slot;
+            wait(&raw_full[s], rp.phase);
+            if (seq >= kTcBuf) wait(&a_empty[b], bp.phase ^ 1u);
+            tc_fence_after();
+            const int rows = min(MC, n - c * MC);
+            const float2 *raw = reinterpret_cast<const float2 *>(ring + (size_t)s * a.stage_bytes);
+            const uint32_t col = 128u * (uint32_t)(b + 1);
+            // 16 rows m at a time: 32 hi and 32 lo columns (K = 2 m + re/im)
+#pragma unroll
+            for (int h = 0; h < MC / 16; h++) {
+                float hv[32], lv[32];
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    const int ml = 16 * h + k;
+                    float2 g = make_float2(0.f, 0.f);
+                    if (i < n && ml < rows) g = raw[(size_t)ml * ldg + i];
+                    tf32_split_fast(g.x, hv[2 * k], lv[2 * k]);
+                    tf32_split_fast(g.y, hv[2 * k + 1], lv[2 * k + 1]);
+                }
+                tmem_st32(trow + col + (uint32_t)(32 * h), hv);
+                tmem_st32(trow + col + (uint32_t)(KC + 32 * h), lv);
+                tmem_wait_st();
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive_local(&raw_empty[s]);
+                mbar_arrive_local(&a_full[b]);
+            }
+            rp.next(a.nstage);
+            bp.next(kTcBuf);
+            if (++c == cpl) c = 0;
+        }
     } else {
-        // ------------------------------------------ converters / epilogue
-        const int q = warp & 3, wg = warp >> 2;
-        const int i = 32 * q + lane;                      // TMEM lane = row of G_j and of D
+        // ----------------------------------------------------- epilogue
+        // warp 4 + e: TMEM lanes 32 (e % 4) + [0, 32), right-hand sides
+        // (e / 4) RH + [0, RH)
+        const int ew = warp - kTcConvWarps;
+        const int q = ew & 3, wg = ew >> 2;
+        const int etid = tid - kTcConvWarps * 32;
+        const int i = 32 * q + lane;
         const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
 
-        // B (hi, lo) of the next line from vst; 16-byte units u in address
-        // order: row & 7, then the K quad, then the 8-row group
+        // B (hi, lo) of the next line from vst.  16-byte units in address
+        // order: row & 7, then the K quad kq, then the 8-row group rg; the
+        // NR / 8 groups are split among the warps (WPR warps each), a warp
+        // writing 4 consecutive K quads of its group per pass (512
+        // contiguous bytes)
+        constexpr int WPR = kTcEpiWarps / (NR / 8);
         auto build_b = [&]() {
             const int kq_n = Kp / 4;
-            const int units = NR * kq_n;
-            for (int u = tid; u < units; u += kTcConsumerWarps * 32) {
-                const int rlo = u & 7, rest = u >> 3;
-                const int kq = rest % kq_n, rg = rest / kq_n;
-                const int row = rg * 8 + rlo, r = row >> 1;
-                const float4 vv = *reinterpret_cast<const float4 *>(vst + (size_t)r * vld + 2 * kq);
+            const int rg = ew / WPR, rlo = lane & 7;
+            const int row = rg * 8 + rlo, r = row >> 1;
+            const float2 *vrow = vst + (size_t)r * vld;
+            for (int kq = (ew % WPR) * 4 + (lane >> 3); kq < kq_n; kq += 4 * WPR) {
+                const int u = (rg * kq_n + kq) * 8 + rlo;
+                const float4 vv = *reinterpret_cast<const float4 *>(vrow + 2 * kq);
                 float4 e;
                 if ((row & 1) == 0) e = make_float4(vv.x, -vv.y, vv.z, -vv.w);   // (Re v, -Im v)
                 else e = make_float4(vv.y, vv.x, vv.w, vv.z);                   // (Im v, Re v)
                 float4 h, l;
-                tf32_split_f(e.x, h.x, l.x);
-                tf32_split_f(e.y, h.y, l.y);
-                tf32_split_f(e.z, h.z, l.z);
-                tf32_split_f(e.w, h.w, l.w);
+                tf32_split_fast(e.x, h.x, l.x);
+                tf32_split_fast(e.y, h.y, l.y);
+                tf32_split_fast(e.z, h.z, l.z);
+                tf32_split_fast(e.w, h.w, l.w);
                 reinterpret_cast<float4 *>(Bhi)[u] = h;
                 reinterpret_cast<float4 *>(Blo)[u] = l;
             }
@@ -230,69 +304,42 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             if (lane == 0) mbar_arrive_local(b_full);
         };
 
-        // one chunk of G^T rows into TMEM buffer seq % kTcBuf (hi and lo)
-        auto convert = [&](long seq) {
-            const int s = (int)(seq % a.nstage);
-            const int b = (int)(seq % kTcBuf);
-            wait(&raw_full[s], (uint32_t)((seq / a.nstage) & 1));
-            if (seq >= kTcBuf) wait(&a_empty[b], (uint32_t)(((seq / kTcBuf) & 1) ^ 1));
-            tc_fence_after();
-            const int c = (int)(seq % cpl);
-            const int rows = min(MC, n - c * MC);
-            const float2 *raw = reinterpret_cast<const float2 *>(ring + (size_t)s * a.stage_bytes);
-            float hv[MC], lv[MC];
-#pragma unroll
-            for (int k = 0; k < MC / 2; k++) {
-                const int ml = wg * (MC / 2) + k;
-                float2 g = make_float2(0.f, 0.f);
-                if (i < n && ml < rows) g = raw[(size_t)ml * ldg + i];
-                tf32_split_f(g.x, hv[2 * k], lv[2 * k]);
-                tf32_split_f(g.y, hv[2 * k + 1], lv[2 * k + 1]);
-            }
-            const uint32_t col = 128u * (uint32_t)(b + 1) + (uint32_t)(wg * MC);
-            if constexpr (MC == 32) {
-                tmem_st32(trow + col, hv);
-                tmem_st32(trow + col + KC, lv);
-            } else {
-                tmem_st16(trow + col, hv);
-                tmem_st16(trow + col + KC, lv);
-            }
-            tmem_wait_st();
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) {
-                mbar_arrive_local(&raw_empty[s]);
-                mbar_arrive_local(&a_full[b]);
-            }
-        };
-
         // line 0's input: f_0 for every right-hand side
-        for (int e = tid; e < RR * npad; e += kTcConsumerWarps * 32) {
+        for (int e = etid; e < RR * npad; e += kTcEpiWarps * 32) {
             const int r = e / npad, m = e - r * npad;
             vst[(size_t)r * vld + m] =
                 (r < Rn && m < n) ? tc_adj_in<ADJ>(a, 0, m, P[(long)r * n + m]) : make_float2(0.f, 0.f);
         }
-        tc_consumer_barrier();
+        tc_epilogue_barrier();
         build_b();
 
-        long conv = 0;
-        for (int t = 0; t < nsteps; t++) {
-            const long target = min(nseq, (long)(t + 1) * cpl + kTcLook);
-            while (conv < target) convert(conv++);
+        // What finishing step t needs besides G v, loaded one step ahead (the
+        // planes do not fit in L2): f_{line+1} forward (and its adjoint
+        // scale), y_line backward.  Written by this same thread earlier, or
+        // untouched input.
+        auto load_pre = [&](int t, float2 (&v)[RH], float2 &dx) {
             const bool fwd = t < ny;
             const int line = fwd ? t : 2 * ny - 2 - t;
-            const bool last_fwd = fwd && line + 1 == ny;
-            // what finishing the line needs besides G v
-            float2 pre[RH];
+            const bool nxt = fwd && line + 1 < ny;
 #pragma unroll
             for (int k = 0; k < RH; k++) {
                 const int r = wg * RH + k;
-                pre[k] = make_float2(0.f, 0.f);
+                v[k] = make_float2(0.f, 0.f);
                 if (i < n && r < Rn) {
-                    if (fwd && !last_fwd) pre[k] = tc_adj_in<ADJ>(a, line + 1, i, P[((long)(line + 1) * Rn + r) * n + i]);
-                    else if (!fwd) pre[k] = P[((long)line * Rn + r) * n + i];
+                    if (nxt) v[k] = P[((long)(line + 1) * Rn + r) * n + i];
+                    else if (!fwd) v[k] = P[((long)line * Rn + r) * n + i];
                 }
             }
+            dx = (ADJ && nxt && i < n) ? a.dxy[(long)(line + 1) * n + i] : make_float2(0.f, 0.f);
+        };
+        float2 pv[RH], pvn[RH], dx, dxn;
+        load_pre(0, pv, dx);
+
+        for (int t = 0; t < nsteps; t++) {
+            if (t + 1 < nsteps) load_pre(t + 1, pvn, dxn);
+            const bool fwd = t < ny;
+            const int line = fwd ? t : 2 * ny - 2 - t;
+            const bool last_fwd = fwd && line + 1 == ny;
             const float2 cn = (fwd && !last_fwd) ? a.cmy[line + 1] : make_float2(0.f, 0.f);
             const float2 cp = fwd ? make_float2(0.f, 0.f) : a.cpy[line];
             wait(d_full, (uint32_t)(t & 1));
@@ -305,15 +352,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
 #pragma unroll
             for (int k = 0; k < RH; k++) {
                 const int r = wg * RH + k;
+                const float2 pre = (ADJ && fwd && !last_fwd) ? cmul(dx, make_float2(pv[k].x, -pv[k].y)) : pv[k];
                 const float2 acc = make_float2(d[2 * k], d[2 * k + 1]);
                 float2 out, vn;
                 bool fin_x;   // out is this line's final x
                 if (fwd) {
                     out = acc;                                        // y_line
                     fin_x = last_fwd;
-                    vn = fin_x ? out : cfms(cn, out, pre[k]);         // f_{line+1} - cmy y_line, or x_{ny-1}
+                    vn = fin_x ? out : cfms(cn, out, pre);            // f_{line+1} - cmy y_line, or x_{ny-1}
                 } else {
-                    out = cfms(cp, acc, pre[k]);                      // x_line = y_line - cpy G x_{line+1}
+                    out = cfms(cp, acc, pre);                         // x_line = y_line - cpy G x_{line+1}
                     fin_x = true;
                     vn = out;
                 }
@@ -322,9 +370,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                 if (i < npad) vst[(size_t)r * vld + i] = valid ? vn : make_float2(0.f, 0.f);
             }
             if (t + 1 < nsteps) {
-                tc_consumer_barrier();
+                tc_epilogue_barrier();
                 build_b();
             }
+#pragma unroll
+            for (int k = 0; k < RH; k++) pv[k] = pvn[k];
+            dx = dxn;
         }
     }
     tc_fence_before();
