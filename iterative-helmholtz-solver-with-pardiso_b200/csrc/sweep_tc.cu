@@ -1,6 +1,7 @@
 // sweep_tc.cu -- the block sweep of sweep.cu for complex64 batches of
 // right-hand sides on the 5th-generation tensor cores (tcgen05, kind::tf32,
-// FP32-class products by 3xTF32: a_hi b_hi + a_hi b_lo + a_lo b_hi).
+// FP32-class products by 3xTF32: a_hi b_hi + a_hi b_lo + a_lo b_hi, as two
+// MMAs per K step: a_hi [b_hi; b_lo] with N = 4 RR, and a_lo b_hi).
 // Same recurrence (the per-kz 2D solve replacing PARDISO phase 33,
 // Source/functions.cpp:5959, and DirSolveFastDiagStruct,
 // Source/HODLR/BinaryTreesHODLR.cpp:2971-3018):
@@ -57,7 +58,7 @@ constexpr int kTcMmaWarp = kTcProducerWarp + 1;
 constexpr int kTcThreads = (kTcMmaWarp + 1) * 32;
 constexpr int kTcMaxN = 128;             // MMA M: one row block
 constexpr int kTcBuf = 3;                // TMEM A chunk buffers
-constexpr uint32_t kTcCols = 512;        // TMEM columns: D at 0, buffer b at 128 (b + 1)
+constexpr uint32_t kTcCols = 512;        // TMEM columns: D at [0, 4 RR), buffer b at 128 (b + 1)
 constexpr uint32_t kTcWaitLimit = 1u << 22;
 
 struct SweepTcK {
@@ -193,9 +194,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
     } else if (warp == kTcMmaWarp) {
         // --------------------------------------------------- MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = umma_idesc_tf32(NR);
+            // Blo follows Bhi as further 8-row groups of the same layout, so
+            // one descriptor with N = 2 NR rows covers [B_hi; B_lo]
+            const uint32_t idesc2 = umma_idesc_tf32(2 * NR), idesc1 = umma_idesc_tf32(NR);
             const uint32_t sbo = (uint32_t)(Kp / 4) * 128u;
-            const uint32_t bhi = smem_u32(Bhi), blo = smem_u32(Blo);
+            const uint32_t bhi = smem_u32(Bhi);
             RingPos bp;
             for (int t = 0; t < nsteps; t++) {
                 wait(b_full, (uint32_t)(t & 1));
@@ -208,10 +211,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
 #pragma unroll
                     for (int ks = 0; ks < KC / 8; ks++) {
                         const uint32_t koff = (uint32_t)((c * KC + ks * 8) / 4) * 128u;
-                        const uint64_t dh = umma_desc(bhi + koff, 128, sbo), dl = umma_desc(blo + koff, 128, sbo);
-                        umma_tf32_ts(tmem, ahi + (uint32_t)(ks * 8), dh, idesc, (c > 0 || ks > 0) ? 1u : 0u);
-                        umma_tf32_ts(tmem, ahi + (uint32_t)(ks * 8), dl, idesc, 1u);
-                        umma_tf32_ts(tmem, alo + (uint32_t)(ks * 8), dh, idesc, 1u);
+                        const uint64_t db = umma_desc(bhi + koff, 128, sbo);
+                        // D[0, 2NR) (+)= a_hi [b_hi; b_lo], then D[0, NR) += a_lo b_hi
+                        umma_tf32_ts(tmem, ahi + (uint32_t)(ks * 8), db, idesc2, (c > 0 || ks > 0) ? 1u : 0u);
+                        umma_tf32_ts(tmem, alo + (uint32_t)(ks * 8), db, idesc1, 1u);
                     }
                     umma_commit(&a_empty[b]);
                     bp.next(kTcBuf);
@@ -344,16 +347,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             const float2 cp = fwd ? make_float2(0.f, 0.f) : a.cpy[line];
             wait(d_full, (uint32_t)(t & 1));
             tc_fence_after();
-            float d[RR];
-            if constexpr (RR == 16) tmem_ld16_nowait(trow + (uint32_t)(wg * RR), d);
-            else tmem_ld8_nowait(trow + (uint32_t)(wg * RR), d);
+            // D = a_hi b_hi + a_lo b_hi (columns c) + a_hi b_lo (columns NR + c)
+            float d[2 * RR];
+            if constexpr (RR == 16) {
+                tmem_ld16_nowait(trow + (uint32_t)(wg * RR), d);
+                tmem_ld16_nowait(trow + (uint32_t)(NR + wg * RR), d + RR);
+            } else {
+                tmem_ld8_nowait(trow + (uint32_t)(wg * RR), d);
+                tmem_ld8_nowait(trow + (uint32_t)(NR + wg * RR), d + RR);
+            }
             tmem_wait_ld(d);
             tc_fence_before();
 #pragma unroll
             for (int k = 0; k < RH; k++) {
                 const int r = wg * RH + k;
                 const float2 pre = (ADJ && fwd && !last_fwd) ? cmul(dx, make_float2(pv[k].x, -pv[k].y)) : pv[k];
-                const float2 acc = make_float2(d[2 * k], d[2 * k + 1]);
+                const float2 acc = make_float2(d[2 * k] + d[RR + 2 * k], d[2 * k + 1] + d[RR + 2 * k + 1]);
                 float2 out, vn;
                 bool fin_x;   // out is this line's final x
                 if (fwd) {
