@@ -278,6 +278,9 @@ def run_ours(args, rank, world, dist):
         "stencil": (16.0 * 2 + 8.0) * N * BATCH,
     }
     top = max(nbytes, key=lambda k: prof[k][0])
+    # DRAM read + write of one launch of the tensor-core sweep on this
+    # workload (128^3, 16 sources), from ncu: profiles/sweep_tc_n128_b16.md
+    traffic = 5.273e9 if (top == "sweep" and p.nx == 128 and BATCH == 16) else None
     k_ms, k_n = prof[top]
     avg_s = (k_ms / max(1, k_n)) / 1e3
     achieved = nbytes[top] / avg_s / 1e9 if avg_s > 0 else None
@@ -319,7 +322,7 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": int(launches_h),
         "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                     "bytes_per_launch": nbytes[top], "traffic": None},
+                     "bytes_per_launch": nbytes[top], "traffic": traffic},
         "kernel_ms_per_step": {k: round(v[0], 3) for k, v in prof.items()},
         "kernel_launches_per_step": {k: int(v[1]) for k, v in prof.items()},
         "kernel_share": {k: round(v[0] / total_prof, 4) for k, v in prof.items()} if total_prof > 0 else None,
