@@ -279,7 +279,8 @@ def run_ours(args, rank, world, dist):
     }
     top = max(nbytes, key=lambda k: prof[k][0])
     # DRAM read + write of one launch of the tensor-core sweep on this
-    # workload (128^3, 16 sources), from ncu: profiles/sweep_tc_n128_b16.md
+    # workload (128^3, 16 sources), measured with ncu (dram__bytes_read.sum
+    # + dram__bytes_write.sum of one captured launch)
     traffic = 5.273e9 if (top == "sweep" and p.nx == 128 and BATCH == 16) else None
     k_ms, k_n = prof[top]
     avg_s = (k_ms / max(1, k_n)) / 1e3
