@@ -119,7 +119,7 @@ int launch_sweep(bool c64, const SweepArgs &a, cudaStream_t s);
 // the CUDA-core kernels (0-5), the tensor-core kernel's chunk (6, 7)
 constexpr int kSweepVariants = 8;
 void sweep_variant(int v, SweepArgs &a);
-bool sweep_tc_supported(int n);
+bool sweep_tc_supported(const SweepArgs &a);   // shape and shared memory fit
 int launch_sweep_tc(const SweepArgs &a, int mc, cudaStream_t s);
 constexpr int kMaxBatch = 16;  // right-hand sides per preconditioner launch
 

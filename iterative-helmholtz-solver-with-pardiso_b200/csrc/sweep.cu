@@ -498,8 +498,8 @@ void sweep_variant(int v, SweepArgs &a) {
 
 int launch_sweep(bool c64, const SweepArgs &sa, cudaStream_t s) {
     if (sa.n < 1 || sa.n > kSweepMaxN || sa.R < 1 || sa.R > kMaxBatch) return HELM3D_ERR_ARG;
-    // the tensor-core kernel where it applies (complex64, one row block)
-    if (c64 && sa.tc_mc && sweep_tc_supported(sa.n)) return launch_sweep_tc(sa, sa.tc_mc, s);
+    // the tensor-core kernel where it applies (complex64, n <= 256, shared memory fits)
+    if (c64 && sa.tc_mc && sweep_tc_supported(sa)) return launch_sweep_tc(sa, sa.tc_mc, s);
     // complex64 batches of 3 or more: the register-tiled kernel (its 16-byte
     // tile loads need ldg, the padded row length, to be a multiple of 4)
     if (c64 && sa.R >= 3 && sa.ldg % 4 == 0) return sa.dxy ? sweep_tiled<true>(sa, s) : sweep_tiled<false>(sa, s);

@@ -56,9 +56,9 @@ constexpr int kTcEpiWarps = 8;           // warps 4-11: finish each line, build 
 constexpr int kTcProducerWarp = kTcConvWarps + kTcEpiWarps;
 constexpr int kTcMmaWarp = kTcProducerWarp + 1;
 constexpr int kTcThreads = (kTcMmaWarp + 1) * 32;
-constexpr int kTcMaxN = 128;             // MMA M: one row block
+constexpr int kTcMaxN = 256;             // two row blocks of MMA M = 128
 constexpr int kTcBuf = 3;                // TMEM A chunk buffers
-constexpr uint32_t kTcCols = 512;        // TMEM columns: D at [0, 4 RR), buffer b at 128 (b + 1)
+constexpr uint32_t kTcCols = 512;        // TMEM columns: D of row block rb at 4 RR rb, buffers from 128
 constexpr uint32_t kTcWaitLimit = 1u << 22;
 
 struct SweepTcK {
@@ -101,11 +101,17 @@ struct RingPos {
     }
 };
 
-template <int RR, int MC, bool ADJ>
+// MB row blocks of 128 rows i (n <= 128 MB).  TMEM: the accumulator of row
+// block rb at columns [2 NR rb, 2 NR (rb + 1)); chunk buffer b at 128 + b BW,
+// row block rb's hi at + 2 KC rb, its lo KC further (3 buffers fit for
+// MB = 1 with MC <= 32 and for MB = 2 with MC = 16).
+template <int RR, int MC, int MB, bool ADJ>
 __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
     constexpr int NR = 2 * RR;        // B rows = D columns
     constexpr int KC = 2 * MC;        // K per chunk (TMEM columns of hi, and of lo)
     constexpr int RH = RR / 2;        // right-hand sides per epilogue warp
+    constexpr int BW = MB * 2 * KC;   // TMEM columns of one chunk buffer
+    static_assert(MB * 2 * NR <= 128 && 128 + kTcBuf * BW <= (int)kTcCols, "TMEM layout");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const int n = a.n, ny = a.ny, ldg = a.ldg, Rn = a.nrhs, npad = a.npad, cpl = a.cpl;
     const int Kp = 2 * npad;
@@ -207,14 +213,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                     const int b = bp.slot;
                     wait(&a_full[b], bp.phase);
                     tc_fence_after();
-                    const uint32_t ahi = tmem + 128u * (uint32_t)(b + 1), alo = ahi + (uint32_t)KC;
+                    const uint32_t buf = tmem + 128u + (uint32_t)(b * BW);
 #pragma unroll
                     for (int ks = 0; ks < KC / 8; ks++) {
                         const uint32_t koff = (uint32_t)((c * KC + ks * 8) / 4) * 128u;
                         const uint64_t db = umma_desc(bhi + koff, 128, sbo);
-                        // D[0, 2NR) (+)= a_hi [b_hi; b_lo], then D[0, NR) += a_lo b_hi
-                        umma_tf32_ts(tmem, ahi + (uint32_t)(ks * 8), db, idesc2, (c > 0 || ks > 0) ? 1u : 0u);
-                        umma_tf32_ts(tmem, alo + (uint32_t)(ks * 8), db, idesc1, 1u);
+#pragma unroll
+                        for (int rb = 0; rb < MB; rb++) {
+                            // D_rb[0, 2NR) (+)= a_hi [b_hi; b_lo], then D_rb[0, NR) += a_lo b_hi
+                            const uint32_t d = tmem + (uint32_t)(rb * 2 * NR);
+                            const uint32_t ahi = buf + (uint32_t)(rb * 2 * KC + ks * 8);
+                            umma_tf32_ts(d, ahi, db, idesc2, (c > 0 || ks > 0) ? 1u : 0u);
+                            umma_tf32_ts(d, ahi + (uint32_t)KC, db, idesc1, 1u);
+                        }
                     }
                     umma_commit(&a_empty[b]);
                     bp.next(kTcBuf);
@@ -240,22 +251,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             tc_fence_after();
             const int rows = min(MC, n - c * MC);
             const float2 *raw = reinterpret_cast<const float2 *>(ring + (size_t)s * a.stage_bytes);
-            const uint32_t col = 128u * (uint32_t)(b + 1);
-            // 16 rows m at a time: 32 hi and 32 lo columns (K = 2 m + re/im)
+            // row block rb, 16 rows m at a time: 32 hi and 32 lo columns (K = 2 m + re/im)
 #pragma unroll
-            for (int h = 0; h < MC / 16; h++) {
-                float hv[32], lv[32];
+            for (int rb = 0; rb < MB; rb++) {
+                const int row = i + 128 * rb;
+                const uint32_t col = 128u + (uint32_t)(b * BW + rb * 2 * KC);
 #pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    const int ml = 16 * h + k;
-                    float2 g = make_float2(0.f, 0.f);
-                    if (i < n && ml < rows) g = raw[(size_t)ml * ldg + i];
-                    tf32_split_fast(g.x, hv[2 * k], lv[2 * k]);
-                    tf32_split_fast(g.y, hv[2 * k + 1], lv[2 * k + 1]);
+                for (int h = 0; h < MC / 16; h++) {
+                    float hv[32], lv[32];
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        const int ml = 16 * h + k;
+                        float2 g = make_float2(0.f, 0.f);
+                        if (row < n && ml < rows) g = raw[(size_t)ml * ldg + row];
+                        tf32_split_fast(g.x, hv[2 * k], lv[2 * k]);
+                        tf32_split_fast(g.y, hv[2 * k + 1], lv[2 * k + 1]);
+                    }
+                    tmem_st32(trow + col + (uint32_t)(32 * h), hv);
+                    tmem_st32(trow + col + (uint32_t)(KC + 32 * h), lv);
+                    tmem_wait_st();
                 }
-                tmem_st32(trow + col + (uint32_t)(32 * h), hv);
-                tmem_st32(trow + col + (uint32_t)(KC + 32 * h), lv);
-                tmem_wait_st();
             }
             tc_fence_before();
             __syncwarp();
@@ -319,23 +334,27 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
         // What finishing step t needs besides G v, loaded one step ahead (the
         // planes do not fit in L2): f_{line+1} forward (and its adjoint
         // scale), y_line backward.  Written by this same thread earlier, or
-        // untouched input.
-        auto load_pre = [&](int t, float2 (&v)[RH], float2 &dx) {
+        // untouched input.  Row i + 128 rb of row block rb.
+        auto load_pre = [&](int t, float2 (&v)[MB][RH], float2 (&dx)[MB]) {
             const bool fwd = t < ny;
             const int line = fwd ? t : 2 * ny - 2 - t;
             const bool nxt = fwd && line + 1 < ny;
 #pragma unroll
-            for (int k = 0; k < RH; k++) {
-                const int r = wg * RH + k;
-                v[k] = make_float2(0.f, 0.f);
-                if (i < n && r < Rn) {
-                    if (nxt) v[k] = P[((long)(line + 1) * Rn + r) * n + i];
-                    else if (!fwd) v[k] = P[((long)line * Rn + r) * n + i];
+            for (int rb = 0; rb < MB; rb++) {
+                const int row = i + 128 * rb;
+#pragma unroll
+                for (int k = 0; k < RH; k++) {
+                    const int r = wg * RH + k;
+                    v[rb][k] = make_float2(0.f, 0.f);
+                    if (row < n && r < Rn) {
+                        if (nxt) v[rb][k] = P[((long)(line + 1) * Rn + r) * n + row];
+                        else if (!fwd) v[rb][k] = P[((long)line * Rn + r) * n + row];
+                    }
                 }
+                dx[rb] = (ADJ && nxt && row < n) ? a.dxy[(long)(line + 1) * n + row] : make_float2(0.f, 0.f);
             }
-            dx = (ADJ && nxt && i < n) ? a.dxy[(long)(line + 1) * n + i] : make_float2(0.f, 0.f);
         };
-        float2 pv[RH], pvn[RH], dx, dxn;
+        float2 pv[MB][RH], pvn[MB][RH], dx[MB], dxn[MB];
         load_pre(0, pv, dx);
 
         for (int t = 0; t < nsteps; t++) {
@@ -347,44 +366,53 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             const float2 cp = fwd ? make_float2(0.f, 0.f) : a.cpy[line];
             wait(d_full, (uint32_t)(t & 1));
             tc_fence_after();
-            // D = a_hi b_hi + a_lo b_hi (columns c) + a_hi b_lo (columns NR + c)
-            float d[2 * RR];
-            if constexpr (RR == 16) {
-                tmem_ld16_nowait(trow + (uint32_t)(wg * RR), d);
-                tmem_ld16_nowait(trow + (uint32_t)(NR + wg * RR), d + RR);
-            } else {
-                tmem_ld8_nowait(trow + (uint32_t)(wg * RR), d);
-                tmem_ld8_nowait(trow + (uint32_t)(NR + wg * RR), d + RR);
-            }
-            tmem_wait_ld(d);
-            tc_fence_before();
 #pragma unroll
-            for (int k = 0; k < RH; k++) {
-                const int r = wg * RH + k;
-                const float2 pre = (ADJ && fwd && !last_fwd) ? cmul(dx, make_float2(pv[k].x, -pv[k].y)) : pv[k];
-                const float2 acc = make_float2(d[2 * k] + d[RR + 2 * k], d[2 * k + 1] + d[RR + 2 * k + 1]);
-                float2 out, vn;
-                bool fin_x;   // out is this line's final x
-                if (fwd) {
-                    out = acc;                                        // y_line
-                    fin_x = last_fwd;
-                    vn = fin_x ? out : cfms(cn, out, pre);            // f_{line+1} - cmy y_line, or x_{ny-1}
+            for (int rb = 0; rb < MB; rb++) {
+                const int row = i + 128 * rb;
+                // D = a_hi b_hi + a_lo b_hi (columns c) + a_hi b_lo (columns NR + c)
+                const uint32_t dcol = (uint32_t)(rb * 2 * NR + wg * RR);
+                float d[2 * RR];
+                if constexpr (RR == 16) {
+                    tmem_ld16_nowait(trow + dcol, d);
+                    tmem_ld16_nowait(trow + dcol + (uint32_t)NR, d + RR);
                 } else {
-                    out = cfms(cp, acc, pre);                         // x_line = y_line - cpy G x_{line+1}
-                    fin_x = true;
-                    vn = out;
+                    tmem_ld8_nowait(trow + dcol, d);
+                    tmem_ld8_nowait(trow + dcol + (uint32_t)NR, d + RR);
                 }
-                const bool valid = i < n && r < Rn;
-                if (valid) P[((long)line * Rn + r) * n + i] = fin_x ? tc_adj_out<ADJ>(a, line, i, out) : out;
-                if (i < npad) vst[(size_t)r * vld + i] = valid ? vn : make_float2(0.f, 0.f);
+                tmem_wait_ld(d);
+#pragma unroll
+                for (int k = 0; k < RH; k++) {
+                    const int r = wg * RH + k;
+                    const float2 pk = pv[rb][k];
+                    const float2 pre = (ADJ && fwd && !last_fwd) ? cmul(dx[rb], make_float2(pk.x, -pk.y)) : pk;
+                    const float2 acc = make_float2(d[2 * k] + d[RR + 2 * k], d[2 * k + 1] + d[RR + 2 * k + 1]);
+                    float2 out, vn;
+                    bool fin_x;   // out is this line's final x
+                    if (fwd) {
+                        out = acc;                                        // y_line
+                        fin_x = last_fwd;
+                        vn = fin_x ? out : cfms(cn, out, pre);            // f_{line+1} - cmy y_line, or x_{ny-1}
+                    } else {
+                        out = cfms(cp, acc, pre);                         // x_line = y_line - cpy G x_{line+1}
+                        fin_x = true;
+                        vn = out;
+                    }
+                    const bool valid = row < n && r < Rn;
+                    if (valid) P[((long)line * Rn + r) * n + row] = fin_x ? tc_adj_out<ADJ>(a, line, row, out) : out;
+                    if (row < npad) vst[(size_t)r * vld + row] = valid ? vn : make_float2(0.f, 0.f);
+                }
             }
+            tc_fence_before();
             if (t + 1 < nsteps) {
                 tc_epilogue_barrier();
                 build_b();
             }
 #pragma unroll
-            for (int k = 0; k < RH; k++) pv[k] = pvn[k];
-            dx = dxn;
+            for (int rb = 0; rb < MB; rb++) {
+#pragma unroll
+                for (int k = 0; k < RH; k++) pv[rb][k] = pvn[rb][k];
+                dx[rb] = dxn[rb];
+            }
         }
     }
     tc_fence_before();
@@ -394,52 +422,83 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
 }
 
 // ------------------------------------------------------------------- host
-bool sweep_tc_supported(int n) { return n >= 1 && n <= kTcMaxN; }
+// The launch shape of a batch: RR right-hand sides (8 or 16), chunk rows MC,
+// row blocks MB, ring depth and shared memory; false when it does not fit.
+struct TcShape {
+    int RR, MC, MB, npad, nstage;
+    uint32_t stage_bytes;
+    size_t smem;
+};
 
-template <int RR, int MC, bool ADJ> static int sweep_tc_impl(const SweepArgs &sa, cudaStream_t st) {
+static bool tc_shape(const SweepArgs &sa, int mc, TcShape &sh) {
+    if (sa.n < 1 || sa.n > kTcMaxN || sa.R < 1 || sa.R > 16) return false;
+    sh.RR = sa.R <= 8 ? 8 : 16;
+    sh.MB = sa.n > 128 ? 2 : 1;
+    sh.MC = (sh.MB == 2 || mc == 16) ? 16 : 32;   // two row blocks: 16-row chunks (TMEM)
+    sh.npad = ((sa.n + sh.MC - 1) / sh.MC) * sh.MC;
+    sh.stage_bytes = (uint32_t)((((size_t)sh.MC * sa.ldg * 8) + 127) & ~(size_t)127);
+    const size_t bbytes = 2 * sizeof(float) * (size_t)(2 * sh.RR) * (2 * sh.npad);
+    const size_t vbytes = sizeof(float2) * (size_t)sh.RR * (sh.npad + 2);
+    const size_t fixed = bbytes + vbytes + sizeof(uint64_t) * (2 * kTcBuf + 3) + 16;
+    const size_t optin = device_info().smem_optin;
+    const size_t per_stage = sh.stage_bytes + 2 * sizeof(uint64_t);
+    if (fixed + 2 * per_stage > optin) return false;
+    int nst = (int)((optin - fixed) / per_stage);
+    const int ring_cap = (int)(((size_t)sa.ring_kb * 1024) / sh.stage_bytes);
+    if (nst > ring_cap) nst = ring_cap;
+    if (nst > 8) nst = 8;
+    if (nst < 2) return false;
+    sh.nstage = nst;
+    sh.smem = (size_t)nst * per_stage + fixed;
+    return true;
+}
+
+bool sweep_tc_supported(const SweepArgs &sa) {
+    TcShape sh;
+    return tc_shape(sa, sa.tc_mc, sh);
+}
+
+template <int RR, int MC, int MB, bool ADJ> static int sweep_tc_impl(const SweepArgs &sa, const TcShape &sh,
+                                                                     cudaStream_t st) {
     SweepTcK k;
     k.n = sa.n;
     k.ny = sa.ny;
     k.ldg = sa.ldg;
     k.nrhs = sa.R;
-    k.npad = ((sa.n + MC - 1) / MC) * MC;
-    k.cpl = k.npad / MC;
+    k.npad = sh.npad;
+    k.cpl = sh.npad / MC;
     k.Gt = (const float2 *)sa.Gt;
     k.cmy = (const float2 *)sa.cmy;
     k.cpy = (const float2 *)sa.cpy;
     k.planes = (float2 *)sa.planes;
     k.dxy = (const float2 *)sa.dxy;
     k.status = sa.status;
-    k.stage_bytes = (uint32_t)((((size_t)MC * sa.ldg * 8) + 127) & ~(size_t)127);
-    const size_t bbytes = 2 * sizeof(float) * (size_t)(2 * RR) * (2 * k.npad);
-    const size_t vbytes = sizeof(float2) * (size_t)RR * (k.npad + 2);
-    const size_t fixed = bbytes + vbytes + sizeof(uint64_t) * (2 * kTcBuf + 3) + 16;
-    const size_t optin = device_info().smem_optin;
-    if (fixed + 2 * (size_t)k.stage_bytes + 2 * sizeof(uint64_t) * 2 > optin) return HELM3D_ERR_ARG;
-    int nst = (int)((optin - fixed) / (k.stage_bytes + 2 * sizeof(uint64_t)));
-    const int ring_cap = (int)(((size_t)sa.ring_kb * 1024) / k.stage_bytes);
-    if (nst > ring_cap) nst = ring_cap;
-    if (nst > 8) nst = 8;
-    if (nst < 2) return HELM3D_ERR_ARG;
-    k.nstage = nst;
-    const size_t smem = (size_t)nst * k.stage_bytes + bbytes + vbytes + sizeof(uint64_t) * (2 * nst + 2 * kTcBuf + 3) +
-                        16;
-    auto kern = sweep_tc_kernel<RR, MC, ADJ>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    k.stage_bytes = sh.stage_bytes;
+    k.nstage = sh.nstage;
+    auto kern = sweep_tc_kernel<RR, MC, MB, ADJ>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem) != cudaSuccess)
         return HELM3D_ERR_CUDA;
-    kern<<<dim3((unsigned)sa.nz), kTcThreads, smem, st>>>(k);
+    kern<<<dim3((unsigned)sa.nz), kTcThreads, sh.smem, st>>>(k);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 
-template <int MC, bool ADJ> static int sweep_tc_rr(const SweepArgs &sa, cudaStream_t s) {
-    if (sa.R <= 8) return sweep_tc_impl<8, MC, ADJ>(sa, s);
-    return sweep_tc_impl<16, MC, ADJ>(sa, s);
+template <bool ADJ> static int sweep_tc_adj(const SweepArgs &sa, const TcShape &sh, cudaStream_t s) {
+    if (sh.MB == 2) {
+        if (sh.RR == 8) return sweep_tc_impl<8, 16, 2, ADJ>(sa, sh, s);
+        return sweep_tc_impl<16, 16, 2, ADJ>(sa, sh, s);
+    }
+    if (sh.MC == 16) {
+        if (sh.RR == 8) return sweep_tc_impl<8, 16, 1, ADJ>(sa, sh, s);
+        return sweep_tc_impl<16, 16, 1, ADJ>(sa, sh, s);
+    }
+    if (sh.RR == 8) return sweep_tc_impl<8, 32, 1, ADJ>(sa, sh, s);
+    return sweep_tc_impl<16, 32, 1, ADJ>(sa, sh, s);
 }
 
 int launch_sweep_tc(const SweepArgs &sa, int mc, cudaStream_t s) {
-    if (!sweep_tc_supported(sa.n) || sa.R < 1 || sa.R > 16) return HELM3D_ERR_ARG;
-    if (mc == 16) return sa.dxy ? sweep_tc_rr<16, true>(sa, s) : sweep_tc_rr<16, false>(sa, s);
-    return sa.dxy ? sweep_tc_rr<32, true>(sa, s) : sweep_tc_rr<32, false>(sa, s);
+    TcShape sh;
+    if (!tc_shape(sa, mc, sh)) return HELM3D_ERR_ARG;
+    return sa.dxy ? sweep_tc_adj<true>(sa, sh, s) : sweep_tc_adj<false>(sa, sh, s);
 }
 
 }  // namespace h3d

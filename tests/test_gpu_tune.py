@@ -55,13 +55,14 @@ def test_solve_shapes_agree(family, count, nrhs, monkeypatch):
         s.close()
 
 
-@pytest.mark.parametrize("nx,nrhs", [(128, 16), (96, 8), (100, 3), (24, 16), (20, 5)])
+@pytest.mark.parametrize("nx,nrhs", [(128, 16), (96, 8), (100, 3), (24, 16), (20, 5), (200, 16), (160, 5), (129, 3)])
 def test_tensor_core_sweep_batches(nx, nrhs, monkeypatch):
     """The tensor-core sweep (variants 6 and 7: G^T chunks of 32 and 16 rows,
     3xTF32 products) in a batched complex64 preconditioner apply, forward and
     adjoint, against the oracle's M^{-1} x_r and M^{-H} x_r of every vector,
     beside the CUDA-core sweep (variant 0); block sizes one full row block
-    (128), padded (96, 100, 24, 20), batches padded to 8 or 16."""
+    (128), padded (96, 100, 24, 20), two row blocks (200, 160, 129), batches
+    padded to 8 or 16."""
     p = small_problem(nx, 10, 8, pml=3, seed=nx + nrhs)
     on = mode_n.setup(p, beta_prec=0.25)
     X = np.stack([rand_c(p.shape, seed=100 + r) for r in range(nrhs)])
