@@ -456,11 +456,13 @@ template <size_t K> static void shapes_for(const FactorShape (&t)[K], int n, int
     }
 }
 
+// After the register shapes, complex64 blocks of n <= 128 have one more
+// variant: the tensor-core factor (factor_tc.cu).
 int factor_variants(bool c64, int n) {
     int first, count;
     if (c64) shapes_for(kShapes64, n, first, count);
     else shapes_for(kShapes128, n, first, count);
-    return count;
+    return count + (factor_tc_supported(c64, n) ? 1 : 0);
 }
 
 bool factor_supported(bool c64, int n) { return n >= 1 && factor_variants(c64, n) > 0; }
@@ -470,6 +472,7 @@ int launch_factor(bool c64, const FactorArgs &fa, cudaStream_t s, int variant) {
     if (c64) shapes_for(kShapes64, fa.n, first, count);
     else shapes_for(kShapes128, fa.n, first, count);
     if (count == 0) return HELM3D_ERR_ARG;
+    if (variant == count && factor_tc_supported(c64, fa.n)) return launch_factor_tc(fa, s);
     if (variant < 0 || variant >= count) variant = 0;
     return (c64 ? kShapes64 : kShapes128)[first + variant].fn(fa, s);
 }

@@ -98,6 +98,9 @@ struct FactorArgs {
 // variant: one of the factor_variants(c64, n) launch shapes (0: the default)
 int launch_factor(bool c64, const FactorArgs &a, cudaStream_t s, int variant = 0);
 int factor_variants(bool c64, int n);
+// the tensor-core factor (complex64, n <= 128): the last factor variant
+bool factor_tc_supported(bool c64, int n);
+int launch_factor_tc(const FactorArgs &a, cudaStream_t s);
 bool factor_supported(bool c64, int n);
 
 // Forward/backward block sweep over y-lines for every kz and all R
