@@ -269,7 +269,11 @@ __global__ void __launch_bounds__(kFtThreads, 1) factor_tc_kernel(FactorTcK a) {
                         if (pv.x == 0.f && pv.y == 0.f) {
                             if (t == 0) atomicOr(a.status, 1);
                         } else {
-                            pinv = cinv(pv);
+                            // 1 / pv with two divisions, scaled against overflow of |pv|^2
+                            const float sc = 1.f / fmaxf(fabsf(pv.x), fabsf(pv.y));
+                            const float ax = pv.x * sc, ay = pv.y * sc;
+                            const float rd = sc / (ax * ax + ay * ay);
+                            pinv = make_float2(ax * rd, -ay * rd);
                         }
                     }
                     if (t == r) {
@@ -279,11 +283,12 @@ __global__ void __launch_bounds__(kFtThreads, 1) factor_tc_kernel(FactorTcK a) {
                         my_step = k;
                         sm.perm[k] = t;
                     } else {
-                        const float2 c = P[kk];
+                        // row -= (c / pv) * pivot row; column k becomes -c / pv
+                        const float2 sfac = cmul(P[kk], pinv);
 #pragma unroll
                         for (int e = 0; e < kFtB; e++)
-                            if (e != kk) P[e] = cfms(c, cmul(prow[e], pinv), P[e]);
-                        P[kk] = make_float2(-(c.x * pinv.x - c.y * pinv.y), -(c.x * pinv.y + c.y * pinv.x));
+                            if (e != kk) P[e] = cfms(sfac, prow[e], P[e]);
+                        P[kk] = make_float2(-sfac.x, -sfac.y);
                     }
                 }
 
