@@ -115,12 +115,17 @@ struct SweepArgs {
     int *status;              // device flag: bit 2 = a bounded wait expired
     int stage_kb = 16;        // bulk-copy stage of G^T rows (KB, about)
     int ring_kb = 200;        // shared-memory ring of stages (KB, at most)
-    int tc_mc = 0;            // complex64, n <= 128: the tensor-core sweep with G^T chunks of tc_mc rows (16, 32)
+    int tc_mc = 0;            // complex64, n <= 256: the tensor-core sweep with G^T chunks of tc_mc rows (16, 32)
+    int tc_f16 = 0;           // ... with FP16 hi/lo products (K = 16 per MMA), scaled by gscale
+    const float *gscale = nullptr;   // [nz][ny] power-of-two scales of the blocks (launch_gscale)
 };
 int launch_sweep(bool c64, const SweepArgs &a, cudaStream_t s);
 // the sweep's launch variants the autotuner times: stage and ring sizes of
-// the CUDA-core kernels (0-5), the tensor-core kernel's chunk (6, 7)
-constexpr int kSweepVariants = 8;
+// the CUDA-core kernels (0-5), the tensor-core kernel's chunk (6, 7), the
+// tensor-core kernel with FP16 products (8)
+constexpr int kSweepVariants = 9;
+// power-of-two scale of every complex64 block G_j for the FP16 products
+int launch_gscale(const void *Gt, int n, int ny, int nz, int ldg, float *gscale, cudaStream_t s);
 void sweep_variant(int v, SweepArgs &a);
 bool sweep_tc_supported(const SweepArgs &a);   // shape and shared memory fit
 int launch_sweep_tc(const SweepArgs &a, int mc, cudaStream_t s);
@@ -296,6 +301,7 @@ struct helm3d_ctx {
 
     // device buffers
     void *d_Gt = nullptr;          // factor
+    float *d_gscale = nullptr;     // [nz][ny] scales of the complex64 blocks (FP16 sweep)
     size_t Gt_bytes = 0;
     void *d_tw = nullptr;          // FFT tables (precision P)
     void *d_cmx = nullptr, *d_cpx = nullptr, *d_cmy = nullptr, *d_cpy = nullptr;   // P precision

@@ -403,6 +403,7 @@ int ctx_setup_grid(helm3d_ctx *c) {
     c->ldg = (nx + 3) & ~3;
     c->Gt_bytes = esz * (size_t)nz * ny * nx * c->ldg;
     if ((rc = dalloc(c, &c->d_Gt, c->Gt_bytes, "block LU factor"))) return rc;
+    if ((rc = dalloc(c, (void **)&c->d_gscale, sizeof(float) * (size_t)nz * ny, "block scales"))) return rc;
     return HELM3D_OK;
 }
 
@@ -528,6 +529,12 @@ int ctx_factor(helm3d_ctx *c) {
     }
     rc = timed(c, HELM3D_K_FACTOR, 1, [&] { return launch_factor(c->c64, a, c->stream, c->tv_factor); });
     if (rc) return set_error(c, rc, std::string("factor launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+    // complex64: the blocks' power-of-two scales for the FP16 sweep
+    if (c->c64) {
+        rc = timed(c, HELM3D_K_FACTOR, 1,
+                   [&] { return launch_gscale(c->d_Gt, a.n, a.ny, a.nz, a.ldg, c->d_gscale, c->stream); });
+        if (rc) return set_error(c, rc, "block scales launch failed");
+    }
     int st = 0;
     rc = cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");
     if (rc) return rc;

@@ -487,13 +487,15 @@ template <typename R, int G> static int sweep_g(const SweepArgs &sa, cudaStream_
 }
 
 void sweep_variant(int v, SweepArgs &a) {
-    static const int kStage[kSweepVariants] = {16, 8, 32, 16, 8, 32, 16, 16};
-    static const int kRingKb[kSweepVariants] = {200, 200, 200, 100, 100, 100, 200, 200};
-    static const int kTcMc[kSweepVariants] = {0, 0, 0, 0, 0, 0, 32, 16};
+    static const int kStage[kSweepVariants] = {16, 8, 32, 16, 8, 32, 16, 16, 16};
+    static const int kRingKb[kSweepVariants] = {200, 200, 200, 100, 100, 100, 200, 200, 200};
+    static const int kTcMc[kSweepVariants] = {0, 0, 0, 0, 0, 0, 32, 16, 32};
+    static const int kTcF16[kSweepVariants] = {0, 0, 0, 0, 0, 0, 0, 0, 1};
     if (v < 0 || v >= kSweepVariants) v = 0;
     a.stage_kb = kStage[v];
     a.ring_kb = kRingKb[v];
     a.tc_mc = kTcMc[v];
+    a.tc_f16 = kTcF16[v];
 }
 
 int launch_sweep(bool c64, const SweepArgs &sa, cudaStream_t s) {

@@ -42,6 +42,8 @@
 // frees its TMEM and returns.
 #include <cuda_runtime.h>
 
+#include <cuda_fp16.h>
+
 #include <cstdint>
 
 #include "cplx.cuh"
@@ -63,6 +65,7 @@ constexpr uint32_t kTcWaitLimit = 1u << 22;
 
 struct SweepTcK {
     int n, ny, ldg, nrhs;
+    const float *gscale; // FP16 products: power-of-two scale of each block G_j ([nz][ny])
     int npad;            // n rounded up to the chunk (K = 2 npad)
     int cpl;             // chunks per line
     int nstage;          // bulk-copy ring depth
@@ -87,6 +90,33 @@ template <bool ADJ> __device__ __forceinline__ float2 tc_adj_out(const SweepTcK 
     return cmul(make_float2(x.x, -x.y), a.dxy[(long)(a.ny + line) * a.n + i]);
 }
 
+// FP16 hi/lo of a pair (x, y), each as a packed pair (x in the low half):
+// hi = x rounded to 11 significant bits in FP32 (exact in FP16 in its
+// normal range), lo = x - hi (exact in FP32) rounded to FP16 -- two
+// conversions per pair
+__device__ __forceinline__ uint2 f16_split2(float x, float y) {
+    const float hx = tf32_round(x), hy = tf32_round(y);
+    const __half2 hi = __floats2half2_rn(hx, hy);
+    const __half2 lo = __floats2half2_rn(x - hx, y - hy);
+    return make_uint2(*reinterpret_cast<const uint32_t *>(&hi), *reinterpret_cast<const uint32_t *>(&lo));
+}
+
+// 2^(13 - e) for mx in [2^e, 2^(e+1)): scales the largest entry into
+// [2^13, 2^14) (1 for mx = 0 or not finite)
+__device__ __forceinline__ float pow2_scale_13(float mx) {
+    const uint32_t b = __float_as_uint(mx);
+    const int ex = (int)((b >> 23) & 0xffu);
+    if (mx <= 0.f || ex == 0xff) return 1.f;
+    int e = (ex == 0 ? -126 : ex - 127);
+    e = max(-100, min(100, e));
+    return __uint_as_float((uint32_t)(127 + 13 - e) << 23);
+}
+
+// 1 / s for a power of two s (exact)
+__device__ __forceinline__ float pow2_inv(float s) {
+    return __uint_as_float((254u - ((__float_as_uint(s) >> 23) & 0xffu)) << 23);
+}
+
 // A position in a ring of `size` slots: the slot, and the parity of the
 // current pass over the ring (the phase an mbarrier of the slot completes
 // on this use).  Advanced by one per use, without divisions.
@@ -104,11 +134,19 @@ struct RingPos {
 // MB row blocks of 128 rows i (n <= 128 MB).  TMEM: the accumulator of row
 // block rb at columns [2 NR rb, 2 NR (rb + 1)); chunk buffer b at 128 + b BW,
 // row block rb's hi at + 2 KC rb, its lo KC further (3 buffers fit for
-// MB = 1 with MC <= 32 and for MB = 2 with MC = 16).
-template <int RR, int MC, int MB, bool ADJ>
+// MB = 1 with MC <= 32 and for MB = 2 with MC = 16, or MC = 32 with F16).
+//
+// F16: the products in kind::f16 (K = 16 per MMA, half the MMAs of tf32)
+// with FP16 hi/lo splits (11 + 11 significant bits, as tf32's), G_j scaled
+// by its power-of-two block scale and each right-hand side's v by a power of
+// two chosen per line from its largest entry (so that the largest scaled
+// entries lie in [2^13, 2^14) and the lo parts stay normal), the
+// accumulator unscaled exactly in the epilogue.  A packs one complex m per
+// TMEM column (re | im as two halves).
+template <int RR, int MC, int MB, bool ADJ, bool F16>
 __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
     constexpr int NR = 2 * RR;        // B rows = D columns
-    constexpr int KC = 2 * MC;        // K per chunk (TMEM columns of hi, and of lo)
+    constexpr int KC = F16 ? MC : 2 * MC;   // TMEM columns of hi, and of lo, per chunk (K = 2 MC)
     constexpr int RH = RR / 2;        // right-hand sides per epilogue warp
     constexpr int BW = MB * 2 * KC;   // TMEM columns of one chunk buffer
     static_assert(MB * 2 * NR <= 128 && 128 + kTcBuf * BW <= (int)kTcCols, "TMEM layout");
@@ -122,10 +160,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
 
     unsigned char *ring = smem_raw;
     float *Bhi = reinterpret_cast<float *>(smem_raw + (size_t)a.nstage * a.stage_bytes);
-    float *Blo = Bhi + (size_t)NR * Kp;
+    // B_lo follows B_hi as further 8-row groups (FP16: half the bytes)
+    float *Blo = Bhi + (size_t)NR * Kp / (F16 ? 2 : 1);
     const int vld = npad + 2;         // padded row of vst (bank spread across right-hand sides)
-    float2 *vst = reinterpret_cast<float2 *>(Blo + (size_t)NR * Kp);   // [RR][vld]
-    uint64_t *raw_full = reinterpret_cast<uint64_t *>(vst + (size_t)RR * vld);
+    float2 *vst = reinterpret_cast<float2 *>(Bhi + 2 * (size_t)NR * Kp);   // [RR][vld]
+    float *vmax = reinterpret_cast<float *>(vst + (size_t)RR * vld);       // F16: [4][RR]
+    uint64_t *raw_full = reinterpret_cast<uint64_t *>(vmax + 4 * RR);
     uint64_t *raw_empty = raw_full + a.nstage;
     uint64_t *a_full = raw_empty + a.nstage;
     uint64_t *a_empty = a_full + kTcBuf;
@@ -202,8 +242,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
         if (lane == 0) {
             // Blo follows Bhi as further 8-row groups of the same layout, so
             // one descriptor with N = 2 NR rows covers [B_hi; B_lo]
-            const uint32_t idesc2 = umma_idesc_tf32(2 * NR), idesc1 = umma_idesc_tf32(NR);
-            const uint32_t sbo = (uint32_t)(Kp / 4) * 128u;
+            const uint32_t idesc2 = F16 ? umma_idesc_f16(2 * NR) : umma_idesc_tf32(2 * NR);
+            const uint32_t idesc1 = F16 ? umma_idesc_f16(NR) : umma_idesc_tf32(NR);
+            constexpr int KE = F16 ? 8 : 4;   // K elements per 16-byte core-matrix row
+            constexpr int KS = F16 ? 16 : 8;  // K per MMA
+            const uint32_t sbo = (uint32_t)(Kp / KE) * 128u;
             const uint32_t bhi = smem_u32(Bhi);
             RingPos bp;
             for (int t = 0; t < nsteps; t++) {
@@ -215,16 +258,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                     tc_fence_after();
                     const uint32_t buf = tmem + 128u + (uint32_t)(b * BW);
 #pragma unroll
-                    for (int ks = 0; ks < KC / 8; ks++) {
-                        const uint32_t koff = (uint32_t)((c * KC + ks * 8) / 4) * 128u;
+                    for (int ks = 0; ks < 2 * MC / KS; ks++) {
+                        const uint32_t koff = (uint32_t)((c * 2 * MC + ks * KS) / KE) * 128u;
                         const uint64_t db = umma_desc(bhi + koff, 128, sbo);
 #pragma unroll
                         for (int rb = 0; rb < MB; rb++) {
                             // D_rb[0, 2NR) (+)= a_hi [b_hi; b_lo], then D_rb[0, NR) += a_lo b_hi
+                            // (8 TMEM columns of A per MMA: 8 tf32, or 16 fp16 in pairs)
                             const uint32_t d = tmem + (uint32_t)(rb * 2 * NR);
                             const uint32_t ahi = buf + (uint32_t)(rb * 2 * KC + ks * 8);
-                            umma_tf32_ts(d, ahi, db, idesc2, (c > 0 || ks > 0) ? 1u : 0u);
-                            umma_tf32_ts(d, ahi + (uint32_t)KC, db, idesc1, 1u);
+                            if constexpr (F16) {
+                                umma_f16_ts(d, ahi, db, idesc2, (c > 0 || ks > 0) ? 1u : 0u);
+                                umma_f16_ts(d, ahi + (uint32_t)KC, db, idesc1, 1u);
+                            } else {
+                                umma_tf32_ts(d, ahi, db, idesc2, (c > 0 || ks > 0) ? 1u : 0u);
+                                umma_tf32_ts(d, ahi + (uint32_t)KC, db, idesc1, 1u);
+                            }
                         }
                     }
                     umma_commit(&a_empty[b]);
@@ -243,7 +292,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
         const int i = 32 * q + lane;
         const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
         RingPos rp, bp;
-        int c = 0;
+        int c = 0, t = 0;
+        float gs = F16 ? a.gscale[(long)kz * ny] : 1.f;   // scale of the current line's block
         for (long seq = 0; seq < nseq; seq++) {
             const int s = rp.slot, b = bp.slot;
             wait(&raw_full[s], rp.phase);
@@ -251,6 +301,30 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             tc_fence_after();
             const int rows = min(MC, n - c * MC);
             const float2 *raw = reinterpret_cast<const float2 *>(ring + (size_t)s * a.stage_bytes);
+            if constexpr (F16) {
+                // one complex m per TMEM column: (re | im) hi, and lo, in FP16
+#pragma unroll
+                for (int rb = 0; rb < MB; rb++) {
+                    const int row = i + 128 * rb;
+                    const uint32_t col = 128u + (uint32_t)(b * BW + rb * 2 * KC);
+#pragma unroll
+                    for (int h = 0; h < MC / 16; h++) {
+                        float hv[16], lv[16];
+#pragma unroll
+                        for (int k = 0; k < 16; k++) {
+                            const int ml = 16 * h + k;
+                            float2 g = make_float2(0.f, 0.f);
+                            if (row < n && ml < rows) g = raw[(size_t)ml * ldg + row];
+                            const uint2 pk = f16_split2(g.x * gs, g.y * gs);
+                            hv[k] = __uint_as_float(pk.x);
+                            lv[k] = __uint_as_float(pk.y);
+                        }
+                        tmem_st16(trow + col + (uint32_t)(16 * h), hv);
+                        tmem_st16(trow + col + (uint32_t)(KC + 16 * h), lv);
+                        tmem_wait_st();
+                    }
+                }
+            } else {
             // row block rb, 16 rows m at a time: 32 hi and 32 lo columns (K = 2 m + re/im)
 #pragma unroll
             for (int rb = 0; rb < MB; rb++) {
@@ -272,6 +346,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                     tmem_wait_st();
                 }
             }
+            }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) {
@@ -280,7 +355,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             }
             rp.next(a.nstage);
             bp.next(kTcBuf);
-            if (++c == cpl) c = 0;
+            if (++c == cpl) {
+                c = 0;
+                if (F16 && ++t < nsteps) gs = a.gscale[(long)kz * ny + (t < ny ? t : 2 * ny - 2 - t)];
+            }
         }
     } else {
         // ----------------------------------------------------- epilogue
@@ -288,7 +366,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
         // (e / 4) RH + [0, RH)
         const int ew = warp - kTcConvWarps;
         const int q = ew & 3, wg = ew >> 2;
-        const int etid = tid - kTcConvWarps * 32;
         const int i = 32 * q + lane;
         const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
 
@@ -298,11 +375,48 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
         // writing 4 consecutive K quads of its group per pass (512
         // contiguous bytes)
         constexpr int WPR = kTcEpiWarps / (NR / 8);
+        // FP16: the power-of-two scale of right-hand side r's next v, from
+        // the per-quarter maxima in vmax (the same value in every thread)
+        auto v_scale = [&](int r) -> float {
+            float mx = 0.f;
+#pragma unroll
+            for (int qq = 0; qq < 4; qq++) mx = fmaxf(mx, vmax[qq * RR + r]);
+            return pow2_scale_13(mx);
+        };
         auto build_b = [&]() {
-            const int kq_n = Kp / 4;
             const int rg = ew / WPR, rlo = lane & 7;
             const int row = rg * 8 + rlo, r = row >> 1;
             const float2 *vrow = vst + (size_t)r * vld;
+            if constexpr (F16) {
+                // 16-byte units of 8 K = 4 complex m, in address order (row & 7, K octet, 8-row group)
+                const int ko_n = Kp / 8;
+                const float sv = v_scale(r);
+                for (int ko = (ew % WPR) * 4 + (lane >> 3); ko < ko_n; ko += 4 * WPR) {
+                    const int u = (rg * ko_n + ko) * 8 + rlo;
+                    const float4 va = *reinterpret_cast<const float4 *>(vrow + 4 * ko);
+                    const float4 vb = *reinterpret_cast<const float4 *>(vrow + 4 * ko + 2);
+                    float e[8];
+                    if ((row & 1) == 0) {   // (Re v, -Im v)
+                        e[0] = va.x; e[1] = -va.y; e[2] = va.z; e[3] = -va.w;
+                        e[4] = vb.x; e[5] = -vb.y; e[6] = vb.z; e[7] = -vb.w;
+                    } else {                // (Im v, Re v)
+                        e[0] = va.y; e[1] = va.x; e[2] = va.w; e[3] = va.z;
+                        e[4] = vb.y; e[5] = vb.x; e[6] = vb.w; e[7] = vb.z;
+                    }
+                    uint4 h, l;
+                    uint2 p0 = f16_split2(e[0] * sv, e[1] * sv), p1 = f16_split2(e[2] * sv, e[3] * sv);
+                    uint2 p2 = f16_split2(e[4] * sv, e[5] * sv), p3 = f16_split2(e[6] * sv, e[7] * sv);
+                    h = make_uint4(p0.x, p1.x, p2.x, p3.x);
+                    l = make_uint4(p0.y, p1.y, p2.y, p3.y);
+                    reinterpret_cast<uint4 *>(Bhi)[u] = h;
+                    reinterpret_cast<uint4 *>(Blo)[u] = l;
+                }
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_local(b_full);
+                return;
+            }
+            const int kq_n = Kp / 4;
             for (int kq = (ew % WPR) * 4 + (lane >> 3); kq < kq_n; kq += 4 * WPR) {
                 const int u = (rg * kq_n + kq) * 8 + rlo;
                 const float4 vv = *reinterpret_cast<const float4 *>(vrow + 2 * kq);
@@ -322,13 +436,48 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             if (lane == 0) mbar_arrive_local(b_full);
         };
 
-        // line 0's input: f_0 for every right-hand side
-        for (int e = etid; e < RR * npad; e += kTcEpiWarps * 32) {
-            const int r = e / npad, m = e - r * npad;
-            vst[(size_t)r * vld + m] =
-                (r < Rn && m < n) ? tc_adj_in<ADJ>(a, 0, m, P[(long)r * n + m]) : make_float2(0.f, 0.f);
+        // FP16: this warp's per-right-hand-side maxima of the next v into
+        // vmax[q][r] (one writer per entry; every reader of the previous
+        // values is past the B-ready barrier by then)
+        auto put_vmax = [&](float (&am)[RH]) {
+            if constexpr (F16) {
+#pragma unroll
+                for (int k = 0; k < RH; k++) {
+                    // non-negative floats order like their bit patterns
+                    const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(am[k]));
+                    if (lane == 0) vmax[q * RR + wg * RH + k] = __uint_as_float(m);
+                }
+            }
+        };
+        float sv_cur[RH];   // scales of the v this thread's line is multiplied with
+#pragma unroll
+        for (int k = 0; k < RH; k++) sv_cur[k] = 1.f;
+
+        // line 0's input: f_0 of this thread's rows and right-hand sides
+        {
+            float am[RH];
+#pragma unroll
+            for (int k = 0; k < RH; k++) am[k] = 0.f;
+#pragma unroll
+            for (int rb = 0; rb < MB; rb++) {
+                const int m = i + 128 * rb;
+                if (m >= npad) continue;
+#pragma unroll
+                for (int k = 0; k < RH; k++) {
+                    const int r = wg * RH + k;
+                    const float2 f = (r < Rn && m < n) ? tc_adj_in<ADJ>(a, 0, m, P[(long)r * n + m])
+                                                       : make_float2(0.f, 0.f);
+                    vst[(size_t)r * vld + m] = f;
+                    am[k] = fmaxf(am[k], fmaxf(fabsf(f.x), fabsf(f.y)));
+                }
+            }
+            put_vmax(am);
         }
         tc_epilogue_barrier();
+        if constexpr (F16) {
+#pragma unroll
+            for (int k = 0; k < RH; k++) sv_cur[k] = v_scale(wg * RH + k);
+        }
         build_b();
 
         // What finishing step t needs besides G v, loaded one step ahead (the
@@ -364,6 +513,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             const bool last_fwd = fwd && line + 1 == ny;
             const float2 cn = (fwd && !last_fwd) ? a.cmy[line + 1] : make_float2(0.f, 0.f);
             const float2 cp = fwd ? make_float2(0.f, 0.f) : a.cpy[line];
+            const float igs = F16 ? pow2_inv(a.gscale[(long)kz * ny + line]) : 1.f;
+            float us[RH];   // exact unscaling: 1 / (block scale * right-hand-side scale)
+#pragma unroll
+            for (int k = 0; k < RH; k++) us[k] = F16 ? igs * pow2_inv(sv_cur[k]) : 1.f;
+            float am[RH];
+#pragma unroll
+            for (int k = 0; k < RH; k++) am[k] = 0.f;
             wait(d_full, (uint32_t)(t & 1));
             tc_fence_after();
 #pragma unroll
@@ -385,7 +541,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                     const int r = wg * RH + k;
                     const float2 pk = pv[rb][k];
                     const float2 pre = (ADJ && fwd && !last_fwd) ? cmul(dx[rb], make_float2(pk.x, -pk.y)) : pk;
-                    const float2 acc = make_float2(d[2 * k] + d[RR + 2 * k], d[2 * k + 1] + d[RR + 2 * k + 1]);
+                    const float2 acc = make_float2((d[2 * k] + d[RR + 2 * k]) * us[k],
+                                                   (d[2 * k + 1] + d[RR + 2 * k + 1]) * us[k]);
                     float2 out, vn;
                     bool fin_x;   // out is this line's final x
                     if (fwd) {
@@ -400,11 +557,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                     const bool valid = row < n && r < Rn;
                     if (valid) P[((long)line * Rn + r) * n + row] = fin_x ? tc_adj_out<ADJ>(a, line, row, out) : out;
                     if (row < npad) vst[(size_t)r * vld + row] = valid ? vn : make_float2(0.f, 0.f);
+                    if (valid) am[k] = fmaxf(am[k], fmaxf(fabsf(vn.x), fabsf(vn.y)));
                 }
             }
             tc_fence_before();
             if (t + 1 < nsteps) {
+                put_vmax(am);
                 tc_epilogue_barrier();
+                if constexpr (F16) {
+#pragma unroll
+                    for (int k = 0; k < RH; k++) sv_cur[k] = v_scale(wg * RH + k);
+                }
                 build_b();
             }
 #pragma unroll
@@ -422,23 +585,55 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
 }
 
 // ------------------------------------------------------------------- host
+// Power-of-two scale of every block G_j (kz, line) for the FP16 products:
+// its largest |re| or |im| scaled into [2^13, 2^14).
+__global__ void __launch_bounds__(256) gscale_kernel(const float2 *Gt, int n, int ldg, float *gscale) {
+    __shared__ float wmax[8];
+    const float2 *g = Gt + (long)blockIdx.x * n * ldg;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float mx = 0.f;
+    for (int m = warp; m < n; m += 8)
+        for (int i = lane; i < n; i += 32) {
+            const float2 v = g[(long)m * ldg + i];
+            mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
+        }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if (lane == 0) wmax[warp] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; w++) mx = fmaxf(mx, wmax[w]);
+        gscale[blockIdx.x] = pow2_scale_13(mx);
+    }
+}
+
+int launch_gscale(const void *Gt, int n, int ny, int nz, int ldg, float *gscale, cudaStream_t s) {
+    gscale_kernel<<<dim3((unsigned)(ny * nz)), 256, 0, s>>>((const float2 *)Gt, n, ldg, gscale);
+    return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
+}
+
 // The launch shape of a batch: RR right-hand sides (8 or 16), chunk rows MC,
-// row blocks MB, ring depth and shared memory; false when it does not fit.
+// row blocks MB, FP16 or TF32 products, ring depth and shared memory; false
+// when it does not fit.
 struct TcShape {
     int RR, MC, MB, npad, nstage;
+    bool f16;
     uint32_t stage_bytes;
     size_t smem;
 };
 
 static bool tc_shape(const SweepArgs &sa, int mc, TcShape &sh) {
     if (sa.n < 1 || sa.n > kTcMaxN || sa.R < 1 || sa.R > 16) return false;
+    sh.f16 = sa.tc_f16 != 0;
+    if (sh.f16 && !sa.gscale) return false;
     sh.RR = sa.R <= 8 ? 8 : 16;
     sh.MB = sa.n > 128 ? 2 : 1;
-    sh.MC = (sh.MB == 2 || mc == 16) ? 16 : 32;   // two row blocks: 16-row chunks (TMEM)
+    // FP16 products: 32-row chunks; TF32: as asked, 16-row chunks with two row blocks (TMEM)
+    sh.MC = sh.f16 ? 32 : ((sh.MB == 2 || mc == 16) ? 16 : 32);
     sh.npad = ((sa.n + sh.MC - 1) / sh.MC) * sh.MC;
     sh.stage_bytes = (uint32_t)((((size_t)sh.MC * sa.ldg * 8) + 127) & ~(size_t)127);
     const size_t bbytes = 2 * sizeof(float) * (size_t)(2 * sh.RR) * (2 * sh.npad);
-    const size_t vbytes = sizeof(float2) * (size_t)sh.RR * (sh.npad + 2);
+    const size_t vbytes = sizeof(float2) * (size_t)sh.RR * (sh.npad + 2) + sizeof(float) * 4 * sh.RR;
     const size_t fixed = bbytes + vbytes + sizeof(uint64_t) * (2 * kTcBuf + 3) + 16;
     const size_t optin = device_info().smem_optin;
     const size_t per_stage = sh.stage_bytes + 2 * sizeof(uint64_t);
@@ -458,13 +653,14 @@ bool sweep_tc_supported(const SweepArgs &sa) {
     return tc_shape(sa, sa.tc_mc, sh);
 }
 
-template <int RR, int MC, int MB, bool ADJ> static int sweep_tc_impl(const SweepArgs &sa, const TcShape &sh,
-                                                                     cudaStream_t st) {
+template <int RR, int MC, int MB, bool ADJ, bool F16>
+static int sweep_tc_impl(const SweepArgs &sa, const TcShape &sh, cudaStream_t st) {
     SweepTcK k;
     k.n = sa.n;
     k.ny = sa.ny;
     k.ldg = sa.ldg;
     k.nrhs = sa.R;
+    k.gscale = sa.gscale;
     k.npad = sh.npad;
     k.cpl = sh.npad / MC;
     k.Gt = (const float2 *)sa.Gt;
@@ -475,7 +671,7 @@ template <int RR, int MC, int MB, bool ADJ> static int sweep_tc_impl(const Sweep
     k.status = sa.status;
     k.stage_bytes = sh.stage_bytes;
     k.nstage = sh.nstage;
-    auto kern = sweep_tc_kernel<RR, MC, MB, ADJ>;
+    auto kern = sweep_tc_kernel<RR, MC, MB, ADJ, F16>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem) != cudaSuccess)
         return HELM3D_ERR_CUDA;
     kern<<<dim3((unsigned)sa.nz), kTcThreads, sh.smem, st>>>(k);
@@ -483,16 +679,24 @@ template <int RR, int MC, int MB, bool ADJ> static int sweep_tc_impl(const Sweep
 }
 
 template <bool ADJ> static int sweep_tc_adj(const SweepArgs &sa, const TcShape &sh, cudaStream_t s) {
+    if (sh.f16) {
+        if (sh.MB == 2) {
+            if (sh.RR == 8) return sweep_tc_impl<8, 32, 2, ADJ, true>(sa, sh, s);
+            return sweep_tc_impl<16, 32, 2, ADJ, true>(sa, sh, s);
+        }
+        if (sh.RR == 8) return sweep_tc_impl<8, 32, 1, ADJ, true>(sa, sh, s);
+        return sweep_tc_impl<16, 32, 1, ADJ, true>(sa, sh, s);
+    }
     if (sh.MB == 2) {
-        if (sh.RR == 8) return sweep_tc_impl<8, 16, 2, ADJ>(sa, sh, s);
-        return sweep_tc_impl<16, 16, 2, ADJ>(sa, sh, s);
+        if (sh.RR == 8) return sweep_tc_impl<8, 16, 2, ADJ, false>(sa, sh, s);
+        return sweep_tc_impl<16, 16, 2, ADJ, false>(sa, sh, s);
     }
     if (sh.MC == 16) {
-        if (sh.RR == 8) return sweep_tc_impl<8, 16, 1, ADJ>(sa, sh, s);
-        return sweep_tc_impl<16, 16, 1, ADJ>(sa, sh, s);
+        if (sh.RR == 8) return sweep_tc_impl<8, 16, 1, ADJ, false>(sa, sh, s);
+        return sweep_tc_impl<16, 16, 1, ADJ, false>(sa, sh, s);
     }
-    if (sh.RR == 8) return sweep_tc_impl<8, 32, 1, ADJ>(sa, sh, s);
-    return sweep_tc_impl<16, 32, 1, ADJ>(sa, sh, s);
+    if (sh.RR == 8) return sweep_tc_impl<8, 32, 1, ADJ, false>(sa, sh, s);
+    return sweep_tc_impl<16, 32, 1, ADJ, false>(sa, sh, s);
 }
 
 int launch_sweep_tc(const SweepArgs &sa, int mc, cudaStream_t s) {
