@@ -103,3 +103,17 @@ __device__ __forceinline__ bool mbar_wait_bounded_cta(uint32_t addr, uint32_t pa
         if (mbar_try_wait_cta(addr, parity)) return true;
     return false;
 }
+
+// A position in a ring of `size` slots: the slot, and the parity of the
+// current pass over the ring (the phase an mbarrier of the slot completes
+// on this use).  Advanced by one per use, without divisions.
+struct RingPos {
+    int slot = 0;
+    uint32_t phase = 0;
+    __device__ __forceinline__ void next(int size) {
+        if (++slot == size) {
+            slot = 0;
+            phase ^= 1u;
+        }
+    }
+};

@@ -117,20 +117,6 @@ __device__ __forceinline__ float pow2_inv(float s) {
     return __uint_as_float((254u - ((__float_as_uint(s) >> 23) & 0xffu)) << 23);
 }
 
-// A position in a ring of `size` slots: the slot, and the parity of the
-// current pass over the ring (the phase an mbarrier of the slot completes
-// on this use).  Advanced by one per use, without divisions.
-struct RingPos {
-    int slot = 0;
-    uint32_t phase = 0;
-    __device__ __forceinline__ void next(int size) {
-        if (++slot == size) {
-            slot = 0;
-            phase ^= 1u;
-        }
-    }
-};
-
 // MB row blocks of 128 rows i (n <= 128 MB).  TMEM: the accumulator of row
 // block rb at columns [2 NR rb, 2 NR (rb + 1)); chunk buffer b at 128 + b BW,
 // row block rb's hi at + 2 KC rb, its lo KC further (3 buffers fit for
@@ -522,6 +508,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             for (int k = 0; k < RH; k++) am[k] = 0.f;
             wait(d_full, (uint32_t)(t & 1));
             tc_fence_after();
+            // this line's y / x, stored to the planes after the next B is
+            // handed over (the stores are off the line-to-line chain)
+            float2 outs[MB][RH];
 #pragma unroll
             for (int rb = 0; rb < MB; rb++) {
                 const int row = i + 128 * rb;
@@ -555,7 +544,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                         vn = out;
                     }
                     const bool valid = row < n && r < Rn;
-                    if (valid) P[((long)line * Rn + r) * n + row] = fin_x ? tc_adj_out<ADJ>(a, line, row, out) : out;
+                    outs[rb][k] = fin_x ? tc_adj_out<ADJ>(a, line, row, out) : out;
                     if (row < npad) vst[(size_t)r * vld + row] = valid ? vn : make_float2(0.f, 0.f);
                     if (valid) am[k] = fmaxf(am[k], fmaxf(fabsf(vn.x), fabsf(vn.y)));
                 }
@@ -569,6 +558,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                     for (int k = 0; k < RH; k++) sv_cur[k] = v_scale(wg * RH + k);
                 }
                 build_b();
+            }
+#pragma unroll
+            for (int rb = 0; rb < MB; rb++) {
+                const int row = i + 128 * rb;
+#pragma unroll
+                for (int k = 0; k < RH; k++) {
+                    const int r = wg * RH + k;
+                    if (row < n && r < Rn) P[((long)line * Rn + r) * n + row] = outs[rb][k];
+                }
             }
 #pragma unroll
             for (int rb = 0; rb < MB; rb++) {

@@ -12,22 +12,31 @@
 // B[2k+1][2j+1] = Re M.  M = 128 rows (tile positions), N = 2 nz (padded to 16,
 // split in two MMAs above 256), K = 2 nz padded to the chunk.
 //
-// Per CTA (persistent over tiles, 256 threads, one CTA per SM):
-//   * B streams chunk by chunk (KC real K per chunk, hi and lo halves already
-//     in the tensor-core layout in global memory, prepared once per grid) by a
-//     1D bulk copy into a two-stage shared-memory ring;
-//   * all threads convert the A chunk (FP64 or FP32 input -> tf32 hi/lo) into
-//     the other half of the stage, one 16-byte store per (position, pair of j);
-//   * thread 0 issues the 3 x (KC / 8) MMAs of the chunk into the TMEM
-//     accumulator (128 lanes x N fp32 columns) and commits them to the stage's
-//     mbarrier, which gates the refill of that stage two chunks later;
-//   * after the last chunk every warp reads its 32 TMEM lanes (tcgen05.ld
-//     32x32b) and writes the outputs of its positions.
+// One persistent CTA per SM walks its tiles chunk by chunk (KC real K per
+// chunk) through a ring of S shared-memory stages, each holding the A chunk
+// (hi, lo) and the B chunk (hi, lo), with warp-specialized roles:
+//   * warps 0-7 (converters): thread (p, half) loads its position's inputs
+//     kZcDepth chunks ahead into registers (the loads stay in flight), splits
+//     them into tf32 hi/lo and stores them into the stage (one 16-byte store
+//     per pair of j), then arrives on the stage's a_full barrier;
+//   * warp 12 (producer): one bulk copy per chunk of B (hi and lo, already in
+//     the tensor-core layout in global memory, prepared once per grid; the
+//     same for every tile, so it comes from L2);
+//   * warp 13 (MMA): 3 x (KC / 8) MMAs per chunk into the tile's TMEM
+//     accumulator, committed to the stage's empty barrier (which gates its
+//     refill); after the tile's last chunk a commit to the accumulator's
+//     full barrier;
+//   * warps 8-11 (epilogue): warp w reads TMEM lanes 32 (w % 4) + [0, 32)
+//     (tcgen05.ld 32x32b) and writes the outputs of those positions, then
+//     frees the accumulator.
+// Two accumulators (2 N <= 512 TMEM columns, nz <= 128) let the epilogue of
+// one tile run under the MMAs of the next; above that one accumulator.
 // Shared-memory operands use the no-swizzle K-major canonical layout: 8 rows x
 // 16 bytes per core matrix, K-adjacent core matrices LBO = 128 bytes apart,
 // 8-row groups SBO = KC/4 * 128 bytes apart.  Every wait is bounded; on
-// expiry the kernel sets bit 2 of *status, stops issuing work, waits (bounded)
-// for its own MMAs, frees its TMEM and returns.
+// expiry the kernel sets bit 2 of *status, every role stops issuing work,
+// the producer waits (bounded) for its copies in flight and the MMA warp for
+// its MMAs, TMEM is freed and the kernel returns.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -41,8 +50,15 @@
 
 namespace h3d {
 
-constexpr int kZcThreads = 256;
-constexpr int kZcM = 128;                  // tile positions (MMA M)
+constexpr int kZcM = 128;                    // tile positions (MMA M)
+constexpr int kZcConvWarps = 8;              // warps 0-7
+constexpr int kZcEpiWarps = 4;               // warps 8-11
+constexpr int kZcProducerWarp = 12;
+constexpr int kZcMmaWarp = 13;
+constexpr int kZcThreads = 14 * 32;
+constexpr int kZcDepth = 4;                  // input chunks in flight per converter thread
+constexpr int kZcMaxStages = 8;
+constexpr uint32_t kZcStageBudget = 200u * 1024u;
 constexpr uint32_t kZcWaitLimit = 1u << 22;
 
 // -------------------------------------------------------------- the kernel
@@ -50,6 +66,8 @@ struct ZtcArgs {
     int nz, nzq;            // nz and nz padded to 8 (output rows)
     int N, K, KC;           // GEMM N = 2 nzq, K = 2 nz padded to KC, chunk
     int nchunks;
+    int nstage;             // shared-memory stages
+    int nacc;               // TMEM accumulators (1 or 2)
     long plane;             // nx*ny
     PlaneLayout L;
     VecBatch vec;           // forward: input x; inverse: output y
@@ -58,7 +76,6 @@ struct ZtcArgs {
     void *planes;           // complex64 planes
     const float *B;         // [nchunks][2 (hi, lo)][N rows x KC] in canonical layout
     int ntiles, tiles_per_rhs;
-    uint32_t tmem_cols;
     int *status;
 };
 
@@ -95,57 +112,77 @@ __device__ __forceinline__ ZtcSrc ztc_src(const ZtcArgs &a, int tile, int p) {
     return q;
 }
 
-// the 2 JP complex values (j = j0 + 2 jp + {0, 1}, jp = half, half + 2, ...)
-// one thread converts for one chunk, as 4 JP doubles
+template <bool FWD> struct ZtcIn;
+template <> struct ZtcIn<true> { typedef double2 T; };
+template <> struct ZtcIn<false> { typedef float2 T; };
+
+// the 2 JP complex inputs (j = j0 + 2 jp + {0, 1}, jp = half, half + 2, ...)
+// of one thread for one chunk; zeros outside the grid
 template <bool FWD, int JP>
-__device__ __forceinline__ void ztc_load(const ZtcArgs &a, const ZtcSrc &q, int j0, int half, double (&v)[4 * JP]) {
+__device__ __forceinline__ void ztc_load(const ZtcArgs &a, const ZtcSrc &q, int j0, int half,
+                                         typename ZtcIn<FWD>::T (&v)[2 * JP]) {
+    typedef typename ZtcIn<FWD>::T In;
 #pragma unroll
     for (int t = 0; t < JP; t++) {
-        const int jp = half + 2 * t;
 #pragma unroll
         for (int e = 0; e < 2; e++) {
-            const int jj = j0 + 2 * jp + e;
-            double re = 0.0, im = 0.0;
-            if (q.valid && jj < a.nz) {
-                if (FWD) {
-                    const double2 x = __ldg(reinterpret_cast<const double2 *>(q.base) + (long)jj * q.step);
-                    re = q.s * x.x;
-                    im = q.s * x.y;
-                } else {
-                    const float2 x = __ldg(reinterpret_cast<const float2 *>(q.base) + (long)jj * q.step);
-                    re = x.x;
-                    im = x.y;
-                }
-            }
-            v[4 * t + 2 * e] = re;
-            v[4 * t + 2 * e + 1] = im;
+            const int jj = j0 + 2 * (half + 2 * t) + e;
+            In x;
+            x.x = 0;
+            x.y = 0;
+            if (q.valid && jj < a.nz) x = __ldg(reinterpret_cast<const In *>(q.base) + (long)jj * q.step);
+            v[2 * t + e] = x;
         }
     }
 }
 
+// The (tile, chunk) cursor of one CTA's sequence, with the thread's source.
+template <bool FWD> struct ZtcCursor {
+    int tile, c;
+    ZtcSrc src;
+    __device__ __forceinline__ void start(const ZtcArgs &a, int p) {
+        tile = blockIdx.x;
+        c = 0;
+        src = ztc_src<FWD>(a, tile, p);
+    }
+    __device__ __forceinline__ void next(const ZtcArgs &a, int p) {
+        if (++c == a.nchunks) {
+            c = 0;
+            tile += gridDim.x;
+            if (tile < a.ntiles) src = ztc_src<FWD>(a, tile, p);
+        }
+    }
+};
+
 template <bool FWD, int KC>
 __global__ void __launch_bounds__(kZcThreads, 1) ztc_kernel(ZtcArgs a) {
-    constexpr int JP = KC / 8;   // 16-byte A stores per thread per chunk
+    constexpr int JP = KC / 8;   // 16-byte A stores (pairs of j) per converter thread per chunk
+    typedef typename ZtcIn<FWD>::T In;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    const int N = a.N;
-    const uint32_t bbytes = 2u * (uint32_t)N * KC * 4u;         // hi + lo
-    const uint32_t abytes = (uint32_t)kZcM * KC * 4u;           // one of hi / lo
-    const uint32_t stage_bytes = bbytes + 2u * abytes;
-    unsigned char *stage0 = smem_raw;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + 2 * stage_bytes);   // b_bar[2], mma_bar[2]
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 4);
+    const int N = a.N, S = a.nstage, nch = a.nchunks;
+    const uint32_t abytes = (uint32_t)kZcM * KC * 4u;         // one of hi / lo
+    const uint32_t bbytes = 2u * (uint32_t)N * KC * 4u;       // hi + lo
+    const uint32_t stage_bytes = 2u * abytes + bbytes;
+    uint64_t *a_full = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S * stage_bytes);
+    uint64_t *b_full = a_full + kZcMaxStages;
+    uint64_t *empty = b_full + kZcMaxStages;
+    uint64_t *acc_full = empty + kZcMaxStages;
+    uint64_t *acc_empty = acc_full + 2;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(acc_empty + 2);
     volatile int *s_dead = reinterpret_cast<volatile int *>(tslot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    uint64_t *b_bar = bars, *mma_bar = bars + 2;
 
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                     "r"(a.tmem_cols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
+    if (warp == 0) tmem_alloc(tslot, 512);
     if (tid == 0) {
-        for (int q = 0; q < 4; q++) mbar_init(&bars[q], 1);
+        for (int q = 0; q < S; q++) {
+            mbar_init(&a_full[q], kZcConvWarps);
+            mbar_init(&b_full[q], 1);
+            mbar_init(&empty[q], 1);
+        }
+        for (int q = 0; q < 2; q++) {
+            mbar_init(&acc_full[q], 1);
+            mbar_init(&acc_empty[q], kZcEpiWarps);
+        }
         fence_mbar_init_cluster();
         *s_dead = 0;
     }
@@ -154,155 +191,203 @@ __global__ void __launch_bounds__(kZcThreads, 1) ztc_kernel(ZtcArgs a) {
     tc_fence_after();
     const uint32_t tmem = *tslot;
 
-    // `dead` is read from shared memory right after a barrier, so every
-    // thread takes the same branches; a thread whose bounded wait expires
-    // sets it (and bit 2 of *status) for the next barrier to publish.
-    auto fail = [&]() {
-        *s_dead = 1;
-        atomicOr(a.status, 4);
-    };
-    const int p = tid & (kZcM - 1), half = tid >> 7;
-    const int nch = a.nchunks;
     const int my_tiles = blockIdx.x < a.ntiles ? (a.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     const long total = (long)my_tiles * nch;
-    int dead = 0;
-    long last_commit = -1;   // chunk of thread 0's last commit
-    // the (tile, chunk) sequence of this CTA; the inputs of chunk g + 1 are
-    // loaded into the other register buffer while chunk g is converted and
-    // multiplied (two buffers, no copy, so the loads stay in flight)
-    double bufA[4 * JP], bufB[4 * JP];
-    ZtcSrc src_nxt = ztc_src<FWD>(a, blockIdx.x, p);
-    if (total > 0) ztc_load<FWD, JP>(a, src_nxt, 0, half, bufA);
-    // one chunk; returns false to leave the loop (dead)
-    auto chunk = [&](long g, double (&cur)[4 * JP], double (&nxt)[4 * JP]) -> bool {
-        const int tile = blockIdx.x + (int)(g / nch) * gridDim.x;
-        const int c = (int)(g % nch);
-        if (g + 1 < total) {
-            const int c1 = (int)((g + 1) % nch);
-            if (c1 == 0) src_nxt = ztc_src<FWD>(a, tile + gridDim.x, p);
-            ztc_load<FWD, JP>(a, src_nxt, c1 * (KC / 2), half, nxt);
-        }
-        const int st = (int)(g & 1);
-        unsigned char *sbase = stage0 + st * stage_bytes;
-        float *Bs = reinterpret_cast<float *>(sbase);
-        unsigned char *Ahi = sbase + bbytes, *Alo = Ahi + abytes;
-        // the MMAs that read this stage two chunks ago must be complete
-        if (g >= 2 && !dead &&
-            !mbar_wait_bounded_cta(smem_u32(&mma_bar[st]), (uint32_t)(((g - 2) >> 1) & 1), kZcWaitLimit))
-            fail();
-        if (tid == 0 && !dead && !*s_dead) {
-            mbar_expect_tx(&b_bar[st], bbytes);
-            bulk_g2s(Bs, a.B + (size_t)c * (bbytes / 4), bbytes, &b_bar[st]);
-        }
+    bool dead = false;
+    auto fail = [&]() {
+        if (!dead) atomicOr(a.status, 4);
+        dead = true;
+        *s_dead = 1;
+    };
+    auto wait = [&](uint64_t *bar, uint32_t parity) {
+        if (!dead && !mbar_wait_bounded_cta(smem_u32(bar), parity, kZcWaitLimit)) fail();
+    };
+    auto stage = [&](int s) { return smem_raw + (size_t)s * stage_bytes; };
+
+    if (warp < kZcConvWarps) {
+        // ------------------------------------------------------ converters
+        const int p = tid & (kZcM - 1), half = tid >> 7;
+        In buf[kZcDepth][2 * JP];
+        double bs[kZcDepth];
+        ZtcCursor<FWD> lc;   // loads: kZcDepth chunks ahead of the conversions
+        lc.start(a, p);
 #pragma unroll
-        for (int t = 0; t < JP; t++) {
-            const int jp = half + 2 * t;
-            float4 hi, lo;
-            tf32_split(cur[4 * t + 0], hi.x, lo.x);
-            tf32_split(cur[4 * t + 1], hi.y, lo.y);
-            tf32_split(cur[4 * t + 2], hi.z, lo.z);
-            tf32_split(cur[4 * t + 3], hi.w, lo.w);
-            const uint32_t off = canon_off(p, 4 * jp, KC);
-            *reinterpret_cast<float4 *>(Ahi + off) = hi;
-            *reinterpret_cast<float4 *>(Alo + off) = lo;
+        for (int d = 0; d < kZcDepth; d++) {
+            if (d < total) {
+                ztc_load<FWD, JP>(a, lc.src, lc.c * (KC / 2), half, buf[d]);
+                bs[d] = lc.src.s;
+                lc.next(a, p);
+            }
         }
-        fence_proxy_async_smem();
-        __syncthreads();
-        dead = *s_dead;
-        if (tid == 0 && !dead) {
-            if (!mbar_wait_bounded_cta(smem_u32(&b_bar[st]), (uint32_t)((g >> 1) & 1), kZcWaitLimit)) {
-                fail();
-            } else {
-                tc_fence_after();
-                const uint32_t sbo = (uint32_t)(KC / 4) * 128u;
-                const uint32_t bs = smem_u32(Bs), ah = smem_u32(Ahi), al = smem_u32(Alo);
-                const uint32_t blo = bs + bbytes / 2;
-                for (int part = 0; part * 256 < N; part++) {
-                    const int n_part = N - part * 256 < 256 ? N - part * 256 : 256;
-                    const uint32_t idesc = umma_idesc_tf32(n_part, kZcM);
-                    const uint32_t brow = (uint32_t)(part * 256 / 8) * sbo;   // row offset of this part
-                    const uint32_t td = tmem + (uint32_t)(part * 256);
+        RingPos sp;
+        for (long g0 = 0; g0 < total && !dead; g0 += kZcDepth) {
 #pragma unroll
-                    for (int ks = 0; ks < KC / 8; ks++) {
-                        const uint32_t koff = (uint32_t)ks * 256u;           // 2 core matrices of 128 B
-                        const uint32_t acc0 = (c > 0 || ks > 0) ? 1u : 0u;
-                        umma_tf32(td, umma_desc(al + koff, 128, sbo), umma_desc(bs + brow + koff, 128, sbo), idesc,
-                                  acc0);
-                        umma_tf32(td, umma_desc(ah + koff, 128, sbo), umma_desc(blo + brow + koff, 128, sbo), idesc,
-                                  1u);
-                        umma_tf32(td, umma_desc(ah + koff, 128, sbo), umma_desc(bs + brow + koff, 128, sbo), idesc,
-                                  1u);
+            for (int d = 0; d < kZcDepth; d++) {
+                const long g = g0 + d;
+                if (g < total && !dead) {
+                    wait(&empty[sp.slot], sp.phase ^ 1u);   // the MMAs that read the stage last are done
+                    // warp-uniform from here (the stores end in a __syncwarp)
+                    if (__any_sync(0xffffffffu, dead || *s_dead)) dead = true;
+                    if (!dead) {
+                        unsigned char *Ahi = stage(sp.slot), *Alo = Ahi + abytes;
+#pragma unroll
+                        for (int t = 0; t < JP; t++) {
+                            const In x0 = buf[d][2 * t], x1 = buf[d][2 * t + 1];
+                            const double s = bs[d];
+                            float4 hi, lo;
+                            tf32_split(s * (double)x0.x, hi.x, lo.x);
+                            tf32_split(s * (double)x0.y, hi.y, lo.y);
+                            tf32_split(s * (double)x1.x, hi.z, lo.z);
+                            tf32_split(s * (double)x1.y, hi.w, lo.w);
+                            const uint32_t off = canon_off(p, 4 * (half + 2 * t), KC);
+                            *reinterpret_cast<float4 *>(Ahi + off) = hi;
+                            *reinterpret_cast<float4 *>(Alo + off) = lo;
+                        }
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive_local(&a_full[sp.slot]);
+                    }
+                    sp.next(S);
+                    if (g + kZcDepth < total) {
+                        ztc_load<FWD, JP>(a, lc.src, lc.c * (KC / 2), half, buf[d]);
+                        bs[d] = lc.src.s;
+                        lc.next(a, p);
                     }
                 }
-                umma_commit(&mma_bar[st]);
-                last_commit = g;
             }
         }
-        if (c != nch - 1) return true;
-
-        // epilogue of the tile: wait for its last MMAs, read 32 lanes per warp
-        if (!dead && !mbar_wait_bounded_cta(smem_u32(&mma_bar[st]), (uint32_t)((g >> 1) & 1), kZcWaitLimit))
-            fail();
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        dead = *s_dead;
-        if (dead) return false;
-        const int r = tile / a.tiles_per_rhs;
-        const int q = warp & 3, colhalf = warp >> 2;
-        const long we = (long)(tile - r * a.tiles_per_rhs) * kZcM + 32 * q + lane;   // TMEM lane = position
-        const bool ve = we < a.plane;
-        long oidx0 = 0, ostep = 0;
-        if (ve) {
-            if (FWD) {
-                oidx0 = zc_plane_index(a.L, r, 0, we);
-                ostep = a.L.plane * a.L.R;
-            } else {
-                oidx0 = we;
-                ostep = a.plane;
+    } else if (warp == kZcProducerWarp) {
+        // -------------------------------------------------------- producer
+        if (lane == 0) {
+            RingPos sp;
+            int c = 0;
+            long issued = 0;
+            for (long g = 0; g < total && !dead; g++) {
+                wait(&empty[sp.slot], sp.phase ^ 1u);
+                if (*s_dead) dead = true;
+                if (dead) break;
+                unsigned char *Bs = stage(sp.slot) + 2u * abytes;
+                mbar_expect_tx(&b_full[sp.slot], bbytes);
+                bulk_g2s(Bs, a.B + (size_t)c * (bbytes / 4), bbytes, &b_full[sp.slot]);
+                issued++;
+                sp.next(S);
+                if (++c == nch) c = 0;
+            }
+            // the copies still in flight land before the CTA exits: the last
+            // use of every slot (sp is one past the final use)
+            for (int k = 0; k < S && k < issued; k++) {
+                int sl = sp.slot - 1 - k;
+                uint32_t ph = sp.phase;
+                if (sl < 0) {
+                    sl += S;
+                    ph ^= 1u;
+                }
+                mbar_wait_bounded_cta(smem_u32(&b_full[sl]), ph, kZcWaitLimit);
             }
         }
-        const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
-        for (int cc = 2 * colhalf; cc < N / 16; cc += 4) {
-            // two 16-column loads in flight, one wait
-            float v[32];
-            tmem_ld16_nowait(trow + (uint32_t)(cc * 16), v);
-            const bool two = cc + 1 < N / 16;
-            if (two) tmem_ld16_nowait(trow + (uint32_t)((cc + 1) * 16), v + 16);
-            tmem_wait_ld(v);
-            if (!ve) continue;
+    } else if (warp == kZcMmaWarp) {
+        // ------------------------------------------------------------- MMA
+        if (lane == 0) {
+            RingPos sp, ap;
+            const uint32_t sbo = (uint32_t)(KC / 4) * 128u;
+            bool any = false;
+            RingPos last;   // accumulator of the last tile committed
+            for (int i = 0; i < my_tiles && !dead; i++) {
+                wait(&acc_empty[ap.slot], ap.phase ^ 1u);   // its previous tile's outputs are read
+                tc_fence_after();
+                const uint32_t tacc = tmem + (uint32_t)(ap.slot * N);
+                for (int c = 0; c < nch && !dead; c++) {
+                    wait(&a_full[sp.slot], sp.phase);
+                    wait(&b_full[sp.slot], sp.phase);
+                    if (*s_dead) dead = true;
+                    if (dead) break;
+                    tc_fence_after();
+                    const uint32_t ah = smem_u32(stage(sp.slot)), al = ah + abytes;
+                    const uint32_t bh = ah + 2u * abytes, bl = bh + bbytes / 2;
+                    for (int part = 0; part * 256 < N; part++) {
+                        const int n_part = N - part * 256 < 256 ? N - part * 256 : 256;
+                        const uint32_t idesc = umma_idesc_tf32(n_part, kZcM);
+                        const uint32_t brow = (uint32_t)(part * 256 / 8) * sbo;   // row offset of this part
+                        const uint32_t td = tacc + (uint32_t)(part * 256);
 #pragma unroll
-            for (int t = 0; t < 16; t++) {
-                const int k = cc * 8 + t;
-                if (k >= a.nz || (t >= 8 && !two)) break;
+                        for (int ks = 0; ks < KC / 8; ks++) {
+                            const uint32_t koff = (uint32_t)ks * 256u;   // 2 core matrices of 128 B
+                            const uint32_t acc0 = (c > 0 || ks > 0) ? 1u : 0u;
+                            umma_tf32(td, umma_desc(al + koff, 128, sbo), umma_desc(bh + brow + koff, 128, sbo),
+                                      idesc, acc0);
+                            umma_tf32(td, umma_desc(ah + koff, 128, sbo), umma_desc(bl + brow + koff, 128, sbo),
+                                      idesc, 1u);
+                            umma_tf32(td, umma_desc(ah + koff, 128, sbo), umma_desc(bh + brow + koff, 128, sbo),
+                                      idesc, 1u);
+                        }
+                    }
+                    umma_commit(&empty[sp.slot]);
+                    sp.next(S);
+                }
+                if (dead) break;
+                umma_commit(&acc_full[ap.slot]);
+                any = true;
+                last = ap;
+                ap.next(a.nacc);
+            }
+            // every MMA issued has completed before TMEM is freed
+            if (any) mbar_wait_bounded_cta(smem_u32(&acc_full[last.slot]), last.phase, kZcWaitLimit);
+        }
+    } else {
+        // -------------------------------------------------------- epilogue
+        const int q = warp & 3;   // TMEM lanes 32 q + [0, 32) (a warp reads its own quarter)
+        const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
+        RingPos ap;
+        for (int i = 0; i < my_tiles && !dead; i++) {
+            const int tile = blockIdx.x + i * gridDim.x;
+            wait(&acc_full[ap.slot], ap.phase);
+            // warp-uniform from here (tcgen05.ld is warp-collective)
+            if (__any_sync(0xffffffffu, dead || *s_dead)) dead = true;
+            if (dead) break;
+            tc_fence_after();
+            const int r = tile / a.tiles_per_rhs;
+            const long we = (long)(tile - r * a.tiles_per_rhs) * kZcM + 32 * q + lane;   // TMEM lane = position
+            const bool ve = we < a.plane;
+            long oidx0 = 0, ostep = 0;
+            if (ve) {
                 if (FWD) {
-                    reinterpret_cast<float2 *>(a.planes)[oidx0 + (long)k * ostep] = make_float2(v[2 * t], v[2 * t + 1]);
+                    oidx0 = zc_plane_index(a.L, r, 0, we);
+                    ostep = a.L.plane * a.L.R;
                 } else {
-                    double2 *yo = a.vec.p + r * a.vec.stride;
-                    yo[oidx0 + (long)k * ostep] = make_double2((double)v[2 * t], (double)v[2 * t + 1]);
+                    oidx0 = r * a.vec.stride + we;
+                    ostep = a.plane;
                 }
             }
+            const uint32_t tacc = trow + (uint32_t)(ap.slot * N);
+            for (int cc = 0; cc < N / 16; cc += 2) {
+                // two 16-column loads in flight, one wait
+                float v[32];
+                tmem_ld16_nowait(tacc + (uint32_t)(cc * 16), v);
+                const bool two = cc + 1 < N / 16;
+                if (two) tmem_ld16_nowait(tacc + (uint32_t)((cc + 1) * 16), v + 16);
+                tmem_wait_ld(v);
+                if (!ve) continue;
+#pragma unroll
+                for (int t = 0; t < 16; t++) {
+                    const int k = cc * 8 + t;
+                    if (k >= a.nz || (t >= 8 && !two)) break;
+                    if (FWD) {
+                        reinterpret_cast<float2 *>(a.planes)[oidx0 + (long)k * ostep] = make_float2(v[2 * t], v[2 * t + 1]);
+                    } else {
+                        a.vec.p[oidx0 + (long)k * ostep] = make_double2((double)v[2 * t], (double)v[2 * t + 1]);
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_local(&acc_empty[ap.slot]);
+            ap.next(a.nacc);
         }
-        // the next tile's first MMA overwrites the accumulator
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        return true;
-    };
-    for (long g = 0; g < total; g += 2) {
-        if (!chunk(g, bufA, bufB)) break;
-        if (g + 1 < total && !chunk(g + 1, bufB, bufA)) break;
     }
-    // free the accumulator once every MMA this CTA issued has completed
-    if (tid == 0 && last_commit >= 0)
-        mbar_wait_bounded_cta(smem_u32(&mma_bar[last_commit & 1]), (uint32_t)((last_commit >> 1) & 1),
-                              kZcWaitLimit);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols)
-                     : "memory");
+    if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
 // ------------------------------------------------------------------- host
@@ -312,7 +397,7 @@ static bool ztc_shape(int nz, int &N, int &K, int &KC) {
     const int nzq = (nz + 7) & ~7;
     N = 2 * nzq;
     if (N > 512) return false;
-    KC = N <= 256 ? 32 : 16;
+    KC = N <= 256 ? 16 : 8;
     K = ((2 * nz + KC - 1) / KC) * KC;
     return true;
 }
@@ -375,12 +460,16 @@ static int ztc_launch(const PlaneLayout &L, const VecBatch &vec, double scale, c
     a.B = B;
     a.tiles_per_rhs = (int)((L.plane + kZcM - 1) / kZcM);
     a.ntiles = a.tiles_per_rhs * L.R;
-    a.tmem_cols = a.N <= 256 ? 256u : 512u;
+    a.nacc = 2 * a.N <= 512 ? 2 : 1;
     a.status = status;
     const size_t stage = (size_t)2 * a.N * a.KC * 4 + (size_t)2 * kZcM * a.KC * 4;
-    const size_t smem = 2 * stage + 4 * sizeof(uint64_t) + 16;   // stages, barriers, TMEM slot, flag
+    a.nstage = (int)(kZcStageBudget / stage);
+    if (a.nstage > kZcMaxStages) a.nstage = kZcMaxStages;
+    if (a.nstage < 2) return HELM3D_ERR_ARG;
+    // stages, barriers (3 per stage slot, 2 per accumulator), TMEM slot, flag
+    const size_t smem = (size_t)a.nstage * stage + (3 * kZcMaxStages + 4) * sizeof(uint64_t) + 16;
     if (smem > device_info().smem_optin) return HELM3D_ERR_ARG;
-    auto kern = a.KC == 32 ? ztc_kernel<FWD, 32> : ztc_kernel<FWD, 16>;
+    auto kern = a.KC == 16 ? ztc_kernel<FWD, 16> : ztc_kernel<FWD, 8>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return HELM3D_ERR_CUDA;
     const int grid = a.ntiles < device_info().sm_count ? a.ntiles : device_info().sm_count;
