@@ -396,7 +396,7 @@ static int launch_cfg(const FactorArgs &fa, cudaStream_t st) {
     k.status = fa.status;
     constexpr size_t smem = factor_smem_bytes<R, NP, NP / C>();
     auto kern = factor_kernel<R, NP, NW, CB, C, MB>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (!smem_limit_max(kern, smem))
         return HELM3D_ERR_CUDA;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(fa.nz * C), 1, 1);

@@ -417,8 +417,7 @@ int launch_factor_tc(const FactorArgs &fa, cudaStream_t st) {
     k.base2d = (const float2 *)fa.base2d;
     k.kz2 = (const float2 *)fa.kz2;
     k.status = fa.status;
-    if (cudaFuncSetAttribute(factor_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFtSmemBytes) !=
-        cudaSuccess)
+    if (!smem_limit_max(factor_tc_kernel, kFtSmemBytes))
         return HELM3D_ERR_CUDA;
     factor_tc_kernel<<<dim3((unsigned)fa.nz), kFtThreads, kFtSmemBytes, st>>>(k);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;

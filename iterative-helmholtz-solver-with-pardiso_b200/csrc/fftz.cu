@@ -208,7 +208,7 @@ static int fwd_impl(const VecBatch &x, double scale, const ScaleBatch &sc, void 
                     const FftPlan &plan, const void *tw, cudaStream_t s) {
     size_t smem = (size_t)2 * plan.n * TW * sizeof(cplx<R>);
     auto kern = fftz_forward_kernel<R, TW>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (!smem_limit_max(kern, smem))
         return HELM3D_ERR_CUDA;
     dim3 grid((unsigned)((L.plane + TW - 1) / TW), (unsigned)L.R);
     kern<<<grid, kFftThreads, smem, s>>>(to_k(plan), x, scale, sc, (cplx<R> *)planes, L, (const cplx<R> *)tw);
@@ -221,7 +221,7 @@ static int inv_impl(const void *planes, const PlaneLayout &L, const VecBatch &y,
                     cudaStream_t s) {
     size_t smem = (size_t)2 * plan.n * TW * sizeof(cplx<R>);
     auto kern = fftz_inverse_kernel<R, TW>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (!smem_limit_max(kern, smem))
         return HELM3D_ERR_CUDA;
     dim3 grid((unsigned)((L.plane + TW - 1) / TW), (unsigned)L.R);
     kern<<<grid, kFftThreads, smem, s>>>(to_k(plan), (const cplx<R> *)planes, L, y, (const cplx<R> *)tw, mode, w,

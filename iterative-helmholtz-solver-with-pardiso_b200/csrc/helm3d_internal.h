@@ -249,6 +249,21 @@ int launch_grad_accum(const VecBatch &lam, const VecBatch &u, int R, double w2, 
 
 Dev &device_info();
 
+// Raise a kernel's dynamic shared-memory limit to the device maximum (less
+// its static shared memory) and check that `need` fits.  The limit belongs to
+// the function and is read by every launch, kernel nodes of instantiated
+// CUDA graphs included, so it is only ever raised: lowering it to one
+// launch's size would break a graph captured earlier with a larger size.
+// Each launch still passes its own size (which sets its occupancy).
+template <typename K> inline bool smem_limit_max(K kern, size_t need) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) return false;
+    const size_t cap = device_info().smem_optin - fa.sharedSizeBytes;
+    if (need > cap) return false;
+    if ((size_t)fa.maxDynamicSharedSizeBytes >= cap) return true;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap) == cudaSuccess;
+}
+
 // ------------------------------------------------------------- autotuner
 // The fastest of nvariants launch shapes of a kernel family for a problem
 // shape: launch(v) runs variant v once on the context's stream; the choice is

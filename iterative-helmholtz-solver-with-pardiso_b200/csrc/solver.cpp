@@ -365,6 +365,7 @@ static int check_status(helm3d_ctx *c) {
     RC(cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status"));
     RC(cuda_check(c, cudaStreamSynchronize(c->stream), "status sync"));
     if (st & 6) return set_error(c, HELM3D_ERR_CUDA, "a bounded wait expired in a kernel");
+    if (st & 8) return set_error(c, HELM3D_ERR_CUDA, "an index check failed in a kernel");
     return HELM3D_OK;
 }
 

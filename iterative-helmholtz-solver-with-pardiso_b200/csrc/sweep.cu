@@ -418,7 +418,7 @@ template <int RR, bool ADJ> static int sweep_tiled_rr(const SweepArgs &sa, cudaS
     k.nstage = nst;
     const size_t smem = (size_t)nst * k.stage_bytes + vbytes + rbytes + 2 * nst * sizeof(uint64_t);
     auto pick = [&](auto kern) -> int {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        if (!smem_limit_max(kern, smem))
             return HELM3D_ERR_CUDA;
         kern<<<dim3((unsigned)sa.nz), (kTiledWarps + 1) * 32, smem, st>>>(k);
         return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;
@@ -468,7 +468,7 @@ template <typename R, int G, int RR, bool ADJ> static int sweep_impl(const Sweep
     k.nstage = nst;
     const size_t smem = (size_t)nst * k.stage_bytes + vbytes + 2 * nst * sizeof(uint64_t);
     auto kern = sweep_kernel<R, G, RR, ADJ>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (!smem_limit_max(kern, smem))
         return HELM3D_ERR_CUDA;
     kern<<<dim3((unsigned)sa.nz), (kSweepConsumerWarps + 1) * 32, smem, st>>>(k);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;

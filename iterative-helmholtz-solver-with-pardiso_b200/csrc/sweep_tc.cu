@@ -670,7 +670,7 @@ static int sweep_tc_impl(const SweepArgs &sa, const TcShape &sh, cudaStream_t st
     k.stage_bytes = sh.stage_bytes;
     k.nstage = sh.nstage;
     auto kern = sweep_tc_kernel<RR, MC, MB, ADJ, F16>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem) != cudaSuccess)
+    if (!smem_limit_max(kern, sh.smem))
         return HELM3D_ERR_CUDA;
     kern<<<dim3((unsigned)sa.nz), kTcThreads, sh.smem, st>>>(k);
     return cudaGetLastError() == cudaSuccess ? HELM3D_OK : HELM3D_ERR_CUDA;

@@ -470,7 +470,7 @@ static int ztc_launch(const PlaneLayout &L, const VecBatch &vec, double scale, c
     const size_t smem = (size_t)a.nstage * stage + (3 * kZcMaxStages + 4) * sizeof(uint64_t) + 16;
     if (smem > device_info().smem_optin) return HELM3D_ERR_ARG;
     auto kern = a.KC == 16 ? ztc_kernel<FWD, 16> : ztc_kernel<FWD, 8>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (!smem_limit_max(kern, smem))
         return HELM3D_ERR_CUDA;
     const int grid = a.ntiles < device_info().sm_count ? a.ntiles : device_info().sm_count;
     kern<<<grid, kZcThreads, smem, s>>>(a);

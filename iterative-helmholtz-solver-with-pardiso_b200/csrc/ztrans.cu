@@ -79,7 +79,7 @@ static int zt_impl(const PlaneLayout &L, const VecBatch &vec, double scale, cons
     const size_t smem = (size_t)L.nz * kZtCols * sizeof(double2);
     auto kern = ztrans_kernel<R, FWD>;
     if (smem > device_info().smem_optin) return HELM3D_ERR_ARG;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (!smem_limit_max(kern, smem))
         return HELM3D_ERR_CUDA;
     const dim3 grid((unsigned)((L.plane + kZtCols - 1) / kZtCols), (unsigned)L.R);
     kern<<<grid, kZtCols * kZtWarps, smem, s>>>(L, vec, scale, sc, (cplx<R> *)planes, M);
