@@ -151,6 +151,7 @@ struct StencilArgs {
     VecBatch f;               // if f.p: y = f - A x
     int R;
     int zchunk = 16;          // z points per thread (autotuned: 8, 16, 32, 64)
+    int src_fast = 0;         // grid z order: 0 = z chunks within a source, 1 = sources within a z chunk
 };
 int launch_stencil(const StencilArgs &a, bool adjoint, cudaStream_t s);
 
@@ -272,9 +273,10 @@ template <typename K> inline bool smem_limit_max(K kern, size_t need) {
 bool tune_enabled();
 // HELM3D_FORCE_<family> as an integer, or -1 when unset
 int tune_forced(const char *family);
-constexpr int kStencilVariants = 4;   // z chunk 16, 8, 32, 64
+constexpr int kStencilVariants = 8;   // z chunk 16, 8, 32, 64; source-major (0-3) or source-minor (4-7) grid
 constexpr int kReduceVariants = 3;    // reduction blocks 2, 1, 4 per SM
 int stencil_zchunk(int v);
+int stencil_src_fast(int v);
 int reduce_blocks(int v);
 
 }  // namespace h3d

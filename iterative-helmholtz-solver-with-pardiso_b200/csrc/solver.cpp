@@ -271,6 +271,7 @@ static StencilArgs stencil_args(helm3d_ctx *c, const VecBatch &x, double xscale,
     a.f = f;
     a.R = R;
     a.zchunk = stencil_zchunk(c->tv_stencil);
+    a.src_fast = stencil_src_fast(c->tv_stencil);
     return a;
 }
 
@@ -585,6 +586,7 @@ int tune_solve(helm3d_ctx *c, int R, bool adjoint) {
         c->tv_stencil = tune_pick(c, "STENCIL", shape, kStencilVariants, [&](int v) {
             StencilArgs t = a0;
             t.zchunk = stencil_zchunk(v);
+            t.src_fast = stencil_src_fast(v);
             return launch_stencil(t, adjoint, c->stream);
         });
     }

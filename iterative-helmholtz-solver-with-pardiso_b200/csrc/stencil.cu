@@ -5,7 +5,9 @@
 // with cp_a(i) = alpha(i) alpha(i+1/2)/h^2 and cm_a(i) = alpha(i) alpha(i-1/2)/h^2
 // (the reference's 5-point form, beta2D_pml, Source/functions.cpp:2347-2402,
 // carried to z).  A thread owns one (i, j) column and marches along z with
-// the z neighbours in registers; x/y neighbours come through L1.
+// the z neighbours in registers; x/y neighbours come through L1.  The grid's
+// z dimension enumerates (source, z chunk) pairs, source-major or
+// source-minor (autotuned).
 #include <cuda_runtime.h>
 
 #include "cplx.cuh"
@@ -21,8 +23,12 @@ __global__ void __launch_bounds__(kStX *kStY) stencil_kernel(StencilArgs a) {
     const int j = blockIdx.y * kStY + threadIdx.y;
     if (i >= a.nx || j >= a.ny) return;
     const int nzc = (a.nz + a.zchunk - 1) / a.zchunk;
-    const int r = blockIdx.z / nzc;
-    const int k0 = (blockIdx.z - r * nzc) * a.zchunk;
+    // source-minor order: the R sources of a z chunk are adjacent in launch
+    // order and run together, so their reads of s2 and the coefficient
+    // tables meet in L2 instead of coming from DRAM once per source
+    const int r = a.src_fast ? (int)(blockIdx.z % a.R) : (int)(blockIdx.z / nzc);
+    const int zc = a.src_fast ? (int)(blockIdx.z / a.R) : (int)(blockIdx.z - r * nzc);
+    const int k0 = zc * a.zchunk;
     const int k1 = min(a.nz, k0 + a.zchunk);
     const long plane = (long)a.nx * a.ny;
     const long col = (long)j * a.nx + i;

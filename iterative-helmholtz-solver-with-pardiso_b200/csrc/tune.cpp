@@ -1,7 +1,7 @@
 // tune.cpp -- the autotuner: for every kernel family with several launch
 // shapes (the factor's cluster and warp layout, the sweep's bulk-copy stage
-// and ring sizes, the stencil's z chunk, the number of reduction blocks of
-// the Gram-Schmidt passes), the shape that runs fastest on this device for a
+// and ring sizes, the stencil's z chunk and grid order, the number of
+// reduction blocks of the Gram-Schmidt passes), the shape that runs fastest on this device for a
 // given problem shape.  Each candidate is launched once to warm up and then
 // timed three times with CUDA events on the context's stream (the best time
 // counts); the choice is kept for the process under a key of the family and
@@ -132,9 +132,11 @@ int tune_pick(helm3d_ctx *c, const char *family, const std::string &shape, int n
 }
 
 int stencil_zchunk(int v) {
-    static const int kZ[kStencilVariants] = {16, 8, 32, 64};
-    return kZ[(v >= 0 && v < kStencilVariants) ? v : 0];
+    static const int kZ[4] = {16, 8, 32, 64};
+    return kZ[(v >= 0 && v < kStencilVariants) ? v % 4 : 0];
 }
+
+int stencil_src_fast(int v) { return (v >= 4 && v < kStencilVariants) ? 1 : 0; }
 
 int reduce_blocks(int v) {
     static const int kPerSm[kReduceVariants] = {2, 1, 4};
