@@ -164,6 +164,7 @@ struct Reduce {
     int nblocks;
     int cap;
     int rmax;
+    int update = 0;           // DCGS2 update pass variant (0: loads one by one, 1: 8 basis loads batched)
 };
 // out[r][i] = <vs_r[i] V_r[i], w_r>   (i < nv); with wnorm also out[r][nv].x = ||w_r||^2
 // (pred: when given and *pred == 0 on the device, the kernels do nothing)
@@ -275,6 +276,7 @@ bool tune_enabled();
 int tune_forced(const char *family);
 constexpr int kStencilVariants = 8;   // z chunk 16, 8, 32, 64; source-major (0-3) or source-minor (4-7) grid
 constexpr int kReduceVariants = 3;    // reduction blocks 2, 1, 4 per SM
+constexpr int kUpdateVariants = 2;    // DCGS2 update pass: basis loads one by one, 8 batched
 int stencil_zchunk(int v);
 int stencil_src_fast(int v);
 int reduce_blocks(int v);
@@ -359,6 +361,7 @@ struct helm3d_ctx {
     int tv_factor = 0;
     int tv_sweep[2] = {0, 0};
     int tv_stencil = 0;
+    int tv_update = 0;
     size_t f_cap = 0, u_cap = 0;                // staging capacities (vectors) of d_f, d_u
     double *d_vs = nullptr;
     double2 *d_h = nullptr;        // small device scalars

@@ -252,6 +252,10 @@ __global__ void __launch_bounds__(kRedThreads) update_kernel(const double2 *__re
 //   V_j <- V_j - sum_{i<j} alpha_i V_i                 (j > 0)
 //   w   <- w - sum_{i<j} delta_i V_i - delta_j V_j(old)
 // and ||w||^2 partials; skip[r] set: zero partials, nothing read or written.
+// U > 1: the basis loads of U consecutive i issued together ahead of their
+// FMAs (more bytes in flight per thread; the FMA order, and so the result,
+// is the same as U = 1).
+template <int U>
 __global__ void __launch_bounds__(kRedThreads) update2_kernel(double2 *__restrict__ V, long ldv, long sV, int j,
                                                               const double2 *__restrict__ coef, long sCoef, int M2,
                                                               double2 *__restrict__ w, long sW, long N,
@@ -278,7 +282,20 @@ __global__ void __launch_bounds__(kRedThreads) update2_kernel(double2 *__restric
     for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
         double2 x = vj[l];
         double2 acc = cfms(delta[j], x, w[l]);
-        for (int i = 0; i < j; i++) {
+        int i = 0;
+        if (U > 1) {
+            for (; i + U <= j; i += U) {
+                double2 v[U];
+#pragma unroll
+                for (int q = 0; q < U; q++) v[q] = V[(long)(i + q) * ldv + l];
+#pragma unroll
+                for (int q = 0; q < U; q++) {
+                    x = cfms(alpha[i + q], v[q], x);
+                    acc = cfms(delta[i + q], v[q], acc);
+                }
+            }
+        }
+        for (; i < j; i++) {
             const double2 v = V[i * ldv + l];
             x = cfms(alpha[i], v, x);
             acc = cfms(delta[i], v, acc);
@@ -438,8 +455,13 @@ int launch_update2(const VecBatch &V, long ldv, int j, const double2 *coef, long
                    const int *skip) {
     if (R > red.rmax) return HELM3D_ERR_ARG;
     const int nb = red.nblocks;
-    update2_kernel<<<dim3(nb, R), kRedThreads, sizeof(double2) * (2 * j + 1), s>>>(
-        V.p, ldv, V.stride, j, coef, sCoef, M2, w.p, w.stride, N, red.partials, red.cap, pred, skip);
+    const size_t smem = sizeof(double2) * (2 * j + 1);
+    if (red.update == 1)
+        update2_kernel<8><<<dim3(nb, R), kRedThreads, smem, s>>>(V.p, ldv, V.stride, j, coef, sCoef, M2, w.p,
+                                                                 w.stride, N, red.partials, red.cap, pred, skip);
+    else
+        update2_kernel<1><<<dim3(nb, R), kRedThreads, smem, s>>>(V.p, ldv, V.stride, j, coef, sCoef, M2, w.p,
+                                                                 w.stride, N, red.partials, red.cap, pred, skip);
     reduce_partials_kernel<<<dim3(1, R), kFinalThreads, 0, s>>>(red.partials, nb, red.cap, 1, out, sOut, pred);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }

@@ -49,6 +49,7 @@ static Reduce reducer(helm3d_ctx *c) {
     r.nblocks = c->red_blocks;
     r.cap = c->red_cap;
     r.rmax = c->r_alloc;
+    r.update = c->tv_update;
     return r;
 }
 
@@ -557,10 +558,11 @@ static int cycle_graph(helm3d_ctx *c, int m, int B, bool adjoint) {
 // ------------------------------------------------------------- autotuning
 int tune_solve(helm3d_ctx *c, int R, bool adjoint) {
     const bool any_forced = std::getenv("HELM3D_FORCE_SWEEP") || std::getenv("HELM3D_FORCE_STENCIL") ||
-                            std::getenv("HELM3D_FORCE_REDUCE");
+                            std::getenv("HELM3D_FORCE_REDUCE") || std::getenv("HELM3D_FORCE_UPDATE");
     if (!tune_enabled() && !any_forced) {
         c->tv_sweep[0] = c->tv_sweep[1] = 0;
         c->tv_stencil = 0;
+        c->tv_update = 0;
         c->red_blocks = reduce_blocks(0);
         return HELM3D_OK;
     }
@@ -601,6 +603,19 @@ int tune_solve(helm3d_ctx *c, int R, bool adjoint) {
                             c->stream, nullptr, nullptr);
     });
     c->red_blocks = reduce_blocks(rv);
+    // the DCGS2 update pass at the same depth, in place on V_j and V_{j+1}
+    // (the solve overwrites both): its basis loads one by one or 8 batched
+    if (c->opts.mode == HELM3D_MODE_N && lowsync(c)) {
+        std::snprintf(shape, sizeof(shape), "%ld|%d|%d", N, R, j);
+        const int M2 = m + 2;
+        c->tv_update = tune_pick(c, "UPDATE", shape, kUpdateVariants, [&](int v) {
+            Reduce red = reducer(c);
+            red.update = v;
+            return launch_update2(VecBatch{c->d_V, ldV}, N, j, c->d_h + 4 * M2, scalars_per_rhs(m), M2,
+                                  VecBatch{c->d_V + (size_t)(j + 1) * N, ldV}, N, R, red, c->d_h + 2 * M2,
+                                  scalars_per_rhs(m), c->stream, nullptr, nullptr);
+        });
+    }
     return HELM3D_OK;
 }
 

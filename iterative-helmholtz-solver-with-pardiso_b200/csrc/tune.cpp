@@ -1,14 +1,15 @@
 // tune.cpp -- the autotuner: for every kernel family with several launch
 // shapes (the factor's cluster and warp layout, the sweep's bulk-copy stage
 // and ring sizes, the stencil's z chunk and grid order, the number of
-// reduction blocks of the Gram-Schmidt passes), the shape that runs fastest on this device for a
+// reduction blocks of the Gram-Schmidt passes, the update pass's load
+// batching), the shape that runs fastest on this device for a
 // given problem shape.  Each candidate is launched once to warm up and then
 // timed three times with CUDA events on the context's stream (the best time
 // counts); the choice is kept for the process under a key of the family and
 // the sizes it depends on and, with HELM3D_TUNE_CACHE=<file>, read from and
 // appended to that file so that later processes skip the timing.
 //   HELM3D_TUNE=0             no timing: the default shape (variant 0) of every family
-//   HELM3D_FORCE_<FAMILY>=v   force variant v (FACTOR, SWEEP, STENCIL, REDUCE)
+//   HELM3D_FORCE_<FAMILY>=v   force variant v (FACTOR, SWEEP, STENCIL, REDUCE, UPDATE)
 #include <cuda_runtime.h>
 
 #include <cstdio>
