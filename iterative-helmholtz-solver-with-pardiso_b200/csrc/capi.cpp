@@ -549,6 +549,7 @@ int helm3d_destroy(helm3d_ctx *c) {
         cudaEventDestroy(e.a);
         cudaEventDestroy(e.b);
     }
+    if (c->h_scal) cudaFreeHost(c->h_scal);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);

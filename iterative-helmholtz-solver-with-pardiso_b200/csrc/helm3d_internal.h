@@ -372,6 +372,8 @@ struct helm3d_ctx {
     size_t bytes = 0;
 
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double2 *h_scal = nullptr;     // pinned host mirror of the Krylov scalars, kept across solves
+    size_t h_scal_cap = 0;         // its capacity (double2)
 };
 
 namespace h3d {

@@ -653,7 +653,7 @@ struct FgmresRun {
     long N = 0, ldV = 0, ldZ = 0;
     size_t vb = 0;
     bool flexible = false;
-    double2 *hbuf = nullptr;     // pinned mirror of the Krylov scalars
+    double2 *hbuf = nullptr;     // pinned mirror of the Krylov scalars (the context's h_scal)
     std::vector<Rhs> S;
     std::vector<int> act;        // packed position p -> right-hand side
     bool x_zero = true;
@@ -666,9 +666,6 @@ struct FgmresRun {
 
     FgmresRun(helm3d_ctx *c_, const double2 *f_, double2 *u_, int R_, bool adj, helm3d_stats *st_)
         : c(c_), f(f_), u(u_), R(R_), adjoint(adj), st(st_) {}
-    ~FgmresRun() {
-        if (hbuf) cudaFreeHost(hbuf);
-    }
     bool done() const { return act.empty(); }
     bool device_cycle() const { return lowsync(c) || graphs_usable(); }
     bool graphs_usable() const { return c->use_graphs && !c->prof && !c->opts.verbose; }
@@ -720,11 +717,22 @@ struct FgmresRun {
         ldZ = (long)m * N;
         M2 = m + 2;
         SH = scalars_per_rhs(m);
-        if (cudaMallocHost((void **)&hbuf, sizeof(double2) * (size_t)SH * R) != cudaSuccess) {
-            cudaGetLastError();
-            hbuf = nullptr;
-            return set_error(c, HELM3D_ERR_OOM, "pinned host buffer");
+        // the pinned mirror lives in the context: pinning and unpinning host
+        // memory are driver calls (cudaFreeHost also waits for the device),
+        // kept out of every solve after the first of a size
+        const size_t need = (size_t)SH * R;
+        if (c->h_scal_cap < need) {
+            if (c->h_scal) cudaFreeHost(c->h_scal);
+            c->h_scal = nullptr;
+            c->h_scal_cap = 0;
+            if (cudaMallocHost((void **)&c->h_scal, sizeof(double2) * need) != cudaSuccess) {
+                cudaGetLastError();
+                c->h_scal = nullptr;
+                return set_error(c, HELM3D_ERR_OOM, "pinned host buffer");
+            }
+            c->h_scal_cap = need;
         }
+        hbuf = c->h_scal;
         cudaEventRecord(c->ev0, c->stream);
         RC(cuda_check(c, cudaMemcpyAsync(c->d_Fw, f, vb * R, cudaMemcpyDeviceToDevice, c->stream), "f copy"));
         RC(cuda_check(c, cudaMemsetAsync(c->d_Uw, 0, vb * R, c->stream), "x0"));
