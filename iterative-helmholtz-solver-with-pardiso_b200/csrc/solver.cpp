@@ -313,13 +313,6 @@ static int residual(helm3d_ctx *c, const VecBatch &f, const VecBatch &x, const V
     return axpby(c, make_double2(1, 0), f, make_double2(-1, 0), r, R);
 }
 
-// small pinned host mirror of device scalars
-struct Pinned {
-    double2 *h = nullptr;
-    explicit Pinned(size_t n) { cudaMallocHost((void **)&h, sizeof(double2) * n); }
-    ~Pinned() { if (h) cudaFreeHost(h); }
-};
-
 static int fetch(helm3d_ctx *c, const double2 *d, size_t n, double2 *h, const char *what) {
     RC(cuda_check(c, cudaMemcpyAsync(h, d, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->stream), what));
     return cuda_check(c, cudaStreamSynchronize(c->stream), what);
