@@ -1,26 +1,41 @@
 """Benchmark: time to relative residual 1e-8 per 3D Helmholtz solve.
 
-Workload (default): the 128^3 heterogeneous medium (1500 -> 3000 m/s linear
+Workload (default): the 200^3 heterogeneous medium (1500 -> 3000 m/s linear
 depth gradient along y, three seeded Gaussian anomalies of +-20 %, radius
-8-15 h), h = 10 m, 12-point PML on every face, 8 points per minimum
+8-15 h), h = 10 m, 16-point PML on every face, 8 points per minimum
 wavelength, 16 seeded Gaussian point sources; the 7-point PML operator
 solved by FGMRES(20) to ||f - A u|| / ||f|| <= 1e-8 for every source.
-Inputs are synthetic (seeded splitmix64), no dataset is read.
+Inputs are synthetic (seeded splitmix64), no dataset is read.  `--grid 128`
+selects the 128^3 medium of the same recipe with a 12-point PML.
 
 One step = one medium: set-up + block LU factor of all kz systems + one
 lockstep batched FGMRES over the 16 sources, with the preconditioner in
 complex64 and the z-transform in the PML eigenbasis (outer loop, operator
 and Gram-Schmidt in complex128).  `value` is seconds per source-solve (step
 time / 16) with the medium and the sources resident on the device, timed
-with CUDA events on the solver's stream.  Beside it: the same preconditioner
-with one source per step, the FFT-z preconditioner (the reference's method)
-in complex64, and the plain complex128 FFT-z path with one source per step
-(`fp64_plain`, the drop-in baseline).  `e2e` repeats the headline step
+with CUDA events on the solver's stream.  `e2e` repeats the headline step
 through the C ABI with pinned host buffers (medium and sources copied in,
 solutions copied out inside the timed region).
 
-    python bench.py [--steps K] [--warmup W] [--impl ours|reference] [--grid 128]
+Beside the headline, one step each (after one warm-up step) of the same
+workload solved other ways, so that each stated change can be read apart:
+
+  fp64_plain          FFT-z, complex128 preconditioner, one source per step
+                      (the plain FP64 GPU drop-in of the reference's method)
+  fft_z_c64_single    FFT-z, complex64 preconditioner, one source
+  fft_z_c64_batched   FFT-z, complex64 preconditioner, 16 sources in lockstep
+  eigen_c128_single   PML eigenbasis, complex128 preconditioner, one source
+  single_source       PML eigenbasis, complex64 preconditioner, one source
+
+Every arm's source-0 solution is compared with the FP64 oracle's solution
+of the same source (tests/golden/port_*_n<grid>.npz, a strided sample).
+
+    python bench.py [--steps K] [--warmup W] [--impl ours|reference] [--grid 200]
     torchrun --nproc-per-node N bench.py --gpus N     (N independent replicas)
+
+`--impl reference` times the CPU port of the reference's method (oracle.port:
+FFT-z + one SuperLU factor per kz + FGMRES(20) in complex128 on every host
+core) on the same workload; see run_reference.
 """
 from __future__ import annotations
 
@@ -36,6 +51,7 @@ import time
 
 REPO = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(REPO, "iterative-helmholtz-solver-with-pardiso_b200")
+GOLDEN = os.path.join(REPO, "tests", "golden")
 for _p in (REPO, PKG_DIR):
     if _p not in sys.path:
         sys.path.insert(0, _p)
@@ -47,19 +63,54 @@ TOL = 1e-8
 RESTART = 20
 BETA_PREC = 0.25
 BATCH = 16
-# FGMRES iterations the complex128 FFT-z path needs at the 128^3 workload
-# (measured on a B200 with this bench: 513); the CPU port times a sample of
-# iterations and scales to this count.
-ITERS_128 = 513
+SAMPLE_STRIDE = 8
 
 
-def workload(n: int, nsrc: int = 1):
-    """The 128^3 heterogeneous medium recipe at size n with nsrc seeded
-    sources (the medium does not depend on nsrc; source 0 is the same)."""
-    from helm3d import media
-    p = media.layered_medium(n, n, n, 10.0, 12, 2024, ppw=8.0, n_sources=nsrc)
-    p.meta["config"] = "C2"
+def pml_for(n: int) -> int:
+    return 16 if n >= 200 else 12
+
+
+def workload(n: int, nsrc: int = BATCH):
+    """The heterogeneous medium recipe at size n with nsrc seeded sources
+    (the medium does not depend on nsrc; source 0 is the same)."""
+    from helm3d import media   # pure Python: loads no native library
+    p = media.layered_medium(n, n, n, 10.0, pml_for(n), 2024, ppw=8.0, n_sources=nsrc)
+    p.meta["config"] = "C5-forward" if n == 200 else "C2"
     return p
+
+
+def workload_config(n: int) -> dict:
+    """The `config` object of both arms' lines: what is solved, not how."""
+    return {
+        "workload": f"{n}^3 heterogeneous medium (1500->3000 m/s depth gradient, three +-20 % Gaussian "
+                    f"anomalies), h = 10 m, PML {pml_for(n)} on all faces, 8 ppw, {BATCH} seeded Gaussian "
+                    f"sources; 7-point PML operator solved to ||f - A u|| / ||f|| <= {TOL} per source; "
+                    f"value = seconds per source-solve including set-up and factor",
+        "n": n, "pml": pml_for(n), "sources": BATCH, "tol": TOL, "restart": RESTART,
+        "l2": "inputs larger than L2 (Krylov bases and factor tens of GB; sources alone 2 GB at 200^3)",
+    }
+
+
+def oracle_record(n: int, kind: str):
+    """The oracle port's full solve of source 0 at grid n (kind "fftz": the
+    reference's method to 1e-8; "eigen": to 1e-12), or None."""
+    path = os.path.join(GOLDEN, f"port_{kind}_n{n}.npz")
+    if not os.path.exists(path):
+        return None
+    d = np.load(path)
+    return {k: d[k] for k in d.files}
+
+
+def sample_err(u0, rec):
+    """Relative error of a source-0 solution (torch or NumPy, (nz, ny, nx))
+    against the oracle's strided sample."""
+    if rec is None:
+        return None
+    s = int(rec["stride"])
+    a = u0[::s, ::s, ::s]
+    a = a.cpu().numpy() if hasattr(a, "cpu") else np.asarray(a)
+    ref = rec["sample"]
+    return float(np.linalg.norm(a - ref) / np.linalg.norm(ref))
 
 
 def read_peaks():
@@ -67,9 +118,23 @@ def read_peaks():
     try:
         with open(path) as fh:
             d = json.load(fh)
-        return float(d["hbm_gbs"]), "measured"
+        return d, "measured"
     except Exception:
-        return 6650.0, "fallback"
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def native_libs_loaded():
+    """In-tree shared objects mapped into this process (Linux)."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as fh:
+            for line in fh:
+                path = line.rsplit(None, 1)[-1]
+                if path.endswith(".so") and path.startswith(REPO):
+                    out.add(os.path.relpath(path, REPO))
+    except OSError:
+        pass
+    return sorted(out)
 
 
 class Clocks:
@@ -156,6 +221,66 @@ def init_dist(world: int):
 
 
 # ---------------------------------------------------------------- GPU arm
+
+
+# ---------------------------------------------------------------- GPU arm
+def family_bytes_flops(p, its_per_source: float, nsrc: int, e: int = 8):
+    """Algorithmic bytes (HBM families) or flops (factor) per launch of each
+    kernel family on the headline step; Krylov is per step (its launches
+    differ in size), from the mean Arnoldi step over a restart cycle."""
+    N = p.nx * p.ny * p.nz
+    R = nsrc
+    # DCGS2 step j moves (2j + 5) 16 N bytes per source; over a cycle of
+    # RESTART steps the mean of 2j + 5 is RESTART + 4
+    krylov_step = (RESTART + 4) * 16.0 * N * its_per_source * R
+    return {
+        # G^T read forward and backward + the planes of all sources read and written in both passes
+        "sweep": ("hbm", 2.0 * p.nz * p.ny * p.nx * p.nx * e + 4.0 * N * e * R),
+        # complex128 x in, planes out (forward); planes in, complex128 y out (inverse)
+        "fft_fwd": ("hbm", (16.0 + e) * N * R),
+        "fft_inv": ("hbm", (16.0 + e) * N * R),
+        # x read, y written per source, s2 once per z chunk (source-minor order)
+        "stencil": ("hbm", 32.0 * N * R + 8.0 * N),
+        # 8 nx^3 real flops per (kz, y-line) block
+        "factor": ("tensor", 8.0 * p.nx ** 3 * p.ny * p.nz),
+        "krylov": ("hbm_per_step", krylov_step),
+    }
+
+
+def roofline_table(p, prof, its_per_source, nsrc, peaks):
+    fam = family_bytes_flops(p, its_per_source, nsrc)
+    hbm = float(peaks["hbm_gbs"])
+    tc = float(peaks.get("bf16_tflops_sustained") or peaks["bf16_tflops"])
+    out = {}
+    for k, (ms, n) in prof.items():
+        if not n or k not in fam:
+            continue
+        kind, amount = fam[k]
+        if kind == "hbm_per_step":
+            t = ms / 1e3
+            ach = amount / t / 1e9
+            out[k] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                      "bytes_per_step": amount, "ms_per_step": ms, "launches": int(n)}
+            continue
+        t = ms / n / 1e3
+        if kind == "hbm":
+            ach = amount / t / 1e9
+            out[k] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                      "bytes_per_launch": amount, "ms_per_launch": ms / n, "launches": int(n)}
+        else:
+            ach = amount / t / 1e12
+            out[k] = {"bound": "tensor", "achieved": ach, "peak": tc, "unit": "TFLOP/s", "frac": ach / tc,
+                      "flops_per_launch": amount, "ms_per_launch": ms / n, "launches": int(n)}
+    return out
+
+
+# DRAM read + write of one launch (ncu: dram__bytes_read.sum +
+# dram__bytes_write.sum of one captured launch), per (family, grid, sources)
+TRAFFIC = {
+    ("sweep", 128, 16): 5.273e9,
+}
+
+
 def run_ours(args, rank, world, dist):
     import torch
 
@@ -163,7 +288,8 @@ def run_ours(args, rank, world, dist):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    p = workload(args.n, BATCH)
+    n = args.n
+    p = workload(n, BATCH)
     F_host = np.stack([p.rhs(i) for i in range(BATCH)])
     s2_host = np.ascontiguousarray(p.s2)
     grid = helm3d.grid_mode_n(p.nx, p.ny, p.nz, p.h, p.pml, p.omega)
@@ -174,6 +300,8 @@ def run_ours(args, rank, world, dist):
     F_dev = torch.from_numpy(F_host).to(dev)
     s2_dev = torch.from_numpy(s2_host).to(dev)
     U_dev = torch.empty_like(F_dev)
+    rec_eig = oracle_record(n, "eigen")
+    rec_fft = oracle_record(n, "fftz")
 
     def make(prec, zt):
         o = helm3d.default_opts(precision=prec, restart=RESTART, tol=TOL, beta_prec=BETA_PREC, max_iter=20000,
@@ -194,18 +322,18 @@ def run_ours(args, rank, world, dist):
         s.set_medium(s2)
         s.solve(F[:nrhs], nrhs=nrhs, u=U[:nrhs], allow_not_converged=True)
 
-    def timed_steps(s, nrhs, steps, warmup):
+    def timed_steps(s, nrhs, steps, warmup, s2=s2_dev, F=F_dev, U=U_dev):
         """ms per step (max over ranks), iterations per source of the last
         step, launches in the timed region, last stats."""
         for _ in range(warmup):
-            step(s, nrhs)
+            step(s, nrhs, s2, F, U)
         barrier()
         launches0 = s.kernel_launches
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(steps):
-            step(s, nrhs)
+            step(s, nrhs, s2, F, U)
         e1.record(stream)
         barrier()
         ms = max_over_ranks(e0.elapsed_time(e1) / steps)
@@ -226,68 +354,58 @@ def run_ours(args, rank, world, dist):
     time.sleep(1.5)   # let the sampler start up before the timed region
     ms_h, its_h, launches_h, st_h = timed_steps(sh, BATCH, args.steps, args.warmup)
     clk = clocks.stop()
+    relres_h = st_h.relres
+    err_h = sample_err(U_dev[0], rec_eig)
     prof = profiled(sh, BATCH)
-    relres_h = sh.last_stats.relres
-    U_h = U_dev.clone()
 
     # e2e through the C ABI with host buffers (pinned): medium and sources in,
     # solutions out, every step
     F_pin = torch.from_numpy(F_host).pin_memory()
     s2_pin = torch.from_numpy(s2_host).pin_memory()
     U_pin = torch.empty_like(F_pin).pin_memory()
-    step(sh, BATCH, s2_pin, F_pin, U_pin)
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step(sh, BATCH, s2_pin, F_pin, U_pin)
-    e1.record(stream)
-    barrier()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-    # the same preconditioner, one source per step
-    ms_1, its_1, _, _ = timed_steps(sh, 1, args.steps, 1)
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    e2e_ms, _, _, _ = timed_steps(sh, BATCH, e2e_steps, 1, s2_pin, F_pin, U_pin)
+    del F_pin, U_pin, s2_pin
     sh.close()
 
-    # the reference's method (FFT-z) with the complex64 preconditioner, one source
-    sf = make(helm3d.PREC_C64, helm3d.ZT_FFT)
-    ms_f, its_f, _, st_f = timed_steps(sf, 1, max(1, args.steps // 2), 1)
-    relres_f = st_f.relres
-    sf.close()
-
-    # plain complex128 FFT-z path, one source per step
-    s64 = make(helm3d.PREC_C128, helm3d.ZT_FFT)
-    ms64, its64, _, st64 = timed_steps(s64, 1, max(1, args.steps // 2), 1)
-    u64 = U_dev[0].clone()
-    relres64 = st64.relres
-    s64.close()
-    relerr = float(torch.linalg.vector_norm(U_h[0] - u64) / torch.linalg.vector_norm(u64))
+    # the same workload solved other ways, one step each after a warm-up step
+    arms = {}
+    for name, prec, zt, nrhs in (("single_source", helm3d.PREC_C64, helm3d.ZT_PML_EIGEN, 1),
+                                 ("fft_z_c64_batched", helm3d.PREC_C64, helm3d.ZT_FFT, BATCH),
+                                 ("fft_z_c64_single", helm3d.PREC_C64, helm3d.ZT_FFT, 1),
+                                 ("eigen_c128_single", helm3d.PREC_C128, helm3d.ZT_PML_EIGEN, 1),
+                                 ("fp64_plain", helm3d.PREC_C128, helm3d.ZT_FFT, 1)):
+        if name in args.skip_arms:
+            continue
+        s = make(prec, zt)
+        ms, its, _, st = timed_steps(s, nrhs, args.arm_steps, 1)
+        arms[name] = {"value": ms / nrhs / 1e3 / world, "unit": "s", "ms_per_step": ms, "sources_per_step": nrhs,
+                      "iterations_per_source": its, "relres": st.relres,
+                      "relerr_vs_fp64_oracle": sample_err(U_dev[0], rec_eig),
+                      "precision": "c64" if prec == helm3d.PREC_C64 else "c128",
+                      "z_transform": "fft" if zt == helm3d.ZT_FFT else "PML eigenbasis"}
+        s.close()
 
     if rank != 0:
         return None
 
-    # roofline of the dominant single kernel of the headline step (the
-    # preconditioner kernels; the Krylov family is several kernels)
-    e = 8
-    nbytes = {
-        # G^T read in both passes, planes of all sources read + written in both
-        "sweep": 2.0 * p.nz * p.ny * p.nx * p.nx * e + 4.0 * N * e * BATCH,
-        # x (complex128) in, planes (complex64) out; W from L2
-        "fft_fwd": (16.0 + e) * N * BATCH,
-        "fft_inv": (16.0 + e) * N * BATCH,
-        "stencil": (16.0 * 2 + 8.0) * N * BATCH,
-    }
-    top = max(nbytes, key=lambda k: prof[k][0])
-    # DRAM read + write of one launch of the tensor-core sweep on this
-    # workload (128^3, 16 sources), measured with ncu (dram__bytes_read.sum
-    # + dram__bytes_write.sum of one captured launch)
-    traffic = 5.273e9 if (top == "sweep" and p.nx == 128 and BATCH == 16) else None
-    k_ms, k_n = prof[top]
-    avg_s = (k_ms / max(1, k_n)) / 1e3
-    achieved = nbytes[top] / avg_s / 1e9 if avg_s > 0 else None
-    peak, peak_kind = read_peaks()
+    peaks, peak_kind = read_peaks()
+    table = roofline_table(p, prof, its_h, BATCH, peaks)
+    # the dominant single kernel: the family with the largest device time
+    # whose launches are one kernel each (Krylov is several kernels per step)
+    single = {k: v for k, v in prof.items() if k in table and k != "krylov"}
+    top = max(single, key=lambda k: single[k][0])
+    r = dict(table[top])
+    r["kernel"] = top
+    r["peak_source"] = peak_kind
+    r["traffic"] = TRAFFIC.get((top, n, BATCH))
     total_prof = sum(v[0] for v in prof.values())
     per_src = ms_h / BATCH
+
+    def ratio(a, b):
+        return (a / b) if (a and b) else None
+
+    fp = arms.get("fp64_plain", {}).get("value")
     line = {
         "metric": METRIC,
         "value": per_src / 1e3 / world,
@@ -301,38 +419,40 @@ def run_ours(args, rank, world, dist):
         "vs_baseline": None,
         "dtype": "c64 preconditioner / c128 outer",
         "data": "synthetic (seeded splitmix64 medium and sources)",
-        "config": {
-            "workload": f"{p.nx}^3 heterogeneous medium, PML 12, 8 ppw, {BATCH} Gaussian sources; one step = "
-                        f"set-up + block LU factor + batched FGMRES({RESTART}) to 1e-8 for all sources; "
-                        f"value = step time / {BATCH}",
-            "n": p.nx, "pml": p.pml, "sources_per_step": BATCH, "restart": RESTART, "tol": TOL,
-            "beta_prec": BETA_PREC, "z_transform": "PML eigenbasis",
-            "l2": "inputs larger than L2 (factor 2.1 GB, sources 0.54 GB, Krylov bases 22 GB)",
-            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-        },
+        "config": dict(workload_config(n), parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+        "method": f"PML-eigenbasis z-transform, complex64 preconditioner (tcgen05 sweep and z-transforms), "
+                  f"complex128 FGMRES({RESTART}) with DCGS2, {BATCH} sources in lockstep, beta_prec {BETA_PREC}",
         "solves_per_s": world * 1e3 / per_src,
         "iterations_per_source": its_h,
         "relres": relres_h,
-        "relerr_vs_fp64_plain": relerr,
-        "single_source": {"value": ms_1 / 1e3 / world, "unit": "s", "iterations": its_1},
-        "fft_z_c64_single": {"value": ms_f / 1e3 / world, "unit": "s", "iterations": its_f, "relres": relres_f},
-        "fp64_plain": {"value": ms64 / 1e3 / world, "unit": "s", "iterations": its64, "relres": relres64},
-        "speedup_vs_fp64_plain": (ms64 / per_src) if per_src > 0 else None,
-        "e2e": {"value": e2e_ms / BATCH / 1e3 / world, "unit": "s",
+        "relerr_vs_fp64_oracle": err_h,
+        "oracle": {"eigen": f"tests/golden/port_eigen_n{n}.npz" if rec_eig is not None else None,
+                   "fftz": f"tests/golden/port_fftz_n{n}.npz" if rec_fft is not None else None,
+                   "compared_on": f"source 0, every {SAMPLE_STRIDE}th point per axis"},
+        **arms,
+        "speedup_vs_fp64_plain": ratio(fp, per_src / 1e3 / world),
+        "forms_apart": {
+            "precision_and_batching_under_fft_z": ratio(fp, arms.get("fft_z_c64_batched", {}).get("value")),
+            "precision_alone_under_fft_z": ratio(fp, arms.get("fft_z_c64_single", {}).get("value")),
+            "precision_and_batching_under_eigenbasis": ratio(arms.get("eigen_c128_single", {}).get("value"),
+                                                             per_src / 1e3 / world),
+            "z_transform_alone_c128": ratio(fp, arms.get("eigen_c128_single", {}).get("value")),
+        },
+        "e2e": {"value": e2e_ms / BATCH / 1e3 / world, "unit": "s", "steps": e2e_steps,
                 "h2d_bytes_per_step": N * 8 + BATCH * N * 16, "d2h_bytes_per_step": BATCH * N * 16},
         "gpu_launches": int(launches_h),
-        "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                     "bytes_per_launch": nbytes[top], "traffic": traffic},
+        "roofline": r,
+        "roofline_by_family": table,
         "kernel_ms_per_step": {k: round(v[0], 3) for k, v in prof.items()},
         "kernel_launches_per_step": {k: int(v[1]) for k, v in prof.items()},
         "kernel_share": {k: round(v[0] / total_prof, 4) for k, v in prof.items()} if total_prof > 0 else None,
         "clocks": clk,
     }
-    return line, round(its64) if its64 else None
+    if rec_fft is not None:
+        line["oracle"]["fftz_iterations"] = int(rec_fft["iterations"])
+    return line
 
 
-# ------------------------------------------------------ kernel microbench
 def run_kernels(args):
     """Per-kernel device times of one batched FGMRES(1) iteration (one
     preconditioner apply and one operator apply for all 16 sources, plus the
@@ -368,7 +488,8 @@ def run_kernels(args):
         "fft_fwd": (16.0 + e) * N * BATCH,
         "fft_inv": (16.0 + e) * N * BATCH,
     }
-    peak, peak_kind = read_peaks()
+    peaks, peak_kind = read_peaks()
+    peak = float(peaks["hbm_gbs"])
     out = {"mode": "kernels", "workload": f"{p.nx}^3, {BATCH} sources, c64 preconditioner, PML eigenbasis",
            "steps": args.steps, "peak_gbs": peak, "peak_source": peak_kind, "kernels": {}}
     for k, (ms, n) in prof.items():
@@ -584,95 +705,145 @@ def helm3d_media():
 
 
 # ------------------------------------------------------------ CPU baseline
-def cpu_port_sample(n: int, iters: int | None, cores: int, budget_iters: int = 2):
-    """Time the oracle port (SciPy SuperLU per kz + NumPy FFT + NumPy stencil,
-    FP64, `cores` threads) on a bounded sample of the workload and scale to
-    one full solve: factor of a subset of kz systems scaled to all nz, plus a
-    few preconditioned FGMRES iterations scaled to `iters`."""
-    from concurrent.futures import ThreadPoolExecutor
 
-    import scipy.sparse.linalg as spla
 
-    from oracle import mode_n
-    from oracle.mode_r import assemble_2d
+# ------------------------------------------------------------ CPU baseline
+def port_iterations(n: int, workers: int):
+    """FGMRES iterations the CPU port of the reference's method needs on
+    source 0 of the n^3 workload: from its recorded full solve
+    (tests/golden/port_fftz_n<n>.npz, made by `python -m oracle.port`), or,
+    for small grids, from a full solve run here.  Never from a GPU run."""
+    rec = oracle_record(n, "fftz")
+    if rec is not None:
+        return int(rec["iterations"]), f"the port's recorded full solve (tests/golden/port_fftz_n{n}.npz)"
+    if n > 64:
+        return None, f"no recorded full solve of the port at {n}^3"
+    from oracle import port
+    p = workload(n, 1)
+    with port.PortPreconditioner(p, beta_prec=BETA_PREC, workers=workers) as pre:
+        pre.factor()
+        op = port.PortOperator(p, threads=workers)
+        _, its, _, _, _ = port.fgmres(op, pre.apply, p.rhs(0), tol=TOL, m=RESTART, max_iter=20000)
+    return its, "a full solve of the port run here"
 
-    p = workload(n)
-    st = mode_n.setup(p, beta_prec=BETA_PREC, factor=False)
-    nz = p.nz
-    kf = min(nz, max(2 * cores, 8))
-    ks = list(range(0, nz, max(1, nz // kf)))[:kf]
-    t0 = time.perf_counter()
-    with ThreadPoolExecutor(cores) as ex:
-        lus = list(ex.map(lambda k: spla.splu(assemble_2d(st.g, st.shifts[k])), ks))
-    t_factor = (time.perf_counter() - t0) * nz / len(ks)
-    # one preconditioner apply: FFT, nz 2D solves (sampled kz, scaled), iFFT
-    f = p.rhs(0)
-    rng = np.random.default_rng(0)
-    v = (rng.standard_normal(p.shape) + 1j * rng.standard_normal(p.shape))
-    t0 = time.perf_counter()
-    vh = np.fft.fft(v, axis=0)
-    t_fft = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    with ThreadPoolExecutor(cores) as ex:
-        list(ex.map(lambda q: lus[q].solve(vh[ks[q]].ravel()), range(len(ks))))
-    t_solves = (time.perf_counter() - t0) * nz / len(ks)
-    t0 = time.perf_counter()
-    w = st.apply_a(v)
-    t_stencil = time.perf_counter() - t0
-    # CGS2 against RESTART/2 basis vectors on average
-    nv = RESTART // 2
-    V = np.stack([v.ravel()] * nv)
-    t0 = time.perf_counter()
-    for _ in range(2):
-        h = V.conj() @ w.ravel()
-        wv = w.ravel() - V.T @ h
-    t_cgs = time.perf_counter() - t0
-    per_it = 2 * t_fft + t_solves + t_stencil + t_cgs
-    its = iters if iters else 0
+
+class PortSample:
+    """The CPU port of the reference's method on the workload: the factor of
+    every kz system (timed in full) and real FGMRES(20) iterations of source
+    0 from a zero start (each timed), with the host's cores."""
+
+    def __init__(self, n: int, workers: int):
+        from oracle import port
+        self.port = port
+        self.n = n
+        self.workers = workers
+        self.p = workload(n, 1)
+        self.pre = port.PortPreconditioner(self.p, beta_prec=BETA_PREC, workers=workers)
+        self.factor_s = self.pre.factor()
+        self.op = port.PortOperator(self.p, threads=workers)
+        f = self.p.rhs(0)
+        t0 = time.perf_counter()
+        r = f - self.op(np.zeros_like(f))
+        np.linalg.norm(r)
+        self.residual_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        self.pre.apply(f)
+        self.apply_s = time.perf_counter() - t0
+
+    def iterations(self, count: int):
+        """Seconds of each of the first `count` FGMRES iterations."""
+        _, _, _, _, times = self.port.fgmres(self.op, self.pre.apply, self.p.rhs(0), tol=TOL, m=RESTART,
+                                             max_iter=count, max_cycles_iters=count)
+        return times
+
+    def close(self):
+        self.pre.close()
+
+
+def cpu_port_value(ps: PortSample, per_it: float, iters: int):
+    restarts = max(1, math.ceil(iters / RESTART))
+    return ps.factor_s + per_it * iters + (restarts + 1) * ps.residual_s
+
+
+def cpu_port_sample(n: int, cores: int, sample_iters: int = 3):
+    """cpu_baseline of the GPU line: the port's factor of all kz systems and
+    its first few FGMRES iterations on the workload, scaled to the port's
+    own iteration count."""
+    iters, src = port_iterations(n, cores)
+    if iters is None:
+        return {"value": None, "unit": "s", "cores": cores, "kind": "port", "sample": src}
+    ps = PortSample(n, cores)
+    try:
+        times = ps.iterations(sample_iters)
+    finally:
+        ps.close()
+    per_it = statistics.mean(times)
     return {
-        "value": t_factor + per_it * its,
+        "value": cpu_port_value(ps, per_it, iters),
         "unit": "s",
         "cores": cores,
         "kind": "port",
-        "sample": f"splu factor of {len(ks)} of {nz} kz systems and one preconditioned FGMRES iteration "
-                  f"(FFT, {len(ks)} 2D solves, stencil, CGS2 on {nv} vectors) on the {n}^3 workload, "
-                  f"scaled to {nz} systems and {its} iterations",
-        "factor_s": t_factor,
+        "sample": f"SuperLU factor of all {ps.p.nz} kz systems ({ps.factor_s:.1f} s) and the first "
+                  f"{len(times)} FGMRES({RESTART}) iterations of source 0 ({per_it:.2f} s each: FFT-z, {ps.p.nz} 2D "
+                  f"solves, 7-point operator, CGS2) on the {n}^3 workload, scaled to {iters} iterations "
+                  f"({src}) plus one true residual per restart",
+        "factor_s": ps.factor_s,
         "per_iteration_s": per_it,
+        "iterations": iters,
     }
 
 
 def run_reference(args, rank):
+    """The reference's method on the host cores: the CPU port (oracle.port,
+    the restatement of Source/FGMRES.cpp:464-684 with Solve3DSparseUsingFT_CSR,
+    Source/functions.cpp:5837-6061: FFT-z, a SuperLU factor per kz in place
+    of PARDISO, complex128) on the same workload and `config` as the GPU arm.
+    Set-up factors all kz systems (timed in full, part of every solve); each
+    step is one real FGMRES(20) iteration of source 0 from a zero start
+    (warm-up iterations first), so that K steps sample the cost of an
+    iteration across the restart cycle.  value = factor + mean iteration x
+    the port's own iteration count for this workload + one true residual
+    per restart.  Loads none of this repository's native code."""
     if rank != 0:
         return None
     cores = os.cpu_count() or 1
-    iters = ITERS_128 if args.n == 128 else None
-    vals = []
-    for _ in range(args.warmup):
-        cpu_port_sample(args.n, iters, cores)
-    for _ in range(args.steps):
-        vals.append(cpu_port_sample(args.n, iters, cores))
-    v = statistics.median(x["value"] for x in vals)
-    base = vals[-1]
-    base["value"] = v
-    p = workload(args.n)
-    return {
-        "impl": "reference",
-        "metric": METRIC,
+    iters, src = port_iterations(args.n, cores)
+    base = {"impl": "reference", "metric": METRIC, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "dtype": "c128",
+            "data": "synthetic (seeded splitmix64 medium and sources)", "config": workload_config(args.n)}
+    if iters is None:
+        return dict(base, unavailable=src)
+    ps = PortSample(args.n, cores)
+    try:
+        times = ps.iterations(args.warmup + max(1, args.steps))
+    finally:
+        ps.close()
+    timed = times[args.warmup:] or times
+    per_it = statistics.mean(timed)
+    v = cpu_port_value(ps, per_it, iters)
+    # the reference applies L0^{-1} three times per iteration
+    # (Source/FGMRES.cpp:503,579,601); the port once
+    t_apply_extra = 2.0 * ps.apply_s
+    line = dict(base)
+    line.update({
         "value": v,
-        "unit": "s",
-        "n_gpus": args.gpus,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "higher_is_better": False,
-        "dtype": "c128",
-        "data": "synthetic (seeded splitmix64 media and sources)",
-        "config": {"workload": f"{p.nx}^3 heterogeneous medium, PML 12, 8 ppw, Gaussian source; the reference's "
-                               f"method (FFT-z + per-kz sparse LU, FGMRES({RESTART}) to 1e-8, complex128) per "
-                               f"source-solve", "n": p.nx},
-        "cpu_baseline": base,
+        "method": f"FFT-z preconditioner, SuperLU per kz (PARDISO in the reference), complex128 FGMRES({RESTART}) "
+                  f"with CGS2, one source per solve as the reference's main loop",
+        "iterations": iters,
+        "iterations_source": src,
+        "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port",
+                         "sample": f"set-up: SuperLU factor of all {ps.p.nz} kz systems ({ps.factor_s:.1f} s); "
+                                   f"each step one FGMRES({RESTART}) iteration of source 0 ({len(timed)} timed after "
+                                   f"{args.warmup} warm-up, mean {per_it:.2f} s); scaled to {iters} iterations",
+                         "factor_s": ps.factor_s, "per_iteration_s": per_it},
+        "reference_structure_estimate": {
+            "value": ps.factor_s + (per_it + t_apply_extra) * iters,
+            "note": f"three preconditioner applies per iteration as Source/FGMRES.cpp:503,579,601 "
+                    f"(one apply timed: {ps.apply_s:.2f} s)"},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+        "native_libs_loaded": native_libs_loaded(),
+    })
+    return line
 
 
 def main():
@@ -681,7 +852,10 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--grid", dest="n", type=int, default=128, help="grid points per axis")
+    ap.add_argument("--grid", dest="n", type=int, default=200, help="grid points per axis")
+    ap.add_argument("--e2e-steps", type=int, default=5, help="timed e2e steps (at most --steps)")
+    ap.add_argument("--arm-steps", type=int, default=1, help="timed steps of each comparison arm")
+    ap.add_argument("--skip-arms", default="", help="comma-separated comparison arms to leave out")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels", action="store_true",
                     help="per-kernel microbench: batched FGMRES(1) iterations instead of full solves")
@@ -690,13 +864,20 @@ def main():
                          "group; c5: 200^3 misfit gradient with finite-difference check; n200: 200^3 batched "
                          "complex64 vs plain complex128")
     args = ap.parse_args()
+    args.skip_arms = set(a for a in args.skip_arms.split(",") if a)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        # the CPU reference runs on rank 0 only; the other ranks exit at once
+        out = run_reference(args, rank)
+        if rank == 0 and out is not None:
+            print(json.dumps(out))
+        return
     if args.kernels:
         print(json.dumps(run_kernels(args)))
         return
-    if args.workload != "headline" and args.impl == "ours":
+    if args.workload != "headline":
         if args.workload == "c3":
             out = run_large(args, 160, 30, "c3")
         elif args.workload == "n200":
@@ -707,18 +888,11 @@ def main():
             out = run_gradient(args)
         print(json.dumps(out))
         return
-    if args.impl == "reference":
-        # the CPU reference runs on rank 0 only; the other ranks exit at once
-        out = run_reference(args, rank)
-        if rank == 0 and out is not None:
-            print(json.dumps(out))
-        return
     dist = init_dist(world)
-    res = run_ours(args, rank, world, dist)
-    if rank == 0 and res is not None:
-        line, its64 = res
+    line = run_ours(args, rank, world, dist)
+    if rank == 0 and line is not None:
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_port_sample(args.n, its64, os.cpu_count() or 1)
+            line["cpu_baseline"] = cpu_port_sample(args.n, os.cpu_count() or 1)
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

@@ -397,7 +397,7 @@ static int apply_common(helm3d_ctx *c, const double *x, double *y, int which) {
     if (rc) return rc;
     rc = ya.copy_out(y, c->N);
     if (rc) return rc;
-    return cuda_check(c, cudaStreamSynchronize(c->stream), "apply");
+    return check_status(c);
 }
 
 int helm3d_apply_op(helm3d_ctx *c, const double *x, double *y) { return apply_common(c, x, y, 0); }
@@ -426,7 +426,7 @@ int helm3d_apply_prec_batch(helm3d_ctx *c, const double *x, double *y, int nrhs,
     if (rc) return rc;
     rc = ya.copy_out(y, cnt);
     if (rc) return rc;
-    return cuda_check(c, cudaStreamSynchronize(c->stream), "apply_prec_batch");
+    return check_status(c);
 }
 
 int helm3d_misfit_grad(helm3d_ctx *c, const double *f, int nsrc, const long long *recv, int nrecv, const double *data,

@@ -425,5 +425,9 @@ int ensure_krylov(helm3d_ctx *c, int m, int R);
 int set_error(helm3d_ctx *c, int code, const std::string &msg);
 bool is_device_ptr(const void *p);   // device or managed memory
 int cuda_check(helm3d_ctx *c, cudaError_t e, const char *what);
+// Reads the context's device status word after the stream's work: a bounded
+// wait that expired (bits 1, 2) or a failed index check (bit 3) in a kernel
+// -> HELM3D_ERR_CUDA.  Synchronizes the stream; allocates nothing.
+int check_status(helm3d_ctx *c);
 void build_fft_plan(int n, FftPlan &plan, std::vector<zc> &tables);
 }  // namespace h3d

@@ -22,7 +22,11 @@
 // stream capture.  All calls share the array and it keeps the last call's
 // contents; every call overwrites all planes it reads, so nothing needs
 // clearing.  Calls whose work overlaps on the GPU (different streams or
-// contexts at the same time) race on the array.
+// contexts at the same time) race on the array.  The address is cached per
+// device ordinal for the life of the process: after cudaDeviceReset (or
+// anything else that re-creates the device's primary context) the cached
+// address is stale, and this entry point must not be used on that device
+// until the process restarts.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -52,8 +56,17 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
         return set_error(c, HELM3D_ERR_ARG,
                          "apply_prec_noalloc: nx*ny*nz*" + std::to_string(c->c64 ? 8 : 16) + " = " +
                              std::to_string(need) + " bytes of planes exceed the 8 MiB static scratch");
-    if (!is_device_ptr(x) || !is_device_ptr(y))
-        return set_error(c, HELM3D_ERR_ARG, "apply_prec_noalloc takes device pointers only");
+    for (const void *p : {(const void *)x, (const void *)y}) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(c, HELM3D_ERR_ARG, "apply_prec_noalloc takes device pointers only");
+        }
+        if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+            return set_error(c, HELM3D_ERR_ARG, "apply_prec_noalloc takes device pointers only");
+        if (at.type == cudaMemoryTypeDevice && at.device != c->device)
+            return set_error(c, HELM3D_ERR_ARG, "apply_prec_noalloc: x and y must be on the context's device");
+    }
     void *scratch = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_mu);
@@ -92,5 +105,7 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
                                       nullptr, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: inverse FFT launch");
     c->launches += 3;
-    return cuda_check(c, cudaStreamSynchronize(c->stream), "apply_prec_noalloc");
+    // a bounded wait that expired in the sweep or a tensor-core z-transform
+    // leaves y invalid and sets a status bit: reported, not returned as OK
+    return check_status(c);
 }

@@ -355,7 +355,7 @@ static int norms(helm3d_ctx *c, const VecBatch &x, int R, bool phys, double2 *ou
     });
 }
 
-static int check_status(helm3d_ctx *c) {
+int check_status(helm3d_ctx *c) {
     int st = 0;
     RC(cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status"));
     RC(cuda_check(c, cudaStreamSynchronize(c->stream), "status sync"));

@@ -69,6 +69,17 @@ __device__ __forceinline__ const cplx<R> *stage_src(const SweepK<R> &a, int kz, 
 // symmetric (every coupling is alpha(node) alpha(half node) / h^2), so the
 // same factor serves; the input is scaled and conjugated where it is loaded
 // and the output where it is stored.
+// The producer lane waits (bounded) for its last copies to land before it
+// returns, so that no bulk copy into this CTA's shared memory is still in
+// flight when the CTA can exit: the final use of each of the last
+// min(nstage, issued) ring slots.
+__device__ __forceinline__ void sweep_drain(uint64_t *full, int nstage, long issued) {
+    for (long k = 1; k <= nstage && k <= issued; k++) {
+        const long seq = issued - k;
+        mbar_wait_bounded_cta(smem_u32(&full[seq % nstage]), (uint32_t)((seq / nstage) & 1), kSweepWaitLimit);
+    }
+}
+
 template <typename R, bool ADJ>
 __device__ __forceinline__ cplx<R> adj_in(const SweepK<R> &a, int line, int i, cplx<R> f) {
     if (!ADJ) return f;
@@ -112,13 +123,14 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
     if (warp == kSweepConsumerWarps) {
         // producer warp: one lane streams every stage of the chain
         if (lane == 0) {
-            bool dead = false;
-            for (long seq = 0; seq < nseq; seq++) {
+            long seq = 0;
+            for (; seq < nseq; seq++) {
                 const int s = (int)(seq % a.nstage);
                 const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
-                if (!dead && !mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, kSweepWaitLimit)) {
-                    dead = true;
+                if (!mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, kSweepWaitLimit)) {
+                    // stop issuing: the consumers' bounded waits on full[] expire in turn
                     atomicOr(a.status, 4);
+                    break;
                 }
                 int rows;
                 const Cx *src = stage_src(a, kz, seq, cpl, &rows);
@@ -126,6 +138,7 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
                 mbar_expect_tx(&full[s], bytes);
                 bulk_g2s(ring + (size_t)s * (a.stage_bytes / sizeof(Cx)), src, bytes, &full[s]);
             }
+            sweep_drain(full, a.nstage, seq);
         }
         return;
     }
@@ -259,13 +272,14 @@ __global__ void __launch_bounds__((CW + 1) * 32, 1) sweep_tiled_kernel(SweepK<fl
 
     if (warp == CW) {
         if (lane == 0) {
-            bool dead = false;
-            for (long seq = 0; seq < nseq; seq++) {
+            long seq = 0;
+            for (; seq < nseq; seq++) {
                 const int s = (int)(seq % a.nstage);
                 const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
-                if (!dead && !mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, kSweepWaitLimit)) {
-                    dead = true;
+                if (!mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, kSweepWaitLimit)) {
+                    // stop issuing: the consumers' bounded waits on full[] expire in turn
                     atomicOr(a.status, 4);
+                    break;
                 }
                 int rows;
                 const Cx *src = stage_src(a, kz, seq, cpl, &rows);
@@ -273,6 +287,7 @@ __global__ void __launch_bounds__((CW + 1) * 32, 1) sweep_tiled_kernel(SweepK<fl
                 mbar_expect_tx(&full[s], bytes);
                 bulk_g2s(ring + (size_t)s * (a.stage_bytes / sizeof(Cx)), src, bytes, &full[s]);
             }
+            sweep_drain(full, a.nstage, seq);
         }
         return;
     }

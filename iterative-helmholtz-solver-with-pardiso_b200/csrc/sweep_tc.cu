@@ -196,8 +196,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             // backward lines ny-2..0, MC rows m per chunk
             RingPos rp;
             int t = 0, c = 0;
+            long issued = 0;
             for (long seq = 0; seq < nseq; seq++) {
                 if (seq >= a.nstage) wait(&raw_empty[rp.slot], rp.phase ^ 1u);
+                if (dead) break;   // stop issuing once a wait has expired
                 const int line = t < ny ? t : 2 * ny - 2 - t;
                 const int m0 = c * MC;
                 const int rows = min(MC, n - m0);
@@ -206,6 +208,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                 mbar_expect_tx(&raw_full[rp.slot], bytes);
                 bulk_g2s(ring + (size_t)rp.slot * a.stage_bytes, src, bytes, &raw_full[rp.slot]);
                 rp.next(a.nstage);
+                issued++;
                 if (++c == cpl) {
                     c = 0;
                     t++;
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             }
             // the copies still in flight land before the CTA exits: the
             // last use of every slot (rp is one past the final use)
-            for (int k = 0; k < a.nstage && k < nseq; k++) {
+            for (int k = 0; k < a.nstage && k < issued; k++) {
                 int sl = rp.slot - 1 - k;
                 uint32_t ph = rp.phase;
                 if (sl < 0) {

@@ -3,8 +3,11 @@
 The solver itself is libhelm3d.so (CUDA kernels for sm_100a + C++ host);
 this module only marshals arguments.  Vectors are complex128 arrays laid out
 (nz, ny, nx); NumPy arrays are passed as host pointers (the library copies
-them), torch CUDA tensors as device pointers.  There is no fallback: if the
-shared library is missing, importing this module fails.
+them), torch CUDA tensors as device pointers.  There is no fallback: the
+shared library is loaded on first use (``lib``, ``load()``), and if it is
+missing that first use raises ImportError.  Importing the package alone
+loads nothing, so its pure-Python modules (``helm3d.media``,
+``helm3d.formats``) can be used by CPU-only code without the CUDA library.
 """
 from __future__ import annotations
 
@@ -18,10 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 # with -DHELM3D_CHECKS, whose kernels check their indices)
 LIB_PATH = os.environ.get("HELM3D_LIB") or os.path.join(_HERE, "libhelm3d.so")
 
-if not os.path.exists(LIB_PATH):
-    raise ImportError(f"helm3d: {LIB_PATH} is not built (run `make` in {os.path.dirname(_HERE)})")
-
-lib = ctypes.CDLL(LIB_PATH)
+_cdll = None
 
 MODE_R, MODE_N = 0, 1
 PREC_C128, PREC_C64 = 0, 1
@@ -82,10 +82,32 @@ _sig = {
     "helm3d_last_error": (ctypes.c_char_p, [_vp]),
     "helm3d_destroy": (ctypes.c_int, [_vp]),
 }
-for _name, (_res, _args) in _sig.items():
-    _f = getattr(lib, _name)
-    _f.restype = _res
-    _f.argtypes = _args
+
+
+def load() -> ctypes.CDLL:
+    """Load libhelm3d.so (once) and declare the C signatures; raises
+    ImportError if the library is not built."""
+    global _cdll
+    if _cdll is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"helm3d: {LIB_PATH} is not built (run `make` in {os.path.dirname(_HERE)})")
+        d = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _sig.items():
+            f = getattr(d, name)
+            f.restype = res
+            f.argtypes = args
+        _cdll = d
+    return _cdll
+
+
+class _Lib:
+    """``helm3d.lib``: the CDLL, loaded on first attribute access."""
+
+    def __getattr__(self, name):
+        return getattr(load(), name)
+
+
+lib = _Lib()
 
 EXPORTS = tuple(_sig)
 

@@ -4,7 +4,7 @@ tests can check file names and printf formatting byte for byte.
 
 Run in a container that has the reference checked out:
 
-    python tests/golden/make_formats_golden.py /root/reference
+    python tests/golden/make_formats_golden.py [reference checkout, default $HELM3D_REFERENCE or /root/reference]
 
 writes tests/golden/formats_golden.json.
 """
@@ -39,4 +39,4 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HELM3D_REFERENCE", "/root/reference"))

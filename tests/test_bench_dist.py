@@ -1,6 +1,7 @@
 """The multi-rank plumbing of bench.py on CPU (gloo, world size 2): the
 max-over-ranks timing reduction, and the reference arm under torchrun
-(rank 0 prints one JSON line, the other rank exits 0 without work)."""
+(rank 0 prints one JSON line, the other rank exits 0 without work, and the
+arm loads none of the repository's native libraries)."""
 import json
 import os
 import socket
@@ -61,3 +62,6 @@ def test_reference_arm_under_torchrun_two_ranks():
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["higher_is_better"] is False
     assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["value"] > 0
+    # the reference arm runs the CPU port only: none of this repository's native code is mapped
+    assert d["native_libs_loaded"] == []
+    assert d["config"]["n"] == 32 and d["iterations"] > 0
