@@ -456,13 +456,14 @@ template <size_t K> static void shapes_for(const FactorShape (&t)[K], int n, int
     }
 }
 
-// After the register shapes, complex64 blocks of n <= 128 have one more
-// variant: the tensor-core factor (factor_tc.cu).
+// After the register shapes, complex64 blocks have one more variant: the
+// tensor-core factor, one CTA per kz for n <= 128 (factor_tc.cu), a CTA pair
+// per kz for 128 < n <= 224 (factor_tc2.cu).
 int factor_variants(bool c64, int n) {
     int first, count;
     if (c64) shapes_for(kShapes64, n, first, count);
     else shapes_for(kShapes128, n, first, count);
-    return count + (factor_tc_supported(c64, n) ? 1 : 0);
+    return count + ((factor_tc_supported(c64, n) || factor_tc2_supported(c64, n)) ? 1 : 0);
 }
 
 bool factor_supported(bool c64, int n) { return n >= 1 && factor_variants(c64, n) > 0; }
@@ -473,6 +474,7 @@ int launch_factor(bool c64, const FactorArgs &fa, cudaStream_t s, int variant) {
     else shapes_for(kShapes128, fa.n, first, count);
     if (count == 0) return HELM3D_ERR_ARG;
     if (variant == count && factor_tc_supported(c64, fa.n)) return launch_factor_tc(fa, s);
+    if (variant == count && factor_tc2_supported(c64, fa.n)) return launch_factor_tc2(fa, s);
     if (variant < 0 || variant >= count) variant = 0;
     return (c64 ? kShapes64 : kShapes128)[first + variant].fn(fa, s);
 }

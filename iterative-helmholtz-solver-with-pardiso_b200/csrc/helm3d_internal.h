@@ -101,6 +101,10 @@ int factor_variants(bool c64, int n);
 // the tensor-core factor (complex64, n <= 128): the last factor variant
 bool factor_tc_supported(bool c64, int n);
 int launch_factor_tc(const FactorArgs &a, cudaStream_t s);
+// the tensor-core factor on a CTA pair per kz (complex64, 128 < n <= 224):
+// the last factor variant of those block sizes
+bool factor_tc2_supported(bool c64, int n);
+int launch_factor_tc2(const FactorArgs &a, cudaStream_t s);
 bool factor_supported(bool c64, int n);
 
 // Forward/backward block sweep over y-lines for every kz and all R

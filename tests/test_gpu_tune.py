@@ -13,13 +13,15 @@ from oracle import mode_n
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("prec,nx,nv", [(1, 128, 3), (1, 100, 3), (1, 40, 2), (1, 17, 2), (1, 200, 2), (1, 250, 2),
-                                         (0, 200, 1), (0, 128, 1)])
+@pytest.mark.parametrize("prec,nx,nv", [(1, 128, 3), (1, 100, 3), (1, 40, 2), (1, 17, 2), (1, 200, 3), (1, 201, 3),
+                                         (1, 224, 3), (1, 129, 2), (1, 250, 2), (0, 200, 1), (0, 128, 1)])
 def test_factor_shapes(prec, nx, nv, monkeypatch):
     """Block sizes 128 (one CTA or a pair per kz), 200 (padded to 224: 4- or
     8-CTA clusters) and 250 (padded to 256) against the oracle, every shape;
     complex64 blocks of n <= 128 (128, 100, 40, 17: full and partial panels)
-    also with the tensor-core factor (the last variant)."""
+    also with the tensor-core factor, and of 128 < n <= 224 (129, 200, 201,
+    224: even and odd splits over the CTA pair, full and partial last
+    panels) with the CTA-pair tensor-core factor (the last variant)."""
     p = small_problem(nx, 10, 8, pml=3, seed=nx + prec)
     on = mode_n.setup(p, beta_prec=0.25)
     v = rand_c(p.shape, seed=3)
