@@ -459,14 +459,21 @@ def run_kernels(args):
     Gram-Schmidt and residual kernels) on the headline workload, with the
     algorithmic bytes and HBM fraction of each kernel family.  The solver
     holds only two Krylov vectors per source (about 4 GB on the device at
-    128^3), which keeps profiler captures of these kernels small."""
+    128^3), which keeps profiler captures of these kernels small.  --nz
+    shortens the z axis (fewer kz chains, the same block size) for captures
+    of a single kernel."""
     import torch
 
     import helm3d
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    p = workload(args.n, BATCH)
+    if args.nz and args.nz != args.n:
+        from helm3d import media
+        p = media.layered_medium(args.n, args.n, args.nz, 10.0, pml_for(min(args.n, args.nz)), 2024, ppw=8.0,
+                                 n_sources=BATCH)
+    else:
+        p = workload(args.n, BATCH)
     F = torch.from_numpy(np.stack([p.rhs(i) for i in range(BATCH)])).to(dev)
     U = torch.empty_like(F)
     grid = helm3d.grid_mode_n(p.nx, p.ny, p.nz, p.h, p.pml, p.omega)
@@ -490,7 +497,7 @@ def run_kernels(args):
     }
     peaks, peak_kind = read_peaks()
     peak = float(peaks["hbm_gbs"])
-    out = {"mode": "kernels", "workload": f"{p.nx}^3, {BATCH} sources, c64 preconditioner, PML eigenbasis",
+    out = {"mode": "kernels", "workload": f"{p.nx}x{p.ny}x{p.nz}, {BATCH} sources, c64 preconditioner, PML eigenbasis",
            "steps": args.steps, "peak_gbs": peak, "peak_source": peak_kind, "kernels": {}}
     for k, (ms, n) in prof.items():
         d = {"ms_total": round(ms, 4), "launches": int(n)}
@@ -856,6 +863,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5, help="timed e2e steps (at most --steps)")
     ap.add_argument("--arm-steps", type=int, default=1, help="timed steps of each comparison arm")
     ap.add_argument("--skip-arms", default="", help="comma-separated comparison arms to leave out")
+    ap.add_argument("--nz", type=int, default=0, help="--kernels: z points (default: the grid size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels", action="store_true",
                     help="per-kernel microbench: batched FGMRES(1) iterations instead of full solves")
