@@ -17,30 +17,33 @@
 // its own lanes) with its own copy of B (the real form of the panel's pivot
 // rows) in shared memory.
 //
-// Pivot steps across the pair.  At step k each warp of both CTAs reduces its
-// candidates to one 32-bit key (redux.sync.max): the top 24 bits of
-// |re| + |im| of column k and 255 - row, so that the largest magnitude wins
-// and ties go to the lowest row (magnitudes equal to 2^-15 relative count as
-// ties).  The warp's winning lane writes the key and its row's 16 panel
-// entries into the step's slot in the shared memory of both CTAs, and one
-// lane arrives on both CTAs' step barrier (8 arrivals per phase: 4 warps
-// per CTA); every row thread then picks the largest of the 8 keys.  The
-// slots alternate by phase parity: a slot is rewritten two phases later,
-// after every warp of both CTAs has arrived once more, so after every reader
-// is done with it.  The same barrier carries one more phase per panel, after
-// which the panel's pivot rows (written by their owners into both CTAs'
-// shared memory) are complete in both CTAs.
+// Panels.  A panel's 16 pivot steps touch only the panel's columns, n x 16
+// complex values, so both CTAs run all of them, on the whole panel, with the
+// same arithmetic and therefore the same pivots: at the start of a panel
+// each CTA sends its rows' panel entries into both CTAs' shared memory
+// (cluster stores, then one arrive per warp on the peer's barrier, release
+// at cluster scope), and thread t of each CTA takes physical rows t and
+// t + 128 into registers.  A step is then local to the CTA: the pivot
+// candidate of each warp is one 32-bit key (redux.sync.max): the top 24
+// bits of |re| + |im| and 255 - row, so that the largest magnitude wins and
+// ties go to the lowest row (magnitudes equal to 2^-15 relative count as
+// ties); the warps' keys and winning rows go through shared memory slots
+// alternating by step parity, one CTA barrier per step.  After the steps
+// each CTA keeps X and the panel of its own rows, and the panel's pivot
+// rows (their other columns live in their owner's TMEM) are exchanged the
+// same way as the panel entries.  Two exchanges between the CTAs per panel.
 //
 // Frames.  The block is never unscrambled.  Physical row g of M holds
 // logical row rho[g], physical column q logical column kap[q].  In-place
 // Gauss-Jordan without row exchanges on A[g][q] = S[rho[g]][kap[q]] leaves
 // M[g][q] = S^{-1}[kap[sigma[g]]][rho[perm[q]]] with perm[k] the pivot row
-// of step k and sigma its inverse, so the next frame is rho' = kap o sigma,
-// kap' = rho o perm.  The next Schur complement is formed in place in that
-// frame, M <- D[rho'][kap'] - c M (D tridiagonal: three entries per row, at
-// the physical columns kapinv of logical columns i-1, i, i+1), and G_j^T is
-// written to global memory as G^T[kap'[q]][rho'[g]] = M[g][q] (the 8-byte
-// stores of a warp scatter within one row of G^T and merge in L2).
+// of step k and sigma its inverse (the step of row g), so the next frame is
+// rho' = kap o sigma, kap' = rho o perm.  The next Schur complement is
+// formed in place in that frame, M <- D[rho'][kap'] - c M (D tridiagonal:
+// three entries per row, at the physical columns kapinv of logical columns
+// i-1, i, i+1), and G_j^T is written to global memory as
+// G^T[kap'[q]][rho'[g]] = M[g][q] (the 8-byte stores of a warp scatter
+// within one row of G^T and merge in L2).
 //
 // Look-ahead.  After panel p's pivot rows are in place, the MMA warp first
 // updates the next panel's 16 columns (commit: next_ready), then every other
@@ -66,7 +69,7 @@
 namespace h3d {
 
 constexpr int kF2RowWarps = 4;
-constexpr int kF2Warps = kF2RowWarps * 2;        // row warps of the pair
+constexpr int kF2RowThreads = kF2RowWarps * 32;
 constexpr int kF2Threads = (kF2RowWarps + 1) * 32;
 constexpr int kF2B = 16;                         // panel width
 constexpr int kF2MaxN = 224;                     // 2 ncol + 64 X columns <= 512
@@ -81,25 +84,22 @@ struct F2K {
     int *status;
 };
 
-// one warp's candidate of a pivot step: its key and its row's panel entries
-struct __align__(16) F2Slot {
-    uint32_t key, pad[3];
-    float4 v[kF2B / 2];
-};
-
 struct F2Smem {
     float *Bhi, *Blo;   // [2 kF2MaxN rows][2 kF2B] canonical K-major each
     float2 *Y;          // [kF2B][kF2MaxN]: the panel's pivot rows
-    F2Slot *slot;       // [2][kF2Warps]
+    float2 *PF;         // [kF2MaxN][kF2B]: the panel's entries of every row
+    float2 *wrow;       // [2][kF2RowWarps][kF2B]: each warp's candidate row, by step parity
+    uint32_t *wkey;     // [2][kF2RowWarps]
     int *rho, *kap;     // [2][kF2Tab] each: the frame, double-buffered by line
-    int *kapinv, *perm, *sigma;   // [kF2Tab]
-    uint64_t *stepbar, *b_ready, *next_ready, *rest_done, *fin;
+    int *kapinv, *perm, *stepof;   // [kF2Tab]; stepof[g]: the step that pivoted row g
+    uint64_t *pan_bar, *y_bar, *b_ready, *next_ready, *rest_done, *fin;
     uint32_t *tslot;
 };
 
 constexpr size_t kF2BBytes = sizeof(float) * 2 * kF2MaxN * 2 * kF2B;
-constexpr size_t kF2SmemBytes = 2 * kF2BBytes + sizeof(float2) * kF2B * kF2MaxN + sizeof(F2Slot) * 2 * kF2Warps +
-                                sizeof(int) * 7 * kF2Tab + 5 * sizeof(uint64_t) + 16 + 1024;
+constexpr size_t kF2SmemBytes = 2 * kF2BBytes + 2 * sizeof(float2) * kF2B * kF2MaxN +
+                                sizeof(float2) * 2 * kF2RowWarps * kF2B + sizeof(uint32_t) * 2 * kF2RowWarps +
+                                sizeof(int) * 7 * kF2Tab + 6 * sizeof(uint64_t) + 16 + 1024 + 16;
 
 __device__ __forceinline__ F2Smem f2_carve(unsigned char *raw) {
     F2Smem s;
@@ -107,25 +107,28 @@ __device__ __forceinline__ F2Smem f2_carve(unsigned char *raw) {
     s.Bhi = reinterpret_cast<float *>(b);
     s.Blo = s.Bhi + 2 * kF2MaxN * 2 * kF2B;
     s.Y = reinterpret_cast<float2 *>(s.Blo + 2 * kF2MaxN * 2 * kF2B);
-    s.slot = reinterpret_cast<F2Slot *>(s.Y + kF2B * kF2MaxN);
-    s.rho = reinterpret_cast<int *>(s.slot + 2 * kF2Warps);
+    s.PF = s.Y + kF2B * kF2MaxN;
+    s.wrow = s.PF + kF2MaxN * kF2B;
+    s.wkey = reinterpret_cast<uint32_t *>(s.wrow + 2 * kF2RowWarps * kF2B);
+    s.rho = reinterpret_cast<int *>(s.wkey + 2 * kF2RowWarps);
     s.kap = s.rho + 2 * kF2Tab;
     s.kapinv = s.kap + 2 * kF2Tab;
     s.perm = s.kapinv + kF2Tab;
-    s.sigma = s.perm + kF2Tab;
-    uintptr_t m = reinterpret_cast<uintptr_t>(s.sigma + kF2Tab);
+    s.stepof = s.perm + kF2Tab;
+    uintptr_t m = reinterpret_cast<uintptr_t>(s.stepof + kF2Tab);
     m = (m + 15) & ~uintptr_t(15);
-    s.stepbar = reinterpret_cast<uint64_t *>(m);
-    s.b_ready = s.stepbar + 1;
-    s.next_ready = s.stepbar + 2;
-    s.rest_done = s.stepbar + 3;
-    s.fin = s.stepbar + 4;
-    s.tslot = reinterpret_cast<uint32_t *>(s.stepbar + 5);
+    s.pan_bar = reinterpret_cast<uint64_t *>(m);
+    s.y_bar = s.pan_bar + 1;
+    s.b_ready = s.pan_bar + 2;
+    s.next_ready = s.pan_bar + 3;
+    s.rest_done = s.pan_bar + 4;
+    s.fin = s.pan_bar + 5;
+    s.tslot = reinterpret_cast<uint32_t *>(s.pan_bar + 6);
     return s;
 }
 
 __device__ __forceinline__ void f2_row_barrier() {
-    asm volatile("bar.sync 1, %0;" ::"n"(kF2RowWarps * 32) : "memory");
+    asm volatile("bar.sync 1, %0;" ::"n"(kF2RowThreads) : "memory");
 }
 
 __device__ __forceinline__ void st_cluster_v4f32(uint32_t addr, float4 v) {
@@ -150,6 +153,14 @@ __device__ __forceinline__ F2Drow f2_drow(const F2K &a, int line, int i, float2 
     return d;
 }
 
+// pivot key of an entry of row g (0 when the row is not a candidate)
+__device__ __forceinline__ uint32_t f2_key(float2 v, bool cand, int g) {
+    if (!cand) return 0u;
+    const float av = fabsf(v.x) + fabsf(v.y);
+    if (!(av == av)) return 0u;
+    return (__float_as_uint(av) & 0xFFFFFF00u) | (uint32_t)(255 - g);
+}
+
 __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     F2Smem sm = f2_carve(smem_raw);
@@ -170,10 +181,11 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
         sm.kap[q] = q;
         sm.kapinv[q] = q;
         sm.perm[q] = 0;
-        sm.sigma[q] = 0;   // every entry stays a valid index, even for a failed step
+        sm.stepof[q] = -1;   // not pivoted in this line yet
     }
     if (tid == 0) {
-        mbar_init(sm.stepbar, kF2Warps);
+        mbar_init(sm.pan_bar, kF2RowWarps);   // the peer's 4 row warps
+        mbar_init(sm.y_bar, kF2RowWarps);
         mbar_init(sm.b_ready, kF2RowWarps);
         mbar_init(sm.next_ready, 1);
         mbar_init(sm.rest_done, 1);
@@ -187,6 +199,12 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
     bool dead = false;
     auto wait_cta = [&](uint64_t *bar, uint32_t parity) {
         if (!dead && !mbar_wait_bounded_cta(smem_u32(bar), parity, kF2WaitLimit)) {
+            dead = true;
+            atomicOr(a.status, 2);
+        }
+    };
+    auto wait_cluster = [&](uint64_t *bar, uint32_t parity) {
+        if (!dead && !mbar_wait_bounded_cluster(smem_u32(bar), parity, kF2WaitLimit)) {
             dead = true;
             atomicOr(a.status, 2);
         }
@@ -240,24 +258,18 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
     } else {
         // ----------------------------------------------------- row threads
         const int t = tid;                       // TMEM lane t
-        const int g = gbase + t;                 // physical row
+        const int g = gbase + t;                 // this CTA's physical row in lane t
         const bool valid = t < nr;
-        const int wg = (int)rank * kF2RowWarps + warp;
+        const int g1 = t + kF2RowThreads;        // the second row of the panel steps (g0 = t)
+        const bool has1 = g1 < n;
         const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
-        const uint32_t bar_loc = mapa_u32(smem_u32(sm.stepbar), rank);
-        const uint32_t bar_peer = mapa_u32(smem_u32(sm.stepbar), peer);
-        const uint32_t slot_peer = mapa_u32(smem_u32(sm.slot), peer);
+        const uint32_t panbar_peer = mapa_u32(smem_u32(sm.pan_bar), peer);
+        const uint32_t ybar_peer = mapa_u32(smem_u32(sm.y_bar), peer);
+        const uint32_t pf_peer = mapa_u32(smem_u32(sm.PF), peer);
         const uint32_t y_peer = mapa_u32(smem_u32(sm.Y), peer);
         const float2 kzv = a.kz2[kz];
-        uint32_t xph = 0, ph_next = 0, ph_rest = 0;
+        uint32_t ph_pan = 0, ph_y = 0, ph_next = 0, ph_rest = 0;
         int cur = 0;
-        auto xwait = [&]() {
-            if (!dead && !mbar_wait_bounded_cluster(smem_u32(sm.stepbar), xph, kF2WaitLimit)) {
-                dead = true;
-                atomicOr(a.status, 2);
-            }
-            xph ^= 1u;
-        };
 
         // ---- S_0 = D_0 (identity frame)
         {
@@ -283,62 +295,69 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
         }
 
         for (int line = 0; line < ny; line++) {
-            bool used = false;
-            int my_step = -1;
+            bool used0 = false, used1 = false;
             for (int p = 0; p < npan; p++) {
                 const int k0 = p * kF2B, bl = min(kF2B, n - k0);
                 if (p > 0) {
                     wait_cta(sm.next_ready, ph_next);
                     ph_next ^= 1u;
                 }
-                // ---- the panel's columns into registers
-                float2 P[kF2B];
+                // ---- this CTA's rows of the panel into both CTAs' PF
                 {
                     float f[32];
                     tc_fence_after();
                     tmem_ld32_nowait(trow + (uint32_t)(2 * k0), f);
                     tmem_wait_ld(f);
+                    if (valid) {
+                        float4 *dst = reinterpret_cast<float4 *>(sm.PF + (size_t)g * kF2B);
+                        const uint32_t rdst = pf_peer + (uint32_t)(g * kF2B * sizeof(float2));
 #pragma unroll
-                    for (int e = 0; e < kF2B; e++) P[e] = make_float2(f[2 * e], f[2 * e + 1]);
-                }
-                // ---- the panel's pivot steps across the pair
-#pragma unroll
-                for (int kk = 0; kk < kF2B; kk++) {
-                    if (kk >= bl) break;
-                    const int k = k0 + kk, sl = (int)(xph & 1u);
-                    const float2 v = P[kk];
-                    uint32_t key = 0;
-                    if (valid && !used) {
-                        const float av = fabsf(v.x) + fabsf(v.y);
-                        if (av == av) key = (__float_as_uint(av) & 0xFFFFFF00u) | (uint32_t)(255 - g);
-                    }
-                    const uint32_t kw = __reduce_max_sync(0xffffffffu, key);
-                    const bool win = kw != 0u ? key == kw : lane == 0;
-                    if (win) {
-                        F2Slot *s = sm.slot + sl * kF2Warps + wg;
-                        const uint32_t rs = slot_peer + (uint32_t)((sl * kF2Warps + wg) * sizeof(F2Slot));
-                        s->key = kw;
-                        st_cluster_u32(rs, kw);
-                        if (kw != 0u) {
-#pragma unroll
-                            for (int e = 0; e < kF2B / 2; e++) {
-                                const float4 q4 = make_float4(P[2 * e].x, P[2 * e].y, P[2 * e + 1].x, P[2 * e + 1].y);
-                                s->v[e] = q4;
-                                st_cluster_v4f32(rs + 16u + 16u * (uint32_t)e, q4);
-                            }
+                        for (int e = 0; e < kF2B / 2; e++) {
+                            const float4 q4 = make_float4(f[4 * e], f[4 * e + 1], f[4 * e + 2], f[4 * e + 3]);
+                            dst[e] = q4;
+                            st_cluster_v4f32(rdst + 16u * (uint32_t)e, q4);
                         }
                     }
                     __syncwarp();
-                    if (lane == 0) {
-                        mbar_arrive_cluster(bar_loc);
-                        mbar_arrive_cluster(bar_peer);
+                    if (lane == 0) mbar_arrive_cluster(panbar_peer);
+                }
+                f2_row_barrier();
+                wait_cluster(sm.pan_bar, ph_pan);
+                ph_pan ^= 1u;
+                float2 P0[kF2B], P1[kF2B];
+                {
+                    const float4 *s0 = reinterpret_cast<const float4 *>(sm.PF + (size_t)t * kF2B);
+                    const float4 *s1 = reinterpret_cast<const float4 *>(sm.PF + (size_t)(has1 ? g1 : t) * kF2B);
+#pragma unroll
+                    for (int e = 0; e < kF2B / 2; e++) {
+                        const float4 x0 = s0[e], x1 = s1[e];
+                        P0[2 * e] = make_float2(x0.x, x0.y);
+                        P0[2 * e + 1] = make_float2(x0.z, x0.w);
+                        P1[2 * e] = make_float2(x1.x, x1.y);
+                        P1[2 * e + 1] = make_float2(x1.z, x1.w);
                     }
-                    xwait();
-                    uint32_t kmax = 0;
+                }
+                // ---- the panel's pivot steps, in each CTA on the whole panel
+#pragma unroll
+                for (int kk = 0; kk < kF2B; kk++) {
+                    if (kk >= bl) break;
+                    const int k = k0 + kk, buf = k & 1;
+                    const uint32_t key0 = f2_key(P0[kk], !used0, t);
+                    const uint32_t key1 = f2_key(P1[kk], has1 && !used1, g1);
+                    const uint32_t key = key0 > key1 ? key0 : key1;
+                    const uint32_t kw = __reduce_max_sync(0xffffffffu, key);
+                    if (lane == 0) sm.wkey[buf * kF2RowWarps + warp] = kw;
+                    if (kw != 0u && key == kw) {
+                        float2 *w = sm.wrow + (size_t)(buf * kF2RowWarps + warp) * kF2B;
+#pragma unroll
+                        for (int e = 0; e < kF2B; e++) w[e] = key0 == kw ? P0[e] : P1[e];
+                    }
+                    f2_row_barrier();
+                    uint32_t kmax = sm.wkey[buf * kF2RowWarps];
                     int wsel = 0;
 #pragma unroll
-                    for (int w2 = 0; w2 < kF2Warps; w2++) {
-                        const uint32_t kk2 = sm.slot[sl * kF2Warps + w2].key;
+                    for (int w2 = 1; w2 < kF2RowWarps; w2++) {
+                        const uint32_t kk2 = sm.wkey[buf * kF2RowWarps + w2];
                         if (kk2 > kmax) {
                             kmax = kk2;
                             wsel = w2;
@@ -353,13 +372,9 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                         for (int e = 0; e < kF2B; e++) prow[e] = make_float2(0.f, 0.f);
                         if (t == 0 && rank == 0) atomicOr(a.status, 1);
                     } else {
-                        const F2Slot *s = sm.slot + sl * kF2Warps + wsel;
+                        const float2 *w = sm.wrow + (size_t)(buf * kF2RowWarps + wsel) * kF2B;
 #pragma unroll
-                        for (int e = 0; e < kF2B / 2; e++) {
-                            const float4 q4 = s->v[e];
-                            prow[2 * e] = make_float2(q4.x, q4.y);
-                            prow[2 * e + 1] = make_float2(q4.z, q4.w);
-                        }
+                        for (int e = 0; e < kF2B; e++) prow[e] = w[e];
                         const float2 pv = prow[kk];
                         if (pv.x == 0.f && pv.y == 0.f) {
                             if (t == 0 && rank == 0) atomicOr(a.status, 1);
@@ -372,49 +387,93 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                         }
                     }
                     if (t == 0) sm.perm[k] = r >= 0 ? r : 0;
-                    if (valid && g == r) {
+                    // row -= (c / pv) * pivot row, column k becomes -c / pv;
+                    // the pivot row is scaled by 1 / pv, its column k becomes 1 / pv
+                    if (t == r) {
 #pragma unroll
-                        for (int e = 0; e < kF2B; e++) P[e] = e == kk ? pinv : cmul(prow[e], pinv);
-                        used = true;
-                        my_step = k;
+                        for (int e = 0; e < kF2B; e++) P0[e] = e == kk ? pinv : cmul(prow[e], pinv);
+                        used0 = true;
+                        sm.stepof[t] = k;
                     } else {
-                        // row -= (c / pv) * pivot row; column k becomes -c / pv
-                        const float2 sfac = cmul(v, pinv);
+                        const float2 sfac = cmul(P0[kk], pinv);
 #pragma unroll
                         for (int e = 0; e < kF2B; e++)
-                            P[e] = e == kk ? make_float2(-sfac.x, -sfac.y) : cfms(sfac, prow[e], P[e]);
+                            if (e != kk) P0[e] = cfms(sfac, prow[e], P0[e]);
+                        P0[kk] = make_float2(-sfac.x, -sfac.y);
+                    }
+                    if (g1 == r) {
+#pragma unroll
+                        for (int e = 0; e < kF2B; e++) P1[e] = e == kk ? pinv : cmul(prow[e], pinv);
+                        used1 = true;
+                        sm.stepof[g1] = k;
+                    } else {
+                        const float2 sfac = cmul(P1[kk], pinv);
+#pragma unroll
+                        for (int e = 0; e < kF2B; e++)
+                            if (e != kk) P1[e] = cfms(sfac, prow[e], P1[e]);
+                        P1[kk] = make_float2(-sfac.x, -sfac.y);
                     }
                 }
+                // ---- the panel after its steps back into PF
+                {
+                    float4 *d0 = reinterpret_cast<float4 *>(sm.PF + (size_t)t * kF2B);
+                    float4 *d1 = reinterpret_cast<float4 *>(sm.PF + (size_t)(has1 ? g1 : t) * kF2B);
+#pragma unroll
+                    for (int e = 0; e < kF2B / 2; e++)
+                        d0[e] = make_float4(P0[2 * e].x, P0[2 * e].y, P0[2 * e + 1].x, P0[2 * e + 1].y);
+                    if (has1) {
+#pragma unroll
+                        for (int e = 0; e < kF2B / 2; e++)
+                            d1[e] = make_float4(P1[2 * e].x, P1[2 * e].y, P1[2 * e + 1].x, P1[2 * e + 1].y);
+                    }
+                }
+                f2_row_barrier();
 
-                // ---- the previous panel's trailing GEMM is done: X, the
-                // panel's own columns and its pivot rows can be written
+                // ---- the previous panel's trailing GEMM is done: X and the
+                // panel's own columns of this CTA's rows into TMEM
                 if (p > 0) {
                     wait_cta(sm.rest_done, ph_rest);
                     ph_rest ^= 1u;
                 }
                 tc_fence_after();
+                const int my_step = valid ? sm.stepof[g] : -1;
+                const bool piv = valid && my_step >= k0 && my_step < k0 + bl;
                 {
                     float xh[32], xl[32], f[32];
+                    const float4 *src = reinterpret_cast<const float4 *>(sm.PF + (size_t)(valid ? g : 0) * kF2B);
+#pragma unroll
+                    for (int e = 0; e < kF2B / 2; e++) {
+                        const float4 q4 = src[e];
+                        f[4 * e] = q4.x;
+                        f[4 * e + 1] = q4.y;
+                        f[4 * e + 2] = q4.z;
+                        f[4 * e + 3] = q4.w;
+                    }
+                    if (!valid) {
+#pragma unroll
+                        for (int e = 0; e < 32; e++) f[e] = 0.f;
+                    }
 #pragma unroll
                     for (int e = 0; e < kF2B; e++) {
                         float2 x = make_float2(0.f, 0.f);
                         if (e < bl) {
-                            x = P[e];
-                            if (my_step == k0 + e) x.x -= 1.f;
+                            x = make_float2(f[2 * e], f[2 * e + 1]);
+                            if (piv && my_step == k0 + e) x.x -= 1.f;
                         }
                         tf32_split_fast(x.x, xh[2 * e], xl[2 * e]);
                         tf32_split_fast(x.y, xh[2 * e + 1], xl[2 * e + 1]);
-                        f[2 * e] = P[e].x;
-                        f[2 * e + 1] = P[e].y;
                     }
                     tmem_st32(trow + kXhi, xh);
                     tmem_st32(trow + kXlo, xl);
                     tmem_st32(trow + (uint32_t)(2 * k0), f);
                     tmem_wait_st();
                 }
-                // ---- the panel's pivot rows (their values before its update,
-                // outside the panel) into Y of both CTAs
-                const bool piv = my_step >= k0 && my_step < k0 + bl;
+                // every read of this panel's PF is done before this CTA's
+                // pivot rows go out (the peer writes the next panel's PF only
+                // after it has them)
+                f2_row_barrier();
+                // ---- the panel's pivot rows of this CTA (their values before
+                // the panel's update, outside the panel) into Y of both CTAs
                 if (__any_sync(0xffffffffu, piv)) {
                     const int yr = piv ? my_step - k0 : 0;
                     float2 *yrow = sm.Y + (size_t)yr * kF2MaxN;
@@ -436,15 +495,14 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive_cluster(bar_loc);
-                    mbar_arrive_cluster(bar_peer);
-                }
-                xwait();
+                if (lane == 0) mbar_arrive_cluster(ybar_peer);
+                f2_row_barrier();
+                wait_cluster(sm.y_bar, ph_y);
+                ph_y ^= 1u;
                 // ---- B = real form of Y (rows 2j + c, K = 2kk + c'), hi and lo,
                 // 16-byte units in address order (row & 7, K quad, 8-row group)
 #pragma unroll 4
-                for (int u = t; u < 2 * ncol * (2 * kF2B / 4); u += kF2RowWarps * 32) {
+                for (int u = t; u < 2 * ncol * (2 * kF2B / 4); u += kF2RowThreads) {
                     const int rlo = u & 7, kq = (u >> 3) & 7, rg = u >> 6;
                     const int row = rg * 8 + rlo, j = row >> 1;
                     const int kk0 = 2 * kq;
@@ -472,16 +530,19 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
             tc_fence_after();
             f2_row_barrier();
             const int nxt = cur ^ 1;
-            int *rho = sm.rho + cur * kF2Tab, *kap = sm.kap + cur * kF2Tab;
+            const int *rho = sm.rho + cur * kF2Tab, *kap = sm.kap + cur * kF2Tab;
             int *rho2 = sm.rho + nxt * kF2Tab, *kap2 = sm.kap + nxt * kF2Tab;
-            for (int k = t; k < n; k += kF2RowWarps * 32) sm.sigma[sm.perm[k]] = k;
-            f2_row_barrier();
-            for (int q = t; q < n; q += kF2RowWarps * 32) {
-                rho2[q] = kap[sm.sigma[q]];
+            for (int q = t; q < n; q += kF2RowThreads) {
+                int st = sm.stepof[q];
+                st = (st >= 0 && st < n) ? st : 0;   // a failed step leaves rows unpivoted (status set)
+                rho2[q] = kap[st];
                 kap2[q] = rho[sm.perm[q]];
             }
             f2_row_barrier();
-            for (int q = t; q < n; q += kF2RowWarps * 32) sm.kapinv[kap2[q]] = q;
+            for (int q = t; q < n; q += kF2RowThreads) {
+                sm.kapinv[kap2[q]] = q;
+                sm.stepof[q] = -1;   // for the next line
+            }
             f2_row_barrier();
             cur = nxt;
 

@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
     // B_lo follows B_hi as further 8-row groups (FP16: half the bytes)
     float *Blo = Bhi + (size_t)NR * Kp / (F16 ? 2 : 1);
     const int vld = npad + 2;         // padded row of vst (bank spread across right-hand sides)
-    float2 *vst = reinterpret_cast<float2 *>(Bhi + 2 * (size_t)NR * Kp);   // [RR][vld]
+    float2 *vst = reinterpret_cast<float2 *>(Bhi + 2 * (size_t)NR * Kp / (F16 ? 2 : 1));   // [RR][vld]
     float *vmax = reinterpret_cast<float *>(vst + (size_t)RR * vld);       // F16: [4][RR]
     uint64_t *raw_full = reinterpret_cast<uint64_t *>(vmax + 4 * RR);
     uint64_t *raw_empty = raw_full + a.nstage;
@@ -633,7 +633,8 @@ static bool tc_shape(const SweepArgs &sa, int mc, TcShape &sh) {
     sh.MC = sh.f16 ? 32 : ((sh.MB == 2 || mc == 16) ? 16 : 32);
     sh.npad = ((sa.n + sh.MC - 1) / sh.MC) * sh.MC;
     sh.stage_bytes = (uint32_t)((((size_t)sh.MC * sa.ldg * 8) + 127) & ~(size_t)127);
-    const size_t bbytes = 2 * sizeof(float) * (size_t)(2 * sh.RR) * (2 * sh.npad);
+    // B hi and lo: tf32 words, or FP16 halves (half the bytes)
+    const size_t bbytes = 2 * sizeof(float) * (size_t)(2 * sh.RR) * (2 * sh.npad) / (sh.f16 ? 2 : 1);
     const size_t vbytes = sizeof(float2) * (size_t)sh.RR * (sh.npad + 2) + sizeof(float) * 4 * sh.RR;
     const size_t fixed = bbytes + vbytes + sizeof(uint64_t) * (2 * kTcBuf + 3) + 16;
     const size_t optin = device_info().smem_optin;
