@@ -337,20 +337,23 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                         P1[2 * e + 1] = make_float2(x1.z, x1.w);
                     }
                 }
-                // ---- the panel's pivot steps, in each CTA on the whole panel
-#pragma unroll
-                for (int kk = 0; kk < kF2B; kk++) {
-                    if (kk >= bl) break;
+                // ---- the panel's pivot steps, in each CTA on the whole panel.
+                // The rows rotate by one column per step, so that the column
+                // of step kk is always P[0] (no register indexed by kk): after
+                // step kk, P[e] holds panel column (kk + 1 + e) mod 16.
+#pragma unroll 1
+                for (int kk = 0; kk < bl; kk++) {
                     const int k = k0 + kk, buf = k & 1;
-                    const uint32_t key0 = f2_key(P0[kk], !used0, t);
-                    const uint32_t key1 = f2_key(P1[kk], has1 && !used1, g1);
+                    const uint32_t key0 = f2_key(P0[0], !used0, t);
+                    const uint32_t key1 = f2_key(P1[0], has1 && !used1, g1);
                     const uint32_t key = key0 > key1 ? key0 : key1;
                     const uint32_t kw = __reduce_max_sync(0xffffffffu, key);
                     if (lane == 0) sm.wkey[buf * kF2RowWarps + warp] = kw;
                     if (kw != 0u && key == kw) {
+                        // the winning row in panel column order
                         float2 *w = sm.wrow + (size_t)(buf * kF2RowWarps + warp) * kF2B;
 #pragma unroll
-                        for (int e = 0; e < kF2B; e++) w[e] = key0 == kw ? P0[e] : P1[e];
+                        for (int e = 0; e < kF2B; e++) w[(kk + e) & (kF2B - 1)] = key0 == kw ? P0[e] : P1[e];
                     }
                     f2_row_barrier();
                     uint32_t kmax = sm.wkey[buf * kF2RowWarps];
@@ -364,67 +367,61 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                         }
                     }
                     const int r = kmax != 0u ? 255 - (int)(kmax & 0xFFu) : -1;
+                    // the pivot row, rotated like the rows: prow[e] = column (kk + 1 + e) mod 16
+                    const float2 *w = sm.wrow + (size_t)(buf * kF2RowWarps + wsel) * kF2B;
                     float2 prow[kF2B];
-                    float2 pinv = make_float2(0.f, 0.f);
-                    if (r < 0) {
-                        // no finite candidate in the column: flagged, the block is invalid
 #pragma unroll
-                        for (int e = 0; e < kF2B; e++) prow[e] = make_float2(0.f, 0.f);
+                    for (int e = 0; e < kF2B; e++) prow[e] = w[(kk + 1 + e) & (kF2B - 1)];
+                    const float2 pv = w[kk];
+                    float2 pinv = make_float2(0.f, 0.f);
+                    if (r < 0 || (pv.x == 0.f && pv.y == 0.f)) {
+                        // no finite candidate, or an exactly zero pivot: flagged, the block is invalid
                         if (t == 0 && rank == 0) atomicOr(a.status, 1);
                     } else {
-                        const float2 *w = sm.wrow + (size_t)(buf * kF2RowWarps + wsel) * kF2B;
-#pragma unroll
-                        for (int e = 0; e < kF2B; e++) prow[e] = w[e];
-                        const float2 pv = prow[kk];
-                        if (pv.x == 0.f && pv.y == 0.f) {
-                            if (t == 0 && rank == 0) atomicOr(a.status, 1);
-                        } else {
-                            // 1 / pv with two divisions, scaled against overflow of |pv|^2
-                            const float sc = 1.f / fmaxf(fabsf(pv.x), fabsf(pv.y));
-                            const float ax = pv.x * sc, ay = pv.y * sc;
-                            const float rd = sc / (ax * ax + ay * ay);
-                            pinv = make_float2(ax * rd, -ay * rd);
-                        }
+                        // 1 / pv, scaled against overflow of |pv|^2
+                        const float sc = __frcp_rn(fmaxf(fabsf(pv.x), fabsf(pv.y)));
+                        const float ax = pv.x * sc, ay = pv.y * sc;
+                        const float rd = sc * __frcp_rn(ax * ax + ay * ay);
+                        pinv = make_float2(ax * rd, -ay * rd);
                     }
                     if (t == 0) sm.perm[k] = r >= 0 ? r : 0;
                     // row -= (c / pv) * pivot row, column k becomes -c / pv;
                     // the pivot row is scaled by 1 / pv, its column k becomes 1 / pv
+                    {
+                        const float2 s0 = cmul(P0[0], pinv), s1 = cmul(P1[0], pinv);
+#pragma unroll
+                        for (int e = 0; e < kF2B - 1; e++) {
+                            P0[e] = cfms(s0, prow[e], P0[e + 1]);
+                            P1[e] = cfms(s1, prow[e], P1[e + 1]);
+                        }
+                        P0[kF2B - 1] = make_float2(-s0.x, -s0.y);
+                        P1[kF2B - 1] = make_float2(-s1.x, -s1.y);
+                    }
                     if (t == r) {
 #pragma unroll
-                        for (int e = 0; e < kF2B; e++) P0[e] = e == kk ? pinv : cmul(prow[e], pinv);
+                        for (int e = 0; e < kF2B - 1; e++) P0[e] = cmul(prow[e], pinv);
+                        P0[kF2B - 1] = pinv;
                         used0 = true;
                         sm.stepof[t] = k;
-                    } else {
-                        const float2 sfac = cmul(P0[kk], pinv);
-#pragma unroll
-                        for (int e = 0; e < kF2B; e++)
-                            if (e != kk) P0[e] = cfms(sfac, prow[e], P0[e]);
-                        P0[kk] = make_float2(-sfac.x, -sfac.y);
                     }
                     if (g1 == r) {
 #pragma unroll
-                        for (int e = 0; e < kF2B; e++) P1[e] = e == kk ? pinv : cmul(prow[e], pinv);
+                        for (int e = 0; e < kF2B - 1; e++) P1[e] = cmul(prow[e], pinv);
+                        P1[kF2B - 1] = pinv;
                         used1 = true;
                         sm.stepof[g1] = k;
-                    } else {
-                        const float2 sfac = cmul(P1[kk], pinv);
-#pragma unroll
-                        for (int e = 0; e < kF2B; e++)
-                            if (e != kk) P1[e] = cfms(sfac, prow[e], P1[e]);
-                        P1[kk] = make_float2(-sfac.x, -sfac.y);
                     }
                 }
-                // ---- the panel after its steps back into PF
+                // ---- the panel after its steps back into PF, in column order
+                // (P[e] holds column (bl + e) mod 16)
                 {
-                    float4 *d0 = reinterpret_cast<float4 *>(sm.PF + (size_t)t * kF2B);
-                    float4 *d1 = reinterpret_cast<float4 *>(sm.PF + (size_t)(has1 ? g1 : t) * kF2B);
+                    float2 *d0 = sm.PF + (size_t)t * kF2B;
+                    float2 *d1 = sm.PF + (size_t)(has1 ? g1 : t) * kF2B;
 #pragma unroll
-                    for (int e = 0; e < kF2B / 2; e++)
-                        d0[e] = make_float4(P0[2 * e].x, P0[2 * e].y, P0[2 * e + 1].x, P0[2 * e + 1].y);
+                    for (int e = 0; e < kF2B; e++) d0[(bl + e) & (kF2B - 1)] = P0[e];
                     if (has1) {
 #pragma unroll
-                        for (int e = 0; e < kF2B / 2; e++)
-                            d1[e] = make_float4(P1[2 * e].x, P1[2 * e].y, P1[2 * e + 1].x, P1[2 * e + 1].y);
+                        for (int e = 0; e < kF2B; e++) d1[(bl + e) & (kF2B - 1)] = P1[e];
                     }
                 }
                 f2_row_barrier();
