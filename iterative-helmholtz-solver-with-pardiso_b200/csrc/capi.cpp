@@ -96,6 +96,18 @@ int validate(const helm3d_grid *g, const helm3d_opts *o) {
 
 }  // namespace
 
+// Start of a call that runs the operator or the preconditioner: refused
+// after a failed set-up or factor of this context (that error again), else
+// the device status word is cleared, so that a bounded wait that expired or
+// an index check that failed in an earlier call is not reported again (the
+// factor's own bits were reported when it ran).
+int h3d::begin_call(helm3d_ctx *c) {
+    if (c->factor_rc)
+        return set_error(c, c->factor_rc,
+                         std::string("the context's last set-up or factor failed: ") + helm3d_status_string(c->factor_rc));
+    return cuda_check(c, cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream), "status reset");
+}
+
 extern "C" {
 
 int helm3d_default_opts(helm3d_opts *o) {
@@ -229,13 +241,16 @@ int helm3d_set_medium(helm3d_ctx *c, const double *s2) {
     if (!c || !s2) return HELM3D_ERR_ARG;
     cudaSetDevice(c->device);
     int rc = ctx_setup_medium(c, s2, is_device_ptr(s2));
-    if (rc) return rc;
-    return ctx_factor(c);
+    if (!rc) rc = ctx_factor(c);
+    c->factor_rc = rc;
+    return rc;
 }
+
 
 static int solve_common(helm3d_ctx *c, const double *f, double *u, int nrhs, helm3d_stats *st, int which) {
     if (!c || !f || !u || nrhs < 1) return HELM3D_ERR_ARG;
     cudaSetDevice(c->device);
+    if (int rc = begin_call(c)) return rc;
     if (st) {
         st->iterations = 0;
         st->restarts = 0;
@@ -298,6 +313,7 @@ int helm3d_solve_group(helm3d_ctx *const *ctxs, int n, const double *const *f, d
         guard.cs.push_back(ctxs[i]);
         guard.saved.push_back(ctxs[i]->stream);
         ctxs[i]->stream = ctxs[0]->stream;
+        if (int rc = begin_call(ctxs[i])) return rc;
         if (stats) {
             helm3d_stats &s = stats[i];
             s.iterations = 0;
@@ -383,6 +399,7 @@ struct DevBuf {
 static int apply_common(helm3d_ctx *c, const double *x, double *y, int which) {
     if (!c || !x || !y) return HELM3D_ERR_ARG;
     cudaSetDevice(c->device);
+    if (int rc = begin_call(c)) return rc;
     VecArg xa(c, x, c->N, true, &c->d_f, &c->f_cap);
     if (xa.rc) return xa.rc;
     VecArg ya(c, y, c->N, false, &c->d_u, &c->u_cap);
@@ -411,6 +428,7 @@ int helm3d_apply_prec_batch(helm3d_ctx *c, const double *x, double *y, int nrhs,
     if (adjoint && c->opts.mode != HELM3D_MODE_N)
         return set_error(c, HELM3D_ERR_ARG, "adjoint preconditioner is mode N only");
     cudaSetDevice(c->device);
+    if (int rc = begin_call(c)) return rc;
     const size_t cnt = (size_t)c->N * nrhs;
     VecArg xa(c, x, cnt, true, &c->d_f, &c->f_cap);
     if (xa.rc) return xa.rc;
@@ -436,6 +454,7 @@ int helm3d_misfit_grad(helm3d_ctx *c, const double *f, int nsrc, const long long
         return set_error(c, HELM3D_ERR_ARG, "misfit_grad: bad arguments");
     if (c->opts.mode != HELM3D_MODE_N) return set_error(c, HELM3D_ERR_ARG, "misfit gradient is mode N only");
     cudaSetDevice(c->device);
+    if (int rc = begin_call(c)) return rc;
     if (st) {
         st->iterations = 0;
         st->restarts = 0;

@@ -27,8 +27,8 @@
 //   shared memory: G_{j-1} (row-major, padded rows) for the next Schur
 //     complement and the write-out; B = real form of M[R, :] (hi and lo,
 //     canonical no-swizzle K-major, 2 n_pad rows x 32); the gathered pivot
-//     rows; the per-warp pivot candidates (double-buffered by step parity,
-//     so one barrier per step); the pivot order.
+//     rows; the per-warp pivot keys and rows (double-buffered by step
+//     parity, so one barrier per step); the pivot order.
 // Warps 0-3: row threads; warp 4, one lane: MMA issuer.  Every wait is
 // bounded: on expiry bit 1 of *status is set and the kernel runs on without
 // waiting (results invalid), waits (bounded) for its MMAs, frees its TMEM
@@ -66,8 +66,7 @@ struct FtSmem {
     float *Bhi, *Blo;   // [2 kFtNP rows][2 kFtB] canonical each
     float2 *Y;          // [kFtB][kFtYld]
     float2 *wrow;       // [2][4][kFtB]
-    float *cval;        // [2][4]
-    int *cidx;          // [2][4]
+    uint32_t *ckey;     // [2][4]: each warp's pivot key, by step parity
     int *perm;          // [kFtNP]
     uint64_t *b_ready, *mma_done, *fin;
     uint32_t *tslot;
@@ -85,9 +84,8 @@ __device__ __forceinline__ FtSmem ft_carve(unsigned char *raw) {
     s.G = reinterpret_cast<float2 *>(s.Blo + 2 * kFtNP * 2 * kFtB);
     s.Y = s.G + kFtNP * kFtGld;
     s.wrow = s.Y + kFtB * kFtYld;
-    s.cval = reinterpret_cast<float *>(s.wrow + 2 * 4 * kFtB);
-    s.cidx = reinterpret_cast<int *>(s.cval + 8);
-    s.perm = s.cidx + 8;
+    s.ckey = reinterpret_cast<uint32_t *>(s.wrow + 2 * 4 * kFtB);
+    s.perm = reinterpret_cast<int *>(s.ckey + 8);
     uintptr_t b = reinterpret_cast<uintptr_t>(s.perm + kFtNP);
     b = (b + 15) & ~uintptr_t(15);
     s.b_ready = reinterpret_cast<uint64_t *>(b);
@@ -216,80 +214,81 @@ __global__ void __launch_bounds__(kFtThreads, 1) factor_tc_kernel(FactorTcK a) {
 #pragma unroll
                     for (int e = 0; e < kFtB; e++) P[e] = make_float2(f[2 * e], f[2 * e + 1]);
                 }
-                // ---- the panel's steps (CUDA cores)
-#pragma unroll
-                for (int kk = 0; kk < kFtB; kk++) {
-                    if (kk >= bl) break;
+                // ---- the panel's steps (CUDA cores), in a rolled loop: the row
+                // rotates by one column per step, so that the column of step kk
+                // is always P[0]; after step kk, P[e] holds panel column
+                // (kk + 1 + e) mod 16.  The pivot of a column is the candidate
+                // row with the largest key: the top 24 bits of |re| + |im| and
+                // 255 - row (ties, to 2^-15 relative, go to the lowest row),
+                // reduced per warp by redux.sync and across the 4 warps through
+                // shared memory slots alternating by step parity.
+#pragma unroll 1
+                for (int kk = 0; kk < bl; kk++) {
                     const int k = k0 + kk, buf = k & 1;
-                    const float2 v = P[kk];
-                    float best = (!used && t < n) ? fabsf(v.x) + fabsf(v.y) : -1.f;
-                    int bi = t;
-#pragma unroll
-                    for (int off = 16; off > 0; off >>= 1) {
-                        const float ov = __shfl_xor_sync(0xffffffffu, best, off);
-                        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                        if (ov > best || (ov == best && oi < bi)) {
-                            best = ov;
-                            bi = oi;
-                        }
+                    uint32_t key = 0;
+                    if (!used && t < n) {
+                        const float av = fabsf(P[0].x) + fabsf(P[0].y);
+                        if (av == av) key = (__float_as_uint(av) & 0xFFFFFF00u) | (uint32_t)(255 - t);
                     }
-                    if (lane == 0) {
-                        sm.cval[buf * 4 + warp] = best;
-                        sm.cidx[buf * 4 + warp] = bi;
-                    }
-                    if (t == bi) {
+                    const uint32_t kw = __reduce_max_sync(0xffffffffu, key);
+                    if (lane == 0) sm.ckey[buf * 4 + warp] = kw;
+                    if (kw != 0u && key == kw) {
 #pragma unroll
-                        for (int e = 0; e < kFtB; e++) sm.wrow[(buf * 4 + warp) * kFtB + e] = P[e];
+                        for (int e = 0; e < kFtB; e++) sm.wrow[(buf * 4 + warp) * kFtB + ((kk + e) & (kFtB - 1))] = P[e];
                     }
                     ft_row_barrier();
-                    float gb = sm.cval[buf * 4];
-                    int r = sm.cidx[buf * 4], wsel = 0;
+                    uint32_t kmax = sm.ckey[buf * 4];
+                    int wsel = 0;
 #pragma unroll
                     for (int w = 1; w < kFtRowWarps; w++) {
-                        const float ov = sm.cval[buf * 4 + w];
-                        const int oi = sm.cidx[buf * 4 + w];
-                        if (ov > gb || (ov == gb && oi < r)) {
-                            gb = ov;
-                            r = oi;
+                        const uint32_t o = sm.ckey[buf * 4 + w];
+                        if (o > kmax) {
+                            kmax = o;
                             wsel = w;
                         }
                     }
+                    const int r = kmax != 0u ? 255 - (int)(kmax & 0xFFu) : -1;
+                    // the pivot row, rotated like the rows: prow[e] = column (kk + 1 + e) mod 16
+                    const float2 *w = sm.wrow + (buf * 4 + wsel) * kFtB;
                     float2 prow[kFtB];
-                    float2 pinv = make_float2(0.f, 0.f);
-                    if (gb < 0.f) {
-                        // no pivot candidate (non-finite column): flagged, the block is invalid
-                        r = -1;
 #pragma unroll
-                        for (int e = 0; e < kFtB; e++) prow[e] = make_float2(0.f, 0.f);
+                    for (int e = 0; e < kFtB; e++) prow[e] = w[(kk + 1 + e) & (kFtB - 1)];
+                    const float2 pv = w[kk];
+                    float2 pinv = make_float2(0.f, 0.f);
+                    if (r < 0 || (pv.x == 0.f && pv.y == 0.f)) {
+                        // no finite candidate, or an exactly zero pivot: flagged, the block is invalid
                         if (t == 0) atomicOr(a.status, 1);
                     } else {
-#pragma unroll
-                        for (int e = 0; e < kFtB; e++) prow[e] = sm.wrow[(buf * 4 + wsel) * kFtB + e];
-                        const float2 pv = prow[kk];
-                        if (pv.x == 0.f && pv.y == 0.f) {
-                            if (t == 0) atomicOr(a.status, 1);
-                        } else {
-                            // 1 / pv with two divisions, scaled against overflow of |pv|^2
-                            const float sc = 1.f / fmaxf(fabsf(pv.x), fabsf(pv.y));
-                            const float ax = pv.x * sc, ay = pv.y * sc;
-                            const float rd = sc / (ax * ax + ay * ay);
-                            pinv = make_float2(ax * rd, -ay * rd);
-                        }
+                        // 1 / pv, scaled against overflow of |pv|^2
+                        const float sc = __frcp_rn(fmaxf(fabsf(pv.x), fabsf(pv.y)));
+                        const float ax = pv.x * sc, ay = pv.y * sc;
+                        const float rd = sc * __frcp_rn(ax * ax + ay * ay);
+                        pinv = make_float2(ax * rd, -ay * rd);
                     }
+                    // row -= (c / pv) * pivot row, column k becomes -c / pv;
+                    // the pivot row is scaled by 1 / pv, its column k becomes 1 / pv
+                    const float2 sfac = cmul(P[0], pinv);
+#pragma unroll
+                    for (int e = 0; e < kFtB - 1; e++) P[e] = cfms(sfac, prow[e], P[e + 1]);
+                    P[kFtB - 1] = make_float2(-sfac.x, -sfac.y);
                     if (t == r) {
 #pragma unroll
-                        for (int e = 0; e < kFtB; e++) P[e] = e == kk ? pinv : cmul(prow[e], pinv);
+                        for (int e = 0; e < kFtB - 1; e++) P[e] = cmul(prow[e], pinv);
+                        P[kFtB - 1] = pinv;
                         used = true;
                         my_step = k;
                         sm.perm[k] = t;
-                    } else {
-                        // row -= (c / pv) * pivot row; column k becomes -c / pv
-                        const float2 sfac = cmul(P[kk], pinv);
-#pragma unroll
-                        for (int e = 0; e < kFtB; e++)
-                            if (e != kk) P[e] = cfms(sfac, prow[e], P[e]);
-                        P[kk] = make_float2(-sfac.x, -sfac.y);
                     }
+                }
+                // back to column order (P[e] holds column (bl + e) mod 16;
+                // only a partial last panel is not back in order), through
+                // this thread's row of G, which holds nothing during the panels
+                if (bl < kFtB) {
+                    float2 *tmp = sm.G + (size_t)t * kFtGld;
+#pragma unroll
+                    for (int e = 0; e < kFtB; e++) tmp[(bl + e) & (kFtB - 1)] = P[e];
+#pragma unroll
+                    for (int e = 0; e < kFtB; e++) P[e] = tmp[e];
                 }
 
                 // ---- X = panel - E_R into TMEM (tf32 hi / lo)

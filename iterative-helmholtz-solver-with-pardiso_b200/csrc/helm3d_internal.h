@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include <complex>
 #include <functional>
 #include <string>
@@ -276,6 +278,10 @@ template <typename K> inline bool smem_limit_max(K kern, size_t need) {
 // cached per (family, shape) for the process (and in HELM3D_TUNE_CACHE).
 // Not for use inside a stream capture.
 bool tune_enabled();
+// The polls a kernel's bounded waits between its warps make before giving
+// up: `dflt`, or HELM3D_WAIT_LIMIT (read at every launch) when set, so that
+// a test can make such a wait expire and check the status it reports.
+uint32_t wait_limit_polls(uint32_t dflt);
 // HELM3D_FORCE_<family> as an integer, or -1 when unset
 int tune_forced(const char *family);
 constexpr int kStencilVariants = 8;   // z chunk 16, 8, 32, 64; source-major (0-3) or source-minor (4-7) grid
@@ -343,6 +349,7 @@ struct helm3d_ctx {
     void *d_planes = nullptr;      // spectral planes, P precision (planes_R right-hand sides)
     int planes_R = 0;
     int *d_status = nullptr;
+    int factor_rc = HELM3D_OK;   // status of the last set-up and factor (set_medium)
     // Krylov workspace for r_alloc right-hand sides of restart length m_alloc
     int m_alloc = 0, r_alloc = 0;
     size_t kry_bytes = 0;
@@ -433,5 +440,7 @@ int cuda_check(helm3d_ctx *c, cudaError_t e, const char *what);
 // wait that expired (bits 1, 2) or a failed index check (bit 3) in a kernel
 // -> HELM3D_ERR_CUDA.  Synchronizes the stream; allocates nothing.
 int check_status(helm3d_ctx *c);
+// Start of a call that runs kernels on the context (see capi.cpp).
+int begin_call(helm3d_ctx *c);
 void build_fft_plan(int n, FftPlan &plan, std::vector<zc> &tables);
 }  // namespace h3d

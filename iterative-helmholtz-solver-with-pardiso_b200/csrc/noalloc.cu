@@ -67,6 +67,7 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
         if (at.type == cudaMemoryTypeDevice && at.device != c->device)
             return set_error(c, HELM3D_ERR_ARG, "apply_prec_noalloc: x and y must be on the context's device");
     }
+    if ((rc = begin_call(c))) return rc;
     void *scratch = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_mu);

@@ -41,8 +41,13 @@ template <typename R> struct SweepK {
     int nstage;          // ring depth
     uint32_t stage_bytes;
     int *status;
+    uint32_t wait_limit;  // polls of a producer/consumer wait before it gives up (status bit 2)
 };
 
+// Polls of a bounded wait.  Waits between the producer and the consumers use
+// SweepK::wait_limit (this value unless HELM3D_WAIT_LIMIT sets it, to make
+// a wait expire in a test); the final drain of the producer's own copies
+// always uses this value, so that no copy is in flight when the CTA exits.
 constexpr uint32_t kSweepWaitLimit = 1u << 20;
 constexpr int kSweepConsumerWarps = 8;
 constexpr int kSweepMaxN = 256;
@@ -127,7 +132,7 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
             for (; seq < nseq; seq++) {
                 const int s = (int)(seq % a.nstage);
                 const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
-                if (!mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, kSweepWaitLimit)) {
+                if (!mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, a.wait_limit)) {
                     // stop issuing: the consumers' bounded waits on full[] expire in turn
                     atomicOr(a.status, 4);
                     break;
@@ -169,7 +174,7 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
         for (int ch = 0; ch < cpl; ch++, seq++) {
             const int s = (int)(seq % a.nstage);
             const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
-            if (!dead && !mbar_wait_bounded_cta(smem_u32(&full[s]), ph, kSweepWaitLimit)) {
+            if (!dead && !mbar_wait_bounded_cta(smem_u32(&full[s]), ph, a.wait_limit)) {
                 dead = true;
                 atomicOr(a.status, 4);
             }
@@ -276,7 +281,7 @@ __global__ void __launch_bounds__((CW + 1) * 32, 1) sweep_tiled_kernel(SweepK<fl
             for (; seq < nseq; seq++) {
                 const int s = (int)(seq % a.nstage);
                 const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
-                if (!mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, kSweepWaitLimit)) {
+                if (!mbar_wait_bounded_cta(smem_u32(&empty[s]), ph ^ 1u, a.wait_limit)) {
                     // stop issuing: the consumers' bounded waits on full[] expire in turn
                     atomicOr(a.status, 4);
                     break;
@@ -325,7 +330,7 @@ __global__ void __launch_bounds__((CW + 1) * 32, 1) sweep_tiled_kernel(SweepK<fl
         for (int ch = 0; ch < cpl; ch++, seq++) {
             const int s = (int)(seq % a.nstage);
             const uint32_t ph = (uint32_t)((seq / a.nstage) & 1);
-            if (!dead && !mbar_wait_bounded_cta(smem_u32(&full[s]), ph, kSweepWaitLimit)) {
+            if (!dead && !mbar_wait_bounded_cta(smem_u32(&full[s]), ph, a.wait_limit)) {
                 dead = true;
                 atomicOr(a.status, 4);
             }
@@ -410,6 +415,7 @@ template <int RR, bool ADJ> static int sweep_tiled_rr(const SweepArgs &sa, cudaS
     k.planes = (Cx *)sa.planes;
     k.dxy = (const Cx *)sa.dxy;
     k.status = sa.status;
+    k.wait_limit = wait_limit_polls(kSweepWaitLimit);
     // groups: the largest power of two GM with tiles <= threads per group
     constexpr int CT = kTiledWarps * 32;
     const int tiles = ((sa.n + kTileM - 1) / kTileM) * (RR / kTileR);
@@ -465,6 +471,7 @@ template <typename R, int G, int RR, bool ADJ> static int sweep_impl(const Sweep
     k.planes = (Cx *)sa.planes;
     k.dxy = (const Cx *)sa.dxy;
     k.status = sa.status;
+    k.wait_limit = wait_limit_polls(kSweepWaitLimit);
     const size_t vbytes = sizeof(Cx) * 2 * (size_t)sa.n * RR;
     const size_t budget = device_info().smem_optin - vbytes - 1024;
     // stages of about stage_kb, as many as fit the rest of shared memory

@@ -62,6 +62,13 @@ bool tune_enabled() {
     return !(e && e[0] == '0');
 }
 
+uint32_t wait_limit_polls(uint32_t dflt) {
+    const char *e = std::getenv("HELM3D_WAIT_LIMIT");
+    if (!e || !*e) return dflt;
+    const long v = std::atol(e);
+    return v >= 1 && v < (long)dflt ? (uint32_t)v : dflt;
+}
+
 int tune_forced(const char *family) {
     char name[64];
     std::snprintf(name, sizeof(name), "HELM3D_FORCE_%s", family);
