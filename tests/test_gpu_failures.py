@@ -78,11 +78,12 @@ def test_exactly_singular_block(prec):
 
 
 def test_device_memory_exhausted_then_recovers():
-    """A grid whose block factor (nz ny nx^2 complex64 = 188 GB) exceeds the
-    device: helm3d_create returns HELM3D_ERR_OOM and frees what it took; a
-    small context on the same device works right after."""
+    """A grid whose block factor (nz ny nx^2 complex64 = 215 GB) exceeds the
+    device's memory (192 GB on a B200): helm3d_create returns HELM3D_ERR_OOM
+    and frees what it took; a small context on the same device works right
+    after."""
     import helm3d
-    nx, ny, nz = 256, 256, 1400
+    nx, ny, nz = 256, 256, 1600
     g = helm3d.grid_mode_n(nx, ny, nz, 10.0, 8, 2 * np.pi * 1500 / 80.0)
     o = helm3d.default_opts(precision=helm3d.PREC_C64, z_transform=helm3d.ZT_FFT)
     s2 = np.full(nx * ny * nz, 1.0 / 1500.0 ** 2)
