@@ -264,6 +264,10 @@ int set_error(helm3d_ctx *c, int code, const std::string &msg) {
 
 int cuda_check(helm3d_ctx *c, cudaError_t e, const char *what) {
     if (e == cudaSuccess) return HELM3D_OK;
+    // a failed call leaves its error as the thread's last error; clear it
+    // (possible for the non-sticky ones, e.g. a failed allocation), so that
+    // the next launch check of this or another context does not report it
+    cudaGetLastError();
     const int code = (e == cudaErrorMemoryAllocation) ? HELM3D_ERR_OOM : HELM3D_ERR_CUDA;
     return set_error(c, code, std::string(what) + ": " + cudaGetErrorString(e));
 }
