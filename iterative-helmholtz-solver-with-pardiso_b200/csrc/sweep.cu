@@ -23,6 +23,8 @@
 // [kz][line][r][i].
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include <cstdint>
 
 #include "cplx.cuh"
@@ -42,6 +44,8 @@ template <typename R> struct SweepK {
     uint32_t stage_bytes;
     int *status;
     uint32_t wait_limit;  // polls of a producer/consumer wait before it gives up (status bit 2)
+    int expire_test;      // HELM3D_TEST_EXPIRE_WAIT: the consumers first wait on a barrier that
+                          // nothing arrives on, so that the wait expires (tests of the status path)
 };
 
 // Polls of a bounded wait.  Waits between the producer and the consumers use
@@ -108,6 +112,7 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
     Cx *vbuf = reinterpret_cast<Cx *>(smem_raw + (size_t)a.nstage * a.stage_bytes);  // [2][n][RR]
     uint64_t *full = reinterpret_cast<uint64_t *>(vbuf + 2 * (size_t)n * RR);
     uint64_t *empty = full + a.nstage;
+    uint64_t *never = empty + a.nstage;         // no thread arrives on it
     Cx *P = a.planes + (long)kz * ny * Rn * n;  // line j, rhs r, row i at ((j*Rn + r)*n + i)
     const int cpl = (n + a.rows_per_stage - 1) / a.rows_per_stage;
     const long nseq = (long)(2 * ny - 1) * cpl;
@@ -117,6 +122,7 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], kSweepConsumerWarps);
         }
+        mbar_init(never, 1);
         fence_mbar_init_cluster();
     }
     for (int q = threadIdx.x; q < n * RR; q += blockDim.x) {  // v of line 0: f_0
@@ -152,6 +158,10 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
     const int i = warp * RW + il;
     const bool own = i < n;
     bool dead = false;
+    if (a.expire_test && !mbar_wait_bounded_cta(smem_u32(never), 0u, a.wait_limit)) {
+        dead = true;
+        atomicOr(a.status, 4);
+    }
     long seq = 0;
     for (int step = 0; step < 2 * ny - 1; step++) {
         const bool fwd = step < ny;
@@ -415,6 +425,7 @@ template <int RR, bool ADJ> static int sweep_tiled_rr(const SweepArgs &sa, cudaS
     k.planes = (Cx *)sa.planes;
     k.dxy = (const Cx *)sa.dxy;
     k.status = sa.status;
+    k.expire_test = 0;
     k.wait_limit = wait_limit_polls(kSweepWaitLimit);
     // groups: the largest power of two GM with tiles <= threads per group
     constexpr int CT = kTiledWarps * 32;
@@ -472,6 +483,10 @@ template <typename R, int G, int RR, bool ADJ> static int sweep_impl(const Sweep
     k.dxy = (const Cx *)sa.dxy;
     k.status = sa.status;
     k.wait_limit = wait_limit_polls(kSweepWaitLimit);
+    {
+        const char *e = std::getenv("HELM3D_TEST_EXPIRE_WAIT");
+        k.expire_test = (e && *e && *e != '0') ? 1 : 0;
+    }
     const size_t vbytes = sizeof(Cx) * 2 * (size_t)sa.n * RR;
     const size_t budget = device_info().smem_optin - vbytes - 1024;
     // stages of about stage_kb, as many as fit the rest of shared memory
@@ -488,7 +503,7 @@ template <typename R, int G, int RR, bool ADJ> static int sweep_impl(const Sweep
     if (nst > 32) nst = 32;
     if (nst < 2) return HELM3D_ERR_ARG;
     k.nstage = nst;
-    const size_t smem = (size_t)nst * k.stage_bytes + vbytes + 2 * nst * sizeof(uint64_t);
+    const size_t smem = (size_t)nst * k.stage_bytes + vbytes + (2 * nst + 1) * sizeof(uint64_t);
     auto kern = sweep_kernel<R, G, RR, ADJ>;
     if (!smem_limit_max(kern, smem))
         return HELM3D_ERR_CUDA;

@@ -99,22 +99,25 @@ def test_device_memory_exhausted_then_recovers():
 
 
 def test_expired_wait_is_reported_and_the_context_recovers(monkeypatch):
-    """The block sweep's waits between its copy producer and its consumers
-    limited to one poll (HELM3D_WAIT_LIMIT=1, read at launch): the copies
-    cannot land that fast, the waits expire, the kernel sets its status bit
-    and finishes without waiting, and the apply returns HELM3D_ERR_CUDA.
-    With the limit unset, the next apply of the same context is right."""
+    """A bounded wait that runs out: with HELM3D_TEST_EXPIRE_WAIT (read at
+    launch) the block sweep's consumers first wait on a barrier that nothing
+    arrives on, limited to 64 polls (HELM3D_WAIT_LIMIT); the wait expires,
+    the kernel sets its status bit and finishes without waiting (its copies
+    drained), and the apply returns HELM3D_ERR_CUDA.  Without the switch,
+    the next apply of the same context is right."""
     import helm3d
     p = small_problem(24, 20, 18, pml=4, seed=8)
     on = mode_n.setup(p, beta_prec=0.25)
     v = rand_c(p.shape, seed=4)
     s = mode_n_solver(p, precision=1)
     monkeypatch.setenv("HELM3D_FORCE_SWEEP", "0")
-    monkeypatch.setenv("HELM3D_WAIT_LIMIT", "1")
+    monkeypatch.setenv("HELM3D_WAIT_LIMIT", "64")
+    monkeypatch.setenv("HELM3D_TEST_EXPIRE_WAIT", "1")
     y = np.empty_like(v)
     rc = helm3d.lib.helm3d_apply_prec(s.h, np.ascontiguousarray(v).ctypes.data, y.ctypes.data)
     assert rc == helm3d.ERR_CUDA, rc
     assert b"bounded wait" in helm3d.lib.helm3d_last_error(s.h)
+    monkeypatch.delenv("HELM3D_TEST_EXPIRE_WAIT")
     monkeypatch.delenv("HELM3D_WAIT_LIMIT")
     assert rel(s.apply_prec(v), on.apply_prec(v)) < 5e-5
     s.close()
