@@ -57,8 +57,15 @@ void FGMRES(size_m x, size_m y, size_m z, int m, int rest, const point source, d
             const dtype *f, double thresh, double &diff_sol, double beta_eq);
 
 /* BCGSTAB (Source/BcGSTAB.cpp:6-666; Source/templates.h:60): BiCGStab on the
- * same operator with the 5-point L0, up to m iterations, exit at an absolute
- * residual RES_EXIT = 1e-8 scaled by ||f||. */
+ * same operator, shadow residual 2 r0, the iterate kept in u-space, up to m
+ * iterations, exit when the absolute residual over the physical domain drops
+ * below RES_EXIT = 1e-8 (Source/BcGSTAB.cpp:503-505, 564).  L0 is the 5-point
+ * operator: the reference assembles BCGSTAB's 2D systems with its 9-point
+ * routine, whose coefficients (a = c = 1, d = 0) make the four diagonal-
+ * neighbour entries exactly zero (Source/functions.cpp:2497-2512, 3557-3559).
+ * With the HOMO medium (the default) the source cross of x_sol and of x_orig
+ * (when not NULL) is zeroed as the reference does (Source/BcGSTAB.cpp:532-533).
+ * diff_sol receives the final relative residual over the physical domain. */
 void BCGSTAB(size_m x, size_m y, size_m z, int m, const point source, dtype *x_sol, dtype *x_orig, const dtype *f,
              double thresh, double &diff_sol, double beta_eq);
 

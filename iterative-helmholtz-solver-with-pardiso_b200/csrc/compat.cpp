@@ -51,7 +51,7 @@ std::vector<double> reference_s2(const size_m &x, const size_m &y, const size_m 
 }
 
 helm3d_ctx *make_ctx(const size_m &x, const size_m &y, const size_m &z, int restart, int max_iter, double tol,
-                     double beta_eq) {
+                     double beta_eq, int stop_phys = 0) {
     helm3d_grid g;
     g.nx = x.n;
     g.ny = y.n;
@@ -76,6 +76,7 @@ helm3d_ctx *make_ctx(const size_m &x, const size_m &y, const size_m &z, int rest
     o.restart = restart;
     o.max_iter = max_iter;
     o.tol = tol;
+    o.stop_phys = stop_phys;
     o.device = g_device;
     const std::vector<double> s2 = reference_s2(x, y, z);
     helm3d_ctx *ctx = nullptr;
@@ -85,6 +86,22 @@ helm3d_ctx *make_ctx(const size_m &x, const size_m &y, const size_m &z, int rest
         return nullptr;
     }
     return ctx;
+}
+
+// NullifySource2D(x, y, u + plane z.n/2, size2D/2, 1) (Source/functions.cpp:
+// 6628-6644): zeroes the points l = 0, 1 to the left, right, below and above
+// index size2D/2 of the middle z plane, with the reference's flat indexing
+// (for even x.n the "left" point is the last one of the row below)
+void nullify_source_cross(const size_m &x, const size_m &y, const size_m &z, dtype *u) {
+    const long size2D = (long)x.n * y.n;
+    dtype *plane = u + (long)(z.n / 2) * size2D;
+    const long src = size2D / 2, jsrc = src / x.n, isrc = src - (long)x.n * jsrc;
+    for (long l = 0; l <= 1; l++) {
+        plane[isrc - l + x.n * jsrc] = 0.0;
+        plane[isrc + l + x.n * jsrc] = 0.0;
+        plane[isrc + x.n * (jsrc - l)] = 0.0;
+        plane[isrc + x.n * (jsrc + l)] = 0.0;
+    }
 }
 
 }  // namespace
@@ -118,16 +135,24 @@ void BCGSTAB(size_m x, size_m y, size_m z, int m, const point source, dtype *x_s
     double nf = 0.0;
     for (size_t q = 0; q < n; q++) nf += std::norm(f[q]);
     nf = std::sqrt(nf);
-    // RES_EXIT = 1e-8 on the absolute residual (Source/BcGSTAB.cpp:564)
+    // RES_EXIT = 1e-8 on the absolute residual of the physical domain
+    // (Source/BcGSTAB.cpp:503-505, 564), at most m iterations
     const double tol = nf > 0 ? 1e-8 / nf : 0.0;
-    helm3d_ctx *ctx = make_ctx(x, y, z, 1, m > 0 ? m : 1, tol, beta_eq);
+    helm3d_ctx *ctx = make_ctx(x, y, z, 1, m > 0 ? m : 1, tol, beta_eq, 1);
     if (!ctx) return;
     helm3d_stats st = {};
     const int rc = helm3d_solve_bicgstab(ctx, reinterpret_cast<const double *>(f), reinterpret_cast<double *>(x_sol),
                                          &st);
     if (rc != HELM3D_OK && rc != HELM3D_ERR_NOT_CONVERGED)
         fprintf(stderr, "!!! helm3d BCGSTAB failed: %s (%s) !!!\n", helm3d_status_string(rc), helm3d_last_error(ctx));
-    printf("helm3d BCGSTAB: %d iterations, relative residual %e\n", st.iterations, st.relres);
+    printf("helm3d BCGSTAB: %d iterations, relative residual %e (physical domain %e)\n", st.iterations, st.relres,
+           st.relres_phys);
     diff_sol = st.relres_phys;
     helm3d_destroy(ctx);
+    // the HOMO build zeroes the source cross of its solution and of x_orig
+    // (Source/BcGSTAB.cpp:532-533)
+    if (!g_linear) {
+        nullify_source_cross(x, y, z, x_sol);
+        if (x_orig) nullify_source_cross(x, y, z, x_orig);
+    }
 }

@@ -1264,9 +1264,11 @@ int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st) {
         RC(axpby1(c, make_double2(1, 0), r, make_double2(beta.real(), beta.imag()), p));
 
         it++;
-        double r2;
-        RC(norm2_one(c, r, false, &r2, nullptr));
-        relres = std::sqrt(r2) / nf;
+        // the recursion's residual, over the whole grid or (stop_phys, as the
+        // reference's test, Source/BcGSTAB.cpp:503-505) the physical domain
+        double r2, rp2 = 0.0;
+        RC(norm2_one(c, r, o.stop_phys != 0, &r2, &rp2));
+        relres = std::sqrt(o.stop_phys ? rp2 : r2) / nf;
         if (st && st->history && st->history_len < st->history_cap) st->history[st->history_len++] = relres;
         if (!std::isfinite(relres)) return set_error(c, HELM3D_ERR_NONFINITE, "BiCGStab residual is NaN/Inf");
         if (relres <= o.tol) break;
@@ -1293,7 +1295,8 @@ int bicgstab(helm3d_ctx *c, const double2 *f, double2 *u, helm3d_stats *st) {
         st->relres_phys = std::sqrt(rp2) / nf;
         st->ms_solve += ms;
     }
-    if (status == HELM3D_OK && relres > o.tol) status = HELM3D_ERR_NOT_CONVERGED;
+    if (status == HELM3D_OK && (o.stop_phys ? std::sqrt(rp2) / nf : relres) > o.tol)
+        status = HELM3D_ERR_NOT_CONVERGED;
     return status;
 }
 

@@ -319,6 +319,23 @@ def fgmres_reference(st: ModeR, f: np.ndarray, m: int = 10, rest: int = 5, thres
     return FgmresLog(rows, x0.reshape(shape), u)
 
 
+def nullify_source_cross(g: Grid3D, u: np.ndarray) -> np.ndarray:
+    """``NullifySource2D(x, y, u + plane nz/2, size2D/2, 1)``
+    (Source/functions.cpp:6628-6644): zero the points 0 and 1 to the left,
+    right, below and above flat index size2D/2 of the middle z plane, with the
+    reference's flat indexing (for even nx the "left" neighbour of the row's
+    first point is the last point of the row below)."""
+    out = np.array(u, dtype=np.complex128, copy=True).reshape(g.shape_zyx)
+    plane = out[g.z.n // 2].reshape(-1)
+    nx = g.x.n
+    src = g.size2d // 2
+    jsrc, isrc = divmod(src, nx)
+    for l in (0, 1):
+        for q in (isrc - l + nx * jsrc, isrc + l + nx * jsrc, isrc + nx * (jsrc - l), isrc + nx * (jsrc + l)):
+            plane[q] = 0.0
+    return out
+
+
 def bicgstab_reference(st: ModeR, f: np.ndarray, m: int = 10, res_exit: float = 1e-8):
     """BiCGStab as ``BCGSTAB`` drives it (Source/BcGSTAB.cpp:397-560).
 
@@ -326,8 +343,10 @@ def bicgstab_reference(st: ModeR, f: np.ndarray, m: int = 10, res_exit: float = 
     (x += alpha L0^{-1} p + omega L0^{-1} s); shadow residual r* = 2 r0;
     residual A_R x - f checked via L0 x then K (:495-496); exit when the
     absolute physical residual < res_exit (:564).  The reference assembles
-    9-point 2D matrices for this driver; the oracle uses the same 5-point
-    L0 as FGMRES.
+    its 2D matrices with the 9-point routine (:143), whose entries at the
+    diagonal neighbours are exactly zero with the coefficients it uses
+    (Source/functions.cpp:2497-2512, 3557-3559), so L0 is the same 5-point
+    operator as FGMRES's (pinned by tests/test_oracle_pins.py).
     """
     shape = st.shape
     mask = physical_mask(st.g)

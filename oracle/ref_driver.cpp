@@ -15,6 +15,16 @@
 //       (Source/main.cpp:418) and calls FGMRES (Source/main.cpp:470); writes
 //       f and x_sol.  FGMRES itself writes its convergence_*.dat file into
 //       the working directory.
+//   ref_driver bcgstab <n_nopml> <pml> <spg> <beta> <niter> <fscale> <outdir>
+//       the same grid and RHS scaled by fscale (BCGSTAB stops on an absolute
+//       residual, RES_EXIT = 1e-8, so the scale sets how many iterations it
+//       runs), then BCGSTAB (Source/BcGSTAB.cpp:6-666, the call main has
+//       commented out at Source/main.cpp:471); writes f and x_sol, and
+//       BCGSTAB writes its convergence_*_BCGSTAB.dat file.
+//   ref_driver setup9 <n_nopml> <pml> <spg> <outdir>
+//       the base 2D matrix of BCGSTAB, GenSparseMatrixOnline2DwithPMLand9Pts
+//       (-1, ...) (Source/BcGSTAB.cpp:143, Source/functions.cpp:3532-3679):
+//       CSR values / ia / ja and the diagonal positions freqs.
 //
 // The reference is compiled with its own definitions.h, i.e. HOMO mode,
 // nu = 4 Hz, c_z = 1280 m/s, LENGTH = 3200 m, REL_RES_EXIT = 1e-4.
@@ -120,6 +130,54 @@ int main(int argc, char **argv) {
         write_bin(out + "/x_sol.bin", x_sol, sizeof(dtype) * size);
         write_bin(out + "/x_orig.bin", x_orig, sizeof(dtype) * size);
         printf("fgmres done: nx=%d nz=%d\n", x.n, z.n);
+        return 0;
+    }
+    if (mode == "bcgstab" && argc == 9) {
+        int n_nopml = atoi(argv[2]), pml = atoi(argv[3]), spg = atoi(argv[4]);
+        double beta = atof(argv[5]);
+        int niter = atoi(argv[6]);
+        double fscale = atof(argv[7]);
+        std::string out = argv[8];
+        size_m x, y, z;
+        make_grid(n_nopml, pml, spg, x, y, z);
+        point source = make_source(x, y, z);
+        int size = x.n * y.n * z.n;
+        dtype *x_orig = alloc_arr<dtype>(size);
+        dtype *x_sol = alloc_arr<dtype>(size);
+        dtype *f = alloc_arr<dtype>(size);
+        GenRHSandSolutionViaSound3D(x, y, z, x_orig, f, source);
+        for (int q = 0; q < size; q++) {
+            f[q] *= fscale;
+            x_orig[q] *= fscale;
+        }
+        double thresh = 1e-4, diff_sol = 0;
+        BCGSTAB(x, y, z, niter, source, x_sol, x_orig, f, thresh, diff_sol, beta);
+        write_bin(out + "/f.bin", f, sizeof(dtype) * size);
+        write_bin(out + "/x_sol.bin", x_sol, sizeof(dtype) * size);
+        printf("bcgstab done: nx=%d nz=%d\n", x.n, z.n);
+        return 0;
+    }
+    if (mode == "setup9" && argc == 6) {
+        int n_nopml = atoi(argv[2]), pml = atoi(argv[3]), spg = atoi(argv[4]);
+        std::string out = argv[5];
+        size_m x, y, z;
+        make_grid(n_nopml, pml, spg, x, y, z);
+        int size2D = x.n * y.n;
+        // the count BCGSTAB allocates (Source/BcGSTAB.cpp:98)
+        int nnz = (x.n + (x.n - 1) * 2) * y.n + 2 * (size2D - x.n) + 4 * (x.n - 1) * (y.n - 1);
+        zcsr *A = (zcsr *)malloc(sizeof(zcsr));
+        A->values = alloc_arr<dtype>(nnz);
+        A->ia = alloc_arr<int>((size_t)size2D + 1);
+        A->ja = alloc_arr<int>(nnz);
+        A->ia[size2D] = nnz + 1;
+        A->non_zeros = nnz;
+        int *freqs = alloc_arr<int>(size2D);
+        GenSparseMatrixOnline2DwithPMLand9Pts(-1, x, y, A, 0, freqs);
+        write_bin(out + "/csr9_values.bin", A->values, sizeof(dtype) * nnz);
+        write_bin(out + "/csr9_ia.bin", A->ia, sizeof(int) * (size2D + 1));
+        write_bin(out + "/csr9_ja.bin", A->ja, sizeof(int) * nnz);
+        write_bin(out + "/csr9_freqs.bin", freqs, sizeof(int) * size2D);
+        printf("setup9 done: nx=%d nnz=%d\n", x.n, nnz);
         return 0;
     }
     fprintf(stderr, "bad arguments\n");

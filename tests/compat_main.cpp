@@ -1,8 +1,9 @@
-// compat_fgmres_main.cpp -- calls FGMRES through include/helm3d_compat.h the
-// way the reference's main does (Source/main.cpp:95-193, 470): grid from
-// n_nopml / pml / spg without SOURCE_SHIFT, niter, restart, beta_eq.  The
+// compat_main.cpp -- calls FGMRES or BCGSTAB through include/helm3d_compat.h
+// the way the reference's main does (Source/main.cpp:95-193, 470-471): grid
+// from n_nopml / pml / spg without SOURCE_SHIFT, niter, restart, beta_eq.  The
 // right-hand side is read from f.bin, the solution written to x_sol.bin.
-//   compat_fgmres_main <n_nopml> <pml> <spg> <beta> <niter> <restart> <dir>
+//   compat_main fgmres  <n_nopml> <pml> <spg> <beta> <niter> <restart> <dir>
+//   compat_main bcgstab <n_nopml> <pml> <spg> <beta> <niter> <dir>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -12,11 +13,14 @@
 #include "helm3d_compat.h"
 
 int main(int argc, char **argv) {
-    if (argc != 8) return 2;
-    const int n_nopml = atoi(argv[1]), pml = atoi(argv[2]), spg = atoi(argv[3]);
-    const double beta = atof(argv[4]);
-    const int niter = atoi(argv[5]), restart = atoi(argv[6]);
-    const std::string dir = argv[7];
+    if (argc < 2) return 2;
+    const std::string solver = argv[1];
+    const bool bcg = solver == "bcgstab";
+    if (argc != (bcg ? 8 : 9)) return 2;
+    const int n_nopml = atoi(argv[2]), pml = atoi(argv[3]), spg = atoi(argv[4]);
+    const double beta = atof(argv[5]);
+    const int niter = atoi(argv[6]), restart = bcg ? 1 : atoi(argv[7]);
+    const std::string dir = argv[bcg ? 7 : 8];
     const double L = 3200.0;  // LENGTH (Source/definitions.h:222)
     size_m x, y, z;
     memset(&x, 0, sizeof(x));
@@ -41,7 +45,8 @@ int main(int argc, char **argv) {
     if (!fh || fread(f.data(), sizeof(dtype), size, fh) != size) return 3;
     fclose(fh);
     double diff_sol = 0;
-    FGMRES(x, y, z, niter, restart, source, x_sol.data(), x_orig.data(), f.data(), 1e-4, diff_sol, beta);
+    if (bcg) BCGSTAB(x, y, z, niter, source, x_sol.data(), x_orig.data(), f.data(), 1e-4, diff_sol, beta);
+    else FGMRES(x, y, z, niter, restart, source, x_sol.data(), x_orig.data(), f.data(), 1e-4, diff_sol, beta);
     fh = fopen((dir + "/x_sol.bin").c_str(), "wb");
     fwrite(x_sol.data(), sizeof(dtype), size, fh);
     fclose(fh);

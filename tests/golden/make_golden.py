@@ -7,6 +7,10 @@ stores what the reference computed:
   ref_setup_<tag>.npz   sound2D, deltaL, base 2D CSR matrix (values/ia/ja)
   ref_fgmres_<tag>.npz  f, x_sol (u = L0^{-1} w), convergence rows
                         (iteration, Res_phys, RelRes_phys, analytic error)
+  ref_setup9_<tag>.npz  BCGSTAB's base 2D matrix (9-point CSR, values/ia/ja,
+                        diagonal positions freqs)
+  ref_bcgstab_<tag>.npz f (the RHS scaled by fscale), x_sol, convergence rows
+                        (iteration, Res_phys, RelRes_phys, analytic error)
 
 The reference is compiled in its default configuration (HOMO, nu = 4 Hz,
 c_z = 1280 m/s, LENGTH = 3200 m, REL_RES_EXIT = 1e-4).  Needs the reference
@@ -33,6 +37,13 @@ CASES = [
     ("n10p4s3", 10, 4, 3, 0.5, 10, 5),
     ("n11p4s3", 11, 4, 3, 0.5, 10, 5),     # odd sizes: source at (n-1)/2
     ("n16p6s4", 16, 6, 4, 0.25, 8, 4),
+]
+# BCGSTAB stops on an absolute residual (RES_EXIT = 1e-8); the RHS scale
+# sets how many iterations it runs: (tag, n_nopml, pml, spg, beta, niter, fscale)
+BCG_CASES = [
+    ("n10p4s3", 10, 4, 3, 0.5, 40, 1e8),
+    ("n11p4s3", 11, 4, 3, 0.5, 40, 1e8),
+    ("n16p6s4", 16, 6, 4, 0.25, 16, 1e8),   # stops at the iteration cap (BiCGStab stagnates here)
 ]
 
 
@@ -71,6 +82,30 @@ def main():
                 conv=conv,
             )
         print("wrote", tag, file=sys.stderr)
+    for tag, n, pml, spg, beta, niter, fscale in BCG_CASES:
+        nx = n + 2 * pml
+        nz = n + 2 * spg
+        with tempfile.TemporaryDirectory() as d:
+            run(["setup9", n, pml, spg, d], d)
+            np.savez_compressed(
+                os.path.join(HERE, f"ref_setup9_{tag}.npz"),
+                params=np.array([n, pml, spg]),
+                csr_values=np.fromfile(os.path.join(d, "csr9_values.bin"), dtype=np.complex128),
+                csr_ia=np.fromfile(os.path.join(d, "csr9_ia.bin"), dtype=np.int32),
+                csr_ja=np.fromfile(os.path.join(d, "csr9_ja.bin"), dtype=np.int32),
+                freqs=np.fromfile(os.path.join(d, "csr9_freqs.bin"), dtype=np.int32),
+            )
+        with tempfile.TemporaryDirectory() as d:
+            run(["bcgstab", n, pml, spg, beta, niter, fscale, d], d)
+            conv = np.loadtxt(glob.glob(os.path.join(d, "convergence_*BCGSTAB*"))[0], ndmin=2)
+            np.savez_compressed(
+                os.path.join(HERE, f"ref_bcgstab_{tag}.npz"),
+                params=np.array([n, pml, spg, beta, niter, fscale]),
+                f=np.fromfile(os.path.join(d, "f.bin"), dtype=np.complex128).reshape(nz, nx, nx),
+                x_sol=np.fromfile(os.path.join(d, "x_sol.bin"), dtype=np.complex128).reshape(nz, nx, nx),
+                conv=conv,
+            )
+        print("wrote bcgstab", tag, file=sys.stderr)
 
 
 if __name__ == "__main__":
