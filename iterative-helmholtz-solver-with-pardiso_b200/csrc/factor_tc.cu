@@ -68,13 +68,13 @@ struct FtSmem {
     float2 *wrow;       // [2][4][kFtB]
     uint32_t *ckey;     // [2][4]: each warp's pivot key, by step parity
     int *perm;          // [kFtNP]
-    uint64_t *b_ready, *mma_done, *fin, *stepbar;
+    uint64_t *b_ready, *mma_done, *fin;
     uint32_t *tslot;
 };
 
 constexpr size_t kFtSmemBytes = sizeof(float2) * kFtNP * kFtGld + 2 * sizeof(float) * 2 * kFtNP * 2 * kFtB +
                                 sizeof(float2) * kFtB * kFtYld + sizeof(float2) * 2 * 4 * kFtB +
-                                sizeof(float) * 8 + sizeof(int) * 8 + sizeof(int) * kFtNP + 4 * sizeof(uint64_t) +
+                                sizeof(float) * 8 + sizeof(int) * 8 + sizeof(int) * kFtNP + 3 * sizeof(uint64_t) +
                                 16 + 128;
 
 __device__ __forceinline__ FtSmem ft_carve(unsigned char *raw) {
@@ -91,8 +91,7 @@ __device__ __forceinline__ FtSmem ft_carve(unsigned char *raw) {
     s.b_ready = reinterpret_cast<uint64_t *>(b);
     s.mma_done = s.b_ready + 1;
     s.fin = s.b_ready + 2;
-    s.stepbar = s.b_ready + 3;
-    s.tslot = reinterpret_cast<uint32_t *>(s.b_ready + 4);
+    s.tslot = reinterpret_cast<uint32_t *>(s.b_ready + 3);
     return s;
 }
 
@@ -114,7 +113,6 @@ __global__ void __launch_bounds__(kFtThreads, 1) factor_tc_kernel(FactorTcK a) {
         mbar_init(sm.b_ready, kFtRowWarps);
         mbar_init(sm.mma_done, 1);
         mbar_init(sm.fin, 1);
-        mbar_init(sm.stepbar, kFtRowWarps);
         fence_mbar_init_cluster();
     }
     tc_fence_before();
@@ -160,7 +158,7 @@ __global__ void __launch_bounds__(kFtThreads, 1) factor_tc_kernel(FactorTcK a) {
         // ----------------------------------------------------- row threads
         const int t = tid;                        // row t, TMEM lane t
         const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
-        uint32_t ph = 0, sph = 0;
+        uint32_t ph = 0;
         const float2 kzv = a.kz2[kz];
         for (int line = 0; line < ny; line++) {
             // ---- S_line = D_line - cmy[line] cpy[line-1] G_{line-1} into TMEM
@@ -222,36 +220,23 @@ __global__ void __launch_bounds__(kFtThreads, 1) factor_tc_kernel(FactorTcK a) {
                 // (kk + 1 + e) mod 16.  The pivot of a column is the candidate
                 // row with the largest key: the top 24 bits of |re| + |im| and
                 // 255 - row (ties, to 2^-15 relative, go to the lowest row),
-                // reduced per warp by redux.sync; each warp publishes its key
-                // and its winning row in shared memory slots alternating by
-                // step parity and arrives on the step barrier (4 arrivals per
-                // step).  A step's candidates are published as soon as the
-                // next column is updated: the rest of a row's update (all of
-                // it for the warp's winner) runs after the arrival, beside
-                // the other warps, off the step-to-step chain.
-                auto publish = [&](int k, int rot, uint32_t key) {
-                    const int buf = k & 1;
-                    const uint32_t kw = __reduce_max_sync(0xffffffffu, key);
-                    if (lane == 0) sm.ckey[buf * 4 + warp] = kw;
-                    if (kw != 0u && key == kw) {
-                        float2 *w = sm.wrow + (buf * 4 + warp) * kFtB;
-#pragma unroll
-                        for (int e = 0; e < kFtB; e++) w[(rot + e) & (kFtB - 1)] = P[e];
-                    }
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive_local(sm.stepbar);
-                };
-                auto cand = [&](float2 v) -> uint32_t {
-                    if (used || t >= n) return 0u;
-                    const float av = fabsf(v.x) + fabsf(v.y);
-                    return (av == av) ? ((__float_as_uint(av) & 0xFFFFFF00u) | (uint32_t)(255 - t)) : 0u;
-                };
-                publish(k0, 0, cand(P[0]));
+                // reduced per warp by redux.sync and across the 4 warps through
+                // shared memory slots alternating by step parity.
 #pragma unroll 1
                 for (int kk = 0; kk < bl; kk++) {
                     const int k = k0 + kk, buf = k & 1;
-                    wait(sm.stepbar, sph);
-                    sph ^= 1u;
+                    uint32_t key = 0;
+                    if (!used && t < n) {
+                        const float av = fabsf(P[0].x) + fabsf(P[0].y);
+                        if (av == av) key = (__float_as_uint(av) & 0xFFFFFF00u) | (uint32_t)(255 - t);
+                    }
+                    const uint32_t kw = __reduce_max_sync(0xffffffffu, key);
+                    if (lane == 0) sm.ckey[buf * 4 + warp] = kw;
+                    if (kw != 0u && key == kw) {
+#pragma unroll
+                        for (int e = 0; e < kFtB; e++) sm.wrow[(buf * 4 + warp) * kFtB + ((kk + e) & (kFtB - 1))] = P[e];
+                    }
+                    ft_row_barrier();
                     uint32_t kmax = sm.ckey[buf * 4];
                     int wsel = 0;
 #pragma unroll
@@ -282,35 +267,17 @@ __global__ void __launch_bounds__(kFtThreads, 1) factor_tc_kernel(FactorTcK a) {
                     }
                     // row -= (c / pv) * pivot row, column k becomes -c / pv;
                     // the pivot row is scaled by 1 / pv, its column k becomes 1 / pv
-                    const bool piv = t == r;
-                    if (piv) {
+                    const float2 sfac = cmul(P[0], pinv);
+#pragma unroll
+                    for (int e = 0; e < kFtB - 1; e++) P[e] = cfms(sfac, prow[e], P[e + 1]);
+                    P[kFtB - 1] = make_float2(-sfac.x, -sfac.y);
+                    if (t == r) {
+#pragma unroll
+                        for (int e = 0; e < kFtB - 1; e++) P[e] = cmul(prow[e], pinv);
+                        P[kFtB - 1] = pinv;
                         used = true;
                         my_step = k;
                         sm.perm[k] = t;
-                    }
-                    const float2 sfac = cmul(P[0], pinv);
-                    auto update = [&]() {
-#pragma unroll
-                        for (int e = 1; e < kFtB - 1; e++) P[e] = piv ? cmul(prow[e], pinv) : cfms(sfac, prow[e], P[e + 1]);
-                        P[kFtB - 1] = piv ? pinv : make_float2(-sfac.x, -sfac.y);
-                    };
-                    // the next column first (P[1] is still the old column k + 1)
-                    const float2 first = piv ? cmul(prow[0], pinv) : cfms(sfac, prow[0], P[1]);
-                    if (kk + 1 < bl) {
-                        const uint32_t key = cand(first);
-                        const uint32_t kw = __reduce_max_sync(0xffffffffu, key);
-                        if (kw != 0u && key == kw) {   // the warp's winner publishes its whole row
-                            update();
-                            P[0] = first;
-                        }
-                        publish(k + 1, kk + 1, key);
-                        if (!(kw != 0u && key == kw)) {
-                            update();
-                            P[0] = first;
-                        }
-                    } else {
-                        update();
-                        P[0] = first;
                     }
                 }
                 // back to column order (P[e] holds column (bl + e) mod 16;

@@ -92,14 +92,14 @@ struct F2Smem {
     uint32_t *wkey;     // [2][kF2RowWarps]
     int *rho, *kap;     // [2][kF2Tab] each: the frame, double-buffered by line
     int *kapinv, *perm, *stepof;   // [kF2Tab]; stepof[g]: the step that pivoted row g
-    uint64_t *pan_bar, *y_bar, *b_ready, *next_ready, *rest_done, *fin, *stepbar;
+    uint64_t *pan_bar, *y_bar, *b_ready, *next_ready, *rest_done, *fin;
     uint32_t *tslot;
 };
 
 constexpr size_t kF2BBytes = sizeof(float) * 2 * kF2MaxN * 2 * kF2B;
 constexpr size_t kF2SmemBytes = 2 * kF2BBytes + 2 * sizeof(float2) * kF2B * kF2MaxN +
                                 sizeof(float2) * 2 * kF2RowWarps * kF2B + sizeof(uint32_t) * 2 * kF2RowWarps +
-                                sizeof(int) * 7 * kF2Tab + 7 * sizeof(uint64_t) + 16 + 1024 + 16;
+                                sizeof(int) * 7 * kF2Tab + 6 * sizeof(uint64_t) + 16 + 1024 + 16;
 
 __device__ __forceinline__ F2Smem f2_carve(unsigned char *raw) {
     F2Smem s;
@@ -123,8 +123,7 @@ __device__ __forceinline__ F2Smem f2_carve(unsigned char *raw) {
     s.next_ready = s.pan_bar + 3;
     s.rest_done = s.pan_bar + 4;
     s.fin = s.pan_bar + 5;
-    s.stepbar = s.pan_bar + 6;
-    s.tslot = reinterpret_cast<uint32_t *>(s.pan_bar + 7);
+    s.tslot = reinterpret_cast<uint32_t *>(s.pan_bar + 6);
     return s;
 }
 
@@ -191,7 +190,6 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
         mbar_init(sm.next_ready, 1);
         mbar_init(sm.rest_done, 1);
         mbar_init(sm.fin, 1);
-        mbar_init(sm.stepbar, kF2RowWarps);   // this CTA's 4 row warps, once per pivot step
         fence_mbar_init_cluster();
     }
     tc_fence_before();
@@ -270,7 +268,7 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
         const uint32_t pf_peer = mapa_u32(smem_u32(sm.PF), peer);
         const uint32_t y_peer = mapa_u32(smem_u32(sm.Y), peer);
         const float2 kzv = a.kz2[kz];
-        uint32_t ph_pan = 0, ph_y = 0, ph_next = 0, ph_rest = 0, ph_step = 0;
+        uint32_t ph_pan = 0, ph_y = 0, ph_next = 0, ph_rest = 0;
         int cur = 0;
 
         // ---- S_0 = D_0 (identity frame)
@@ -342,31 +340,22 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                 // ---- the panel's pivot steps, in each CTA on the whole panel.
                 // The rows rotate by one column per step, so that the column
                 // of step kk is always P[0] (no register indexed by kk): after
-                // step kk, P[e] holds panel column (kk + 1 + e) mod 16.  Each
-                // warp publishes its key and winning row in the step's slot
-                // and arrives on the step barrier (4 arrivals per step); a
-                // step's candidates go out as soon as the next column is
-                // updated, the rest of the rows' update (all of it for the
-                // warp's winner) after the arrival, off the step-to-step chain.
-                auto publish = [&](int k, int rot, uint32_t key0, uint32_t key1) {
-                    const int buf = k & 1;
+                // step kk, P[e] holds panel column (kk + 1 + e) mod 16.
+#pragma unroll 1
+                for (int kk = 0; kk < bl; kk++) {
+                    const int k = k0 + kk, buf = k & 1;
+                    const uint32_t key0 = f2_key(P0[0], !used0, t);
+                    const uint32_t key1 = f2_key(P1[0], has1 && !used1, g1);
                     const uint32_t key = key0 > key1 ? key0 : key1;
                     const uint32_t kw = __reduce_max_sync(0xffffffffu, key);
                     if (lane == 0) sm.wkey[buf * kF2RowWarps + warp] = kw;
                     if (kw != 0u && key == kw) {
+                        // the winning row in panel column order
                         float2 *w = sm.wrow + (size_t)(buf * kF2RowWarps + warp) * kF2B;
 #pragma unroll
-                        for (int e = 0; e < kF2B; e++) w[(rot + e) & (kF2B - 1)] = key0 == kw ? P0[e] : P1[e];
+                        for (int e = 0; e < kF2B; e++) w[(kk + e) & (kF2B - 1)] = key0 == kw ? P0[e] : P1[e];
                     }
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive_local(sm.stepbar);
-                };
-                publish(k0, 0, f2_key(P0[0], !used0, t), f2_key(P1[0], has1 && !used1, g1));
-#pragma unroll 1
-                for (int kk = 0; kk < bl; kk++) {
-                    const int k = k0 + kk, buf = k & 1;
-                    wait_cta(sm.stepbar, ph_step);
-                    ph_step ^= 1u;
+                    f2_row_barrier();
                     uint32_t kmax = sm.wkey[buf * kF2RowWarps];
                     int wsel = 0;
 #pragma unroll
@@ -398,47 +387,29 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                     if (t == 0) sm.perm[k] = r >= 0 ? r : 0;
                     // row -= (c / pv) * pivot row, column k becomes -c / pv;
                     // the pivot row is scaled by 1 / pv, its column k becomes 1 / pv
-                    const bool piv0 = t == r, piv1 = g1 == r;
-                    if (piv0) {
+                    {
+                        const float2 s0 = cmul(P0[0], pinv), s1 = cmul(P1[0], pinv);
+#pragma unroll
+                        for (int e = 0; e < kF2B - 1; e++) {
+                            P0[e] = cfms(s0, prow[e], P0[e + 1]);
+                            P1[e] = cfms(s1, prow[e], P1[e + 1]);
+                        }
+                        P0[kF2B - 1] = make_float2(-s0.x, -s0.y);
+                        P1[kF2B - 1] = make_float2(-s1.x, -s1.y);
+                    }
+                    if (t == r) {
+#pragma unroll
+                        for (int e = 0; e < kF2B - 1; e++) P0[e] = cmul(prow[e], pinv);
+                        P0[kF2B - 1] = pinv;
                         used0 = true;
                         sm.stepof[t] = k;
                     }
-                    if (piv1) {
+                    if (g1 == r) {
+#pragma unroll
+                        for (int e = 0; e < kF2B - 1; e++) P1[e] = cmul(prow[e], pinv);
+                        P1[kF2B - 1] = pinv;
                         used1 = true;
                         sm.stepof[g1] = k;
-                    }
-                    const float2 s0 = cmul(P0[0], pinv), s1 = cmul(P1[0], pinv);
-                    auto update = [&]() {
-#pragma unroll
-                        for (int e = 1; e < kF2B - 1; e++) {
-                            P0[e] = piv0 ? cmul(prow[e], pinv) : cfms(s0, prow[e], P0[e + 1]);
-                            P1[e] = piv1 ? cmul(prow[e], pinv) : cfms(s1, prow[e], P1[e + 1]);
-                        }
-                        P0[kF2B - 1] = piv0 ? pinv : make_float2(-s0.x, -s0.y);
-                        P1[kF2B - 1] = piv1 ? pinv : make_float2(-s1.x, -s1.y);
-                    };
-                    // the next column first (P[1] is still the old column k + 1)
-                    const float2 f0 = piv0 ? cmul(prow[0], pinv) : cfms(s0, prow[0], P0[1]);
-                    const float2 f1 = piv1 ? cmul(prow[0], pinv) : cfms(s1, prow[0], P1[1]);
-                    if (kk + 1 < bl) {
-                        const uint32_t key0 = f2_key(f0, !used0, t), key1 = f2_key(f1, has1 && !used1, g1);
-                        const uint32_t key = key0 > key1 ? key0 : key1;
-                        const bool win = __reduce_max_sync(0xffffffffu, key) == key && key != 0u;
-                        if (win) {   // the warp's winner publishes its whole row
-                            update();
-                            P0[0] = f0;
-                            P1[0] = f1;
-                        }
-                        publish(k + 1, kk + 1, key0, key1);
-                        if (!win) {
-                            update();
-                            P0[0] = f0;
-                            P1[0] = f1;
-                        }
-                    } else {
-                        update();
-                        P0[0] = f0;
-                        P1[0] = f1;
                     }
                 }
                 // ---- the panel after its steps back into PF, in column order
