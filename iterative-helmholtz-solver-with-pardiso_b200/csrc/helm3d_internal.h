@@ -158,6 +158,7 @@ struct StencilArgs {
     int R;
     int zchunk = 16;          // z points per thread (autotuned: 8, 16, 32, 64)
     int src_fast = 0;         // grid z order: 0 = z chunks within a source, 1 = sources within a z chunk
+    int smem = 0;             // 1: x/y neighbours from the plane's tile staged in shared memory
 };
 int launch_stencil(const StencilArgs &a, bool adjoint, cudaStream_t s);
 
@@ -284,11 +285,14 @@ bool tune_enabled();
 uint32_t wait_limit_polls(uint32_t dflt);
 // HELM3D_FORCE_<family> as an integer, or -1 when unset
 int tune_forced(const char *family);
-constexpr int kStencilVariants = 8;   // z chunk 16, 8, 32, 64; source-major (0-3) or source-minor (4-7) grid
+// z chunk 16, 8, 32, 64; source-major (0-3) or source-minor (4-7) grid;
+// 8-11: the shared-memory staged kernel, source-minor, z chunk 16, 32, 64, 8
+constexpr int kStencilVariants = 12;
 constexpr int kReduceVariants = 3;    // reduction blocks 2, 1, 4 per SM
 constexpr int kUpdateVariants = 2;    // DCGS2 update pass: basis loads one by one, 8 batched
 int stencil_zchunk(int v);
 int stencil_src_fast(int v);
+int stencil_smem(int v);
 int reduce_blocks(int v);
 
 }  // namespace h3d

@@ -273,6 +273,7 @@ static StencilArgs stencil_args(helm3d_ctx *c, const VecBatch &x, double xscale,
     a.R = R;
     a.zchunk = stencil_zchunk(c->tv_stencil);
     a.src_fast = stencil_src_fast(c->tv_stencil);
+    a.smem = stencil_smem(c->tv_stencil);
     return a;
 }
 
@@ -582,6 +583,7 @@ int tune_solve(helm3d_ctx *c, int R, bool adjoint) {
             StencilArgs t = a0;
             t.zchunk = stencil_zchunk(v);
             t.src_fast = stencil_src_fast(v);
+            t.smem = stencil_smem(v);
             return launch_stencil(t, adjoint, c->stream);
         });
     }

@@ -141,10 +141,14 @@ int tune_pick(helm3d_ctx *c, const char *family, const std::string &shape, int n
 
 int stencil_zchunk(int v) {
     static const int kZ[4] = {16, 8, 32, 64};
+    static const int kZs[4] = {16, 32, 64, 8};
+    if (v >= 8 && v < kStencilVariants) return kZs[v - 8];
     return kZ[(v >= 0 && v < kStencilVariants) ? v % 4 : 0];
 }
 
 int stencil_src_fast(int v) { return (v >= 4 && v < kStencilVariants) ? 1 : 0; }
+
+int stencil_smem(int v) { return (v >= 8 && v < kStencilVariants) ? 1 : 0; }
 
 int reduce_blocks(int v) {
     static const int kPerSm[kReduceVariants] = {2, 1, 4};

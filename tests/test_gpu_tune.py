@@ -34,7 +34,7 @@ def test_factor_shapes(prec, nx, nv, monkeypatch):
         s.close()
 
 
-@pytest.mark.parametrize("family,count", [("SWEEP", 9), ("STENCIL", 8), ("REDUCE", 3), ("UPDATE", 2)])
+@pytest.mark.parametrize("family,count", [("SWEEP", 9), ("STENCIL", 12), ("REDUCE", 3), ("UPDATE", 2)])
 @pytest.mark.parametrize("nrhs", [1, 3])
 def test_solve_shapes_agree(family, count, nrhs, monkeypatch):
     """A batched solve with every variant of one family forced: the same
