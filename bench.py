@@ -241,8 +241,9 @@ def family_bytes_flops(p, its_per_source: float, nsrc: int, e: int = 8):
         "fft_inv": ("hbm", (16.0 + e) * N * R),
         # x read, y written per source, s2 once per z chunk (source-minor order)
         "stencil": ("hbm", 32.0 * N * R + 8.0 * N),
-        # 8 nx^3 real flops per (kz, y-line) block
-        "factor": ("tensor", 8.0 * p.nx ** 3 * p.ny * p.nz),
+        # 8 nx^3 real flops per (kz, y-line) block, per step (the family's
+        # second launch, the blocks' power-of-two scales, takes ~1 %)
+        "factor": ("tensor_per_step", 8.0 * p.nx ** 3 * p.ny * p.nz),
         "krylov": ("hbm_per_step", krylov_step),
     }
 
@@ -261,6 +262,12 @@ def roofline_table(p, prof, its_per_source, nsrc, peaks):
             ach = amount / t / 1e9
             out[k] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                       "bytes_per_step": amount, "ms_per_step": ms, "launches": int(n)}
+            continue
+        if kind == "tensor_per_step":
+            t = ms / 1e3
+            ach = amount / t / 1e12
+            out[k] = {"bound": "tensor", "achieved": ach, "peak": tc, "unit": "TFLOP/s", "frac": ach / tc,
+                      "flops_per_step": amount, "ms_per_step": ms, "launches": int(n)}
             continue
         t = ms / n / 1e3
         if kind == "hbm":
@@ -772,10 +779,11 @@ def cpu_port_value(ps: PortSample, per_it: float, iters: int):
     return ps.factor_s + per_it * iters + (restarts + 1) * ps.residual_s
 
 
-def cpu_port_sample(n: int, cores: int, sample_iters: int = 3):
+def cpu_port_sample(n: int, cores: int, sample_iters: int = RESTART):
     """cpu_baseline of the GPU line: the port's factor of all kz systems and
-    its first few FGMRES iterations on the workload, scaled to the port's
-    own iteration count."""
+    its first restart cycle of FGMRES iterations on the workload (the
+    Gram-Schmidt work grows along a cycle), scaled to the port's own
+    iteration count."""
     iters, src = port_iterations(n, cores)
     if iters is None:
         return {"value": None, "unit": "s", "cores": cores, "kind": "port", "sample": src}
