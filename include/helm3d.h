@@ -180,11 +180,14 @@ int helm3d_apply_prec_batch(helm3d_ctx *ctx, const double *x, double *y, int nrh
  * the point of use (inside an allocator or pool callback, with free memory
  * held by a caching allocator, or on a path that must avoid cudaMalloc's
  * device synchronization).  It allocates nothing: x and y must be device
- * pointers, and the spectral planes use an 8 MiB static device array of the
- * library (nx*ny*nz*8 bytes for C64, *16 for C128 must fit, else
- * HELM3D_ERR_ARG).  The first call on a device looks the array up and should
- * come before any stream capture; calls that overlap on the GPU race on the
- * array.  No counterpart in the reference, which has no device code. */
+ * pointers on the context's device, and the spectral planes use an 8 MiB
+ * static device array of the library (nx*ny*nz*8 bytes for C64, *16 for
+ * C128 must fit, else HELM3D_ERR_ARG).  The first call on a device looks the
+ * array up and should come before any stream capture; the address is kept
+ * for the process, so after cudaDeviceReset the call must not be used on
+ * that device until the process restarts.  Calls that overlap on the GPU
+ * race on the array.  No counterpart in the reference, which has no device
+ * code. */
 int helm3d_apply_prec_noalloc(helm3d_ctx *ctx, const double *x, double *y);
 
 /* Gradient of J = 0.5 sum_s ||P u_s - d_s||^2 with respect to s2 (mode N),
