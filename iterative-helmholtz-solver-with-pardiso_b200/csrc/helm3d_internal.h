@@ -124,17 +124,27 @@ struct SweepArgs {
     int tc_mc = 0;            // complex64, n <= 256: the tensor-core sweep with G^T chunks of tc_mc rows (16, 32)
     int tc_f16 = 0;           // ... with FP16 hi/lo products (K = 16 per MMA), scaled by gscale
     const float *gscale = nullptr;   // [nz][ny] power-of-two scales of the blocks (launch_gscale)
+    int tc_pack = 0;          // the tensor-core sweep on the packed factor (sweep_tcp.cu)
+    const void *gpack = nullptr;     // the packed factor (launch_gpack), or null
 };
 int launch_sweep(bool c64, const SweepArgs &a, cudaStream_t s);
 // the sweep's launch variants the autotuner times: stage and ring sizes of
 // the CUDA-core kernels (0-5), the tensor-core kernel's chunk (6, 7), the
-// tensor-core kernel with FP16 products (8)
-constexpr int kSweepVariants = 9;
+// tensor-core kernel with FP16 products (8), the tensor-core kernel on the
+// packed factor (9)
+constexpr int kSweepVariants = 10;
 // power-of-two scale of every complex64 block G_j for the FP16 products
 int launch_gscale(const void *Gt, int n, int ny, int nz, int ldg, float *gscale, cudaStream_t s);
 void sweep_variant(int v, SweepArgs &a);
 bool sweep_tc_supported(const SweepArgs &a);   // shape and shared memory fit
 int launch_sweep_tc(const SweepArgs &a, int mc, cudaStream_t s);
+// the complex64 factor (n <= 256) packed once into FP16 hi/lo tiles of
+// s_j G_j (s_j = gscale) in the tensor core's operand layout, gpack_bytes
+// bytes (about those of the complex64 factor), for launch_sweep_tcp
+size_t gpack_bytes(int n, int ny, int nz);
+int launch_gpack(const void *Gt, int n, int ny, int nz, int ldg, const float *gscale, void *Gp, cudaStream_t s);
+bool sweep_tcp_supported(const SweepArgs &a);
+int launch_sweep_tcp(const SweepArgs &a, cudaStream_t s);
 constexpr int kMaxBatch = 16;  // right-hand sides per preconditioner launch
 
 // Classical Gram-Schmidt takes a second pass when the first left less than
@@ -335,6 +345,7 @@ struct helm3d_ctx {
     // device buffers
     void *d_Gt = nullptr;          // factor
     float *d_gscale = nullptr;     // [nz][ny] scales of the complex64 blocks (FP16 sweep)
+    void *d_gpack = nullptr;       // complex64, n <= 256: the factor packed as FP16 hi/lo tiles (launch_gpack)
     size_t Gt_bytes = 0;
     void *d_tw = nullptr;          // FFT tables (precision P)
     void *d_cmx = nullptr, *d_cpx = nullptr, *d_cmy = nullptr, *d_cpy = nullptr;   // P precision

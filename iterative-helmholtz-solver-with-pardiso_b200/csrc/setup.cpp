@@ -408,6 +408,7 @@ int ctx_setup_grid(helm3d_ctx *c) {
     c->Gt_bytes = esz * (size_t)nz * ny * nx * c->ldg;
     if ((rc = dalloc(c, &c->d_Gt, c->Gt_bytes, "block LU factor"))) return rc;
     if ((rc = dalloc(c, (void **)&c->d_gscale, sizeof(float) * (size_t)nz * ny, "block scales"))) return rc;
+    if (c->c64 && nx <= 256 && (rc = dalloc(c, &c->d_gpack, gpack_bytes(nx, ny, nz), "packed factor"))) return rc;
     return HELM3D_OK;
 }
 
@@ -538,6 +539,12 @@ int ctx_factor(helm3d_ctx *c) {
         rc = timed(c, HELM3D_K_FACTOR, 1,
                    [&] { return launch_gscale(c->d_Gt, a.n, a.ny, a.nz, a.ldg, c->d_gscale, c->stream); });
         if (rc) return set_error(c, rc, "block scales launch failed");
+        if (c->d_gpack) {
+            rc = timed(c, HELM3D_K_FACTOR, 1, [&] {
+                return launch_gpack(c->d_Gt, a.n, a.ny, a.nz, a.ldg, c->d_gscale, c->d_gpack, c->stream);
+            });
+            if (rc) return set_error(c, rc, "factor packing launch failed");
+        }
     }
     int st = 0;
     rc = cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");

@@ -195,6 +195,7 @@ static SweepArgs sweep_args(helm3d_ctx *c, int R, bool adjoint) {
     s.dxy = adjoint ? c->d_dxy : nullptr;
     s.status = c->d_status;
     s.gscale = c->d_gscale;
+    s.gpack = c->d_gpack;
     sweep_variant(c->tv_sweep[adjoint ? 1 : 0], s);
     return s;
 }

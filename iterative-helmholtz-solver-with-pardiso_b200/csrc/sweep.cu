@@ -524,21 +524,24 @@ template <typename R, int G> static int sweep_g(const SweepArgs &sa, cudaStream_
 }
 
 void sweep_variant(int v, SweepArgs &a) {
-    static const int kStage[kSweepVariants] = {16, 8, 32, 16, 8, 32, 16, 16, 16};
-    static const int kRingKb[kSweepVariants] = {200, 200, 200, 100, 100, 100, 200, 200, 200};
-    static const int kTcMc[kSweepVariants] = {0, 0, 0, 0, 0, 0, 32, 16, 32};
-    static const int kTcF16[kSweepVariants] = {0, 0, 0, 0, 0, 0, 0, 0, 1};
+    static const int kStage[kSweepVariants] = {16, 8, 32, 16, 8, 32, 16, 16, 16, 16};
+    static const int kRingKb[kSweepVariants] = {200, 200, 200, 100, 100, 100, 200, 200, 200, 200};
+    static const int kTcMc[kSweepVariants] = {0, 0, 0, 0, 0, 0, 32, 16, 32, 0};
+    static const int kTcF16[kSweepVariants] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 0};
+    static const int kTcPack[kSweepVariants] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 1};
     if (v < 0 || v >= kSweepVariants) v = 0;
     a.stage_kb = kStage[v];
     a.ring_kb = kRingKb[v];
     a.tc_mc = kTcMc[v];
     a.tc_f16 = kTcF16[v];
+    a.tc_pack = kTcPack[v];
 }
 
 int launch_sweep(bool c64, const SweepArgs &sa, cudaStream_t s) {
     if (sa.n < 1 || sa.n > kSweepMaxN || sa.R < 1 || sa.R > kMaxBatch) return HELM3D_ERR_ARG;
     // the tensor-core kernel where it applies (complex64, n <= 256, shared memory fits)
     if (c64 && sa.tc_mc && sweep_tc_supported(sa)) return launch_sweep_tc(sa, sa.tc_mc, s);
+    if (c64 && sa.tc_pack && sweep_tcp_supported(sa)) return launch_sweep_tcp(sa, s);
     // complex64 batches of 3 or more: the register-tiled kernel (its 16-byte
     // tile loads need ldg, the padded row length, to be a multiple of 4)
     if (c64 && sa.R >= 3 && sa.ldg % 4 == 0) return sa.dxy ? sweep_tiled<true>(sa, s) : sweep_tiled<false>(sa, s);

@@ -16,7 +16,7 @@
 // D[i][2r] + i D[i][2r+1] = (G_j v)[i][r].  M = 128 (rows i, n <= 128),
 // N = 2 RR, K = 2 n padded to the chunk.
 //
-// Roles (14 warps):
+// Roles (15 warps):
 //   * warp 12, one lane: streams G_j^T (rows m, i contiguous, as the factor
 //     stores it) chunk by chunk (MC rows m) into a ring of shared-memory
 //     stages with 1D bulk copies, as far ahead as the ring allows;
@@ -30,10 +30,15 @@
 //     line's v to shared memory and from it the next B (hi and lo, canonical
 //     no-swizzle K-major layout, 16-byte units in address order so that the
 //     stores of a warp are contiguous);
-//   * warp 13, one lane: issues the MMAs of a line (A from TMEM, B from
-//     shared memory) chunk by chunk as the buffers fill, and commits them to
-//     the buffer-free barriers and, after the last chunk, to the
-//     accumulator-ready barrier.
+//   * warps 13 and 14, one lane each: issue the MMAs of a line (A from TMEM,
+//     B from shared memory) chunk by chunk as the buffers fill, and commit
+//     them to the buffer-free barriers and, after the last chunk, to the
+//     accumulator-ready barrier.  The issuing thread waits about 70 cycles
+//     per tcgen05.mma whatever its N (measured on the B200), while two
+//     issuers' MMAs run side by side, so the line's MMAs are split between
+//     two issuers: with two row blocks issuer u takes row block u, with one
+//     issuer 0 takes the a_hi [b_hi; b_lo] products and issuer 1 the
+//     a_lo b_hi products, into an accumulator of their own.
 // The dependence chain per line is MMAs -> epilogue -> B; the conversion of
 // the next chunks and the bulk copies run beside it.  Ring positions advance
 // by counters (no integer division in the loops).  Every wait is bounded; on
@@ -41,8 +46,6 @@
 // (results then invalid), waits (bounded) for its own MMAs and bulk copies,
 // frees its TMEM and returns.
 #include <cuda_runtime.h>
-
-#include <cuda_fp16.h>
 
 #include <cstdint>
 
@@ -56,8 +59,9 @@ namespace h3d {
 constexpr int kTcConvWarps = 4;          // warps 0-3: G^T chunks -> TMEM
 constexpr int kTcEpiWarps = 8;           // warps 4-11: finish each line, build the next B
 constexpr int kTcProducerWarp = kTcConvWarps + kTcEpiWarps;
-constexpr int kTcMmaWarp = kTcProducerWarp + 1;
-constexpr int kTcThreads = (kTcMmaWarp + 1) * 32;
+constexpr int kTcMmaWarp = kTcProducerWarp + 1;   // first of the MMA issuers
+constexpr int kTcMmaWarps = 2;
+constexpr int kTcThreads = (kTcMmaWarp + kTcMmaWarps) * 32;
 constexpr int kTcMaxN = 256;             // two row blocks of MMA M = 128
 constexpr int kTcBuf = 3;                // TMEM A chunk buffers
 constexpr uint32_t kTcCols = 512;        // TMEM columns: D of row block rb at 4 RR rb, buffers from 128
@@ -90,35 +94,9 @@ template <bool ADJ> __device__ __forceinline__ float2 tc_adj_out(const SweepTcK 
     return cmul(make_float2(x.x, -x.y), a.dxy[(long)(a.ny + line) * a.n + i]);
 }
 
-// FP16 hi/lo of a pair (x, y), each as a packed pair (x in the low half):
-// hi = x rounded to 11 significant bits in FP32 (exact in FP16 in its
-// normal range), lo = x - hi (exact in FP32) rounded to FP16 -- two
-// conversions per pair
-__device__ __forceinline__ uint2 f16_split2(float x, float y) {
-    const float hx = tf32_round(x), hy = tf32_round(y);
-    const __half2 hi = __floats2half2_rn(hx, hy);
-    const __half2 lo = __floats2half2_rn(x - hx, y - hy);
-    return make_uint2(*reinterpret_cast<const uint32_t *>(&hi), *reinterpret_cast<const uint32_t *>(&lo));
-}
-
-// 2^(13 - e) for mx in [2^e, 2^(e+1)): scales the largest entry into
-// [2^13, 2^14) (1 for mx = 0 or not finite)
-__device__ __forceinline__ float pow2_scale_13(float mx) {
-    const uint32_t b = __float_as_uint(mx);
-    const int ex = (int)((b >> 23) & 0xffu);
-    if (mx <= 0.f || ex == 0xff) return 1.f;
-    int e = (ex == 0 ? -126 : ex - 127);
-    e = max(-100, min(100, e));
-    return __uint_as_float((uint32_t)(127 + 13 - e) << 23);
-}
-
-// 1 / s for a power of two s (exact)
-__device__ __forceinline__ float pow2_inv(float s) {
-    return __uint_as_float((254u - ((__float_as_uint(s) >> 23) & 0xffu)) << 23);
-}
-
 // MB row blocks of 128 rows i (n <= 128 MB).  TMEM: the accumulator of row
-// block rb at columns [2 NR rb, 2 NR (rb + 1)); chunk buffer b at 128 + b BW,
+// block rb at columns [2 NR rb, 2 NR (rb + 1)) (with one row block, the
+// a_lo b_hi products in their own at [2 NR, 3 NR)); chunk buffer b at 128 + b BW,
 // row block rb's hi at + 2 KC rb, its lo KC further (3 buffers fit for
 // MB = 1 with MC <= 32 and for MB = 2 with MC = 16, or MC = 32 with F16).
 //
@@ -135,7 +113,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
     constexpr int KC = F16 ? MC : 2 * MC;   // TMEM columns of hi, and of lo, per chunk (K = 2 MC)
     constexpr int RH = RR / 2;        // right-hand sides per epilogue warp
     constexpr int BW = MB * 2 * KC;   // TMEM columns of one chunk buffer
-    static_assert(MB * 2 * NR <= 128 && 128 + kTcBuf * BW <= (int)kTcCols, "TMEM layout");
+    static_assert((MB == 2 ? 4 * NR : 3 * NR) <= 128 && 128 + kTcBuf * BW <= (int)kTcCols, "TMEM layout");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const int n = a.n, ny = a.ny, ldg = a.ldg, Rn = a.nrhs, npad = a.npad, cpl = a.cpl;
     const int Kp = 2 * npad;
@@ -157,8 +135,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
     uint64_t *a_empty = a_full + kTcBuf;
     uint64_t *b_full = a_empty + kTcBuf;
     uint64_t *d_full = b_full + 1;
-    uint64_t *fin = d_full + 1;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(fin + 1);
+    uint64_t *fin = d_full + 1;       // [kTcMmaWarps]
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(fin + kTcMmaWarps);
     float2 *P = a.planes + (long)kz * ny * Rn * n;   // line j, rhs r, row i at ((j*Rn + r)*n + i)
 
     if (warp == 0) tmem_alloc(tslot, kTcCols);
@@ -169,11 +147,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
         }
         for (int b = 0; b < kTcBuf; b++) {
             mbar_init(&a_full[b], kTcConvWarps);
-            mbar_init(&a_empty[b], 1);
+            mbar_init(&a_empty[b], kTcMmaWarps);
         }
         mbar_init(b_full, kTcEpiWarps);
-        mbar_init(d_full, 1);
-        mbar_init(fin, 1);
+        mbar_init(d_full, kTcMmaWarps);
+        for (int u = 0; u < kTcMmaWarps; u++) mbar_init(&fin[u], 1);
         fence_mbar_init_cluster();
     }
     tc_fence_before();
@@ -226,9 +204,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                 mbar_wait_bounded_cta(smem_u32(&raw_full[sl]), ph, kTcWaitLimit);
             }
         }
-    } else if (warp == kTcMmaWarp) {
-        // --------------------------------------------------- MMA issuer
+    } else if (warp >= kTcMmaWarp) {
+        // -------------------------------------------------- MMA issuers
         if (lane == 0) {
+            const int u = warp - kTcMmaWarp;
             // Blo follows Bhi as further 8-row groups of the same layout, so
             // one descriptor with N = 2 NR rows covers [B_hi; B_lo]
             const uint32_t idesc2 = F16 ? umma_idesc_f16(2 * NR) : umma_idesc_tf32(2 * NR);
@@ -236,7 +215,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
             constexpr int KE = F16 ? 8 : 4;   // K elements per 16-byte core-matrix row
             constexpr int KS = F16 ? 16 : 8;  // K per MMA
             const uint32_t sbo = (uint32_t)(Kp / KE) * 128u;
-            const uint32_t bhi = smem_u32(Bhi);
+            // descriptor of B at K = 0; K steps advance its start address
+            // field (16-byte units: one core matrix of 128 bytes is 8), which
+            // stays below 2^14 for any shared-memory address
+            const uint64_t db0 = umma_desc(smem_u32(Bhi), 128, sbo);
+            // what issuer u issues: D_rb[0, 2NR) (+)= a_hi [b_hi; b_lo] and
+            // D_rb[0, NR) += a_lo b_hi for row block rb = u (two row blocks),
+            // or with one row block the a_hi products into D_a = [0, 2NR)
+            // (issuer 0) and the a_lo products into D_b = [2NR, 3NR) (issuer 1)
+            const bool hi_part = MB == 2 || u == 0, lo_part = MB == 2 || u == 1;
+            const int rb = MB == 2 ? u : 0;
+            const uint32_t d_hi = tmem + (uint32_t)(rb * 2 * NR);
+            const uint32_t d_lo = MB == 2 ? d_hi : tmem + (uint32_t)(2 * NR);
             RingPos bp;
             for (int t = 0; t < nsteps; t++) {
                 wait(b_full, (uint32_t)(t & 1));
@@ -245,24 +235,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                     const int b = bp.slot;
                     wait(&a_full[b], bp.phase);
                     tc_fence_after();
-                    const uint32_t buf = tmem + 128u + (uint32_t)(b * BW);
+                    // 8 TMEM columns of A per MMA: 8 tf32, or 16 fp16 in pairs
+                    const uint32_t ahi0 = tmem + 128u + (uint32_t)(b * BW + rb * 2 * KC);
+                    const uint64_t dbc = db0 + (uint64_t)((c * 2 * MC / KE) * 8);
 #pragma unroll
                     for (int ks = 0; ks < 2 * MC / KS; ks++) {
-                        const uint32_t koff = (uint32_t)((c * 2 * MC + ks * KS) / KE) * 128u;
-                        const uint64_t db = umma_desc(bhi + koff, 128, sbo);
-#pragma unroll
-                        for (int rb = 0; rb < MB; rb++) {
-                            // D_rb[0, 2NR) (+)= a_hi [b_hi; b_lo], then D_rb[0, NR) += a_lo b_hi
-                            // (8 TMEM columns of A per MMA: 8 tf32, or 16 fp16 in pairs)
-                            const uint32_t d = tmem + (uint32_t)(rb * 2 * NR);
-                            const uint32_t ahi = buf + (uint32_t)(rb * 2 * KC + ks * 8);
-                            if constexpr (F16) {
-                                umma_f16_ts(d, ahi, db, idesc2, (c > 0 || ks > 0) ? 1u : 0u);
-                                umma_f16_ts(d, ahi + (uint32_t)KC, db, idesc1, 1u);
-                            } else {
-                                umma_tf32_ts(d, ahi, db, idesc2, (c > 0 || ks > 0) ? 1u : 0u);
-                                umma_tf32_ts(d, ahi + (uint32_t)KC, db, idesc1, 1u);
-                            }
+                        const uint64_t db = dbc + (uint64_t)(ks * (KS / KE) * 8);
+                        const uint32_t ahi = ahi0 + (uint32_t)(ks * 8);
+                        const uint32_t first = (c > 0 || ks > 0) ? 1u : 0u;
+                        if constexpr (F16) {
+                            if (hi_part) umma_f16_ts(d_hi, ahi, db, idesc2, first);
+                            if (lo_part) umma_f16_ts(d_lo, ahi + (uint32_t)KC, db, idesc1, MB == 2 ? 1u : first);
+                        } else {
+                            if (hi_part) umma_tf32_ts(d_hi, ahi, db, idesc2, first);
+                            if (lo_part) umma_tf32_ts(d_lo, ahi + (uint32_t)KC, db, idesc1, MB == 2 ? 1u : first);
                         }
                     }
                     umma_commit(&a_empty[b]);
@@ -270,9 +256,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
                 }
                 umma_commit(d_full);
             }
-            // every MMA of this CTA complete before the TMEM is freed
-            umma_commit(fin);
-            mbar_wait_bounded_cta(smem_u32(fin), 0u, kTcWaitLimit);
+            // every MMA of this issuer complete before the TMEM is freed
+            umma_commit(&fin[u]);
+            mbar_wait_bounded_cta(smem_u32(&fin[u]), 0u, kTcWaitLimit);
         }
     } else if (warp < kTcConvWarps) {
         // --------------------------------------------------- converters
@@ -517,24 +503,33 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
 #pragma unroll
             for (int rb = 0; rb < MB; rb++) {
                 const int row = i + 128 * rb;
-                // D = a_hi b_hi + a_lo b_hi (columns c) + a_hi b_lo (columns NR + c)
+                // D = a_hi b_hi (+ a_lo b_hi with two row blocks) (columns c) +
+                // a_hi b_lo (columns NR + c); with one row block a_lo b_hi at 2 NR + c
                 const uint32_t dcol = (uint32_t)(rb * 2 * NR + wg * RR);
-                float d[2 * RR];
+                float d[2 * RR], d3[RR];
                 if constexpr (RR == 16) {
                     tmem_ld16_nowait(trow + dcol, d);
                     tmem_ld16_nowait(trow + dcol + (uint32_t)NR, d + RR);
+                    if constexpr (MB == 1) tmem_ld16_nowait(trow + dcol + (uint32_t)(2 * NR), d3);
                 } else {
                     tmem_ld8_nowait(trow + dcol, d);
                     tmem_ld8_nowait(trow + dcol + (uint32_t)NR, d + RR);
+                    if constexpr (MB == 1) tmem_ld8_nowait(trow + dcol + (uint32_t)(2 * NR), d3);
                 }
                 tmem_wait_ld(d);
+                if constexpr (MB == 1) {
+                    tmem_wait_ld(d3);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < RR; k++) d3[k] = 0.f;
+                }
 #pragma unroll
                 for (int k = 0; k < RH; k++) {
                     const int r = wg * RH + k;
                     const float2 pk = pv[rb][k];
                     const float2 pre = (ADJ && fwd && !last_fwd) ? cmul(dx[rb], make_float2(pk.x, -pk.y)) : pk;
-                    const float2 acc = make_float2((d[2 * k] + d[RR + 2 * k]) * us[k],
-                                                   (d[2 * k + 1] + d[RR + 2 * k + 1]) * us[k]);
+                    const float2 acc = make_float2((d[2 * k] + d[RR + 2 * k] + d3[2 * k]) * us[k],
+                                                   (d[2 * k + 1] + d[RR + 2 * k + 1] + d3[2 * k + 1]) * us[k]);
                     float2 out, vn;
                     bool fin_x;   // out is this line's final x
                     if (fwd) {
@@ -636,7 +631,7 @@ static bool tc_shape(const SweepArgs &sa, int mc, TcShape &sh) {
     // B hi and lo: tf32 words, or FP16 halves (half the bytes)
     const size_t bbytes = 2 * sizeof(float) * (size_t)(2 * sh.RR) * (2 * sh.npad) / (sh.f16 ? 2 : 1);
     const size_t vbytes = sizeof(float2) * (size_t)sh.RR * (sh.npad + 2) + sizeof(float) * 4 * sh.RR;
-    const size_t fixed = bbytes + vbytes + sizeof(uint64_t) * (2 * kTcBuf + 3) + 16;
+    const size_t fixed = bbytes + vbytes + sizeof(uint64_t) * (2 * kTcBuf + 2 + kTcMmaWarps) + 16;
     const size_t optin = device_info().smem_optin;
     const size_t per_stage = sh.stage_bytes + 2 * sizeof(uint64_t);
     if (fixed + 2 * per_stage > optin) return false;

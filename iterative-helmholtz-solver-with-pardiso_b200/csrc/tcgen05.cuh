@@ -6,6 +6,8 @@
 // core matrix is 8 rows x 16 bytes (4 tf32 along K), K-adjacent core
 // matrices are LBO = 128 bytes apart, 8-row groups SBO bytes apart.
 #pragma once
+#include <cuda_fp16.h>
+
 #include <cstdint>
 #include <cstring>
 
@@ -51,6 +53,34 @@ __host__ __device__ inline void tf32_split_fast(float v, float &hi, float &lo) {
 // rows hold KC elements (8-row groups SBO = KC / 4 * 128 bytes apart)
 __host__ __device__ inline uint32_t canon_off(int row, int kk, int KC) {
     return (uint32_t)((row >> 3) * (KC / 4) * 128 + (kk >> 2) * 128 + (row & 7) * 16 + (kk & 3) * 4);
+}
+
+// ------------------------------------------------ FP16 hi/lo operands
+// FP16 hi/lo of a pair (x, y), each as a packed pair (x in the low half):
+// hi = x rounded to 11 significant bits in FP32 (exact in FP16 in its
+// normal range), lo = x - hi (exact in FP32) rounded to FP16 -- two
+// conversions per pair
+__device__ __forceinline__ uint2 f16_split2(float x, float y) {
+    const float hx = tf32_round(x), hy = tf32_round(y);
+    const __half2 hi = __floats2half2_rn(hx, hy);
+    const __half2 lo = __floats2half2_rn(x - hx, y - hy);
+    return make_uint2(*reinterpret_cast<const uint32_t *>(&hi), *reinterpret_cast<const uint32_t *>(&lo));
+}
+
+// 2^(13 - e) for mx in [2^e, 2^(e+1)): scales the largest entry into
+// [2^13, 2^14) (1 for mx = 0 or not finite)
+__device__ __forceinline__ float pow2_scale_13(float mx) {
+    const uint32_t b = __float_as_uint(mx);
+    const int ex = (int)((b >> 23) & 0xffu);
+    if (mx <= 0.f || ex == 0xff) return 1.f;
+    int e = (ex == 0 ? -126 : ex - 127);
+    e = max(-100, min(100, e));
+    return __uint_as_float((uint32_t)(127 + 13 - e) << 23);
+}
+
+// 1 / s for a power of two s (exact)
+__device__ __forceinline__ float pow2_inv(float s) {
+    return __uint_as_float((254u - ((__float_as_uint(s) >> 23) & 0xffu)) << 23);
 }
 
 // ------------------------------------------------------------ tcgen05 PTX
@@ -101,6 +131,17 @@ __device__ __forceinline__ void umma_f16_ts(uint32_t tmem_d, uint32_t tmem_a, ui
         "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
         :
         : "r"(tmem_d), "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+// kind::f16: D (TMEM) (+)= A (shared memory) B^T (shared memory), K = 16
+__device__ __forceinline__ void umma_f16_ss(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        :
+        : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
 // arrive on `bar` once every tcgen05 operation this thread issued so far has completed

@@ -34,7 +34,7 @@ def test_factor_shapes(prec, nx, nv, monkeypatch):
         s.close()
 
 
-@pytest.mark.parametrize("family,count", [("SWEEP", 9), ("STENCIL", 12), ("REDUCE", 3), ("UPDATE", 2)])
+@pytest.mark.parametrize("family,count", [("SWEEP", 10), ("STENCIL", 12), ("REDUCE", 3), ("UPDATE", 2)])
 @pytest.mark.parametrize("nrhs", [1, 3])
 def test_solve_shapes_agree(family, count, nrhs, monkeypatch):
     """A batched solve with every variant of one family forced: the same
@@ -60,22 +60,24 @@ def test_solve_shapes_agree(family, count, nrhs, monkeypatch):
         s.close()
 
 
-@pytest.mark.parametrize("nx,nrhs", [(128, 16), (96, 8), (100, 3), (24, 16), (20, 5), (200, 16), (160, 5), (129, 3)])
+@pytest.mark.parametrize("nx,nrhs", [(128, 16), (96, 8), (100, 3), (24, 16), (20, 5), (200, 16), (160, 5), (129, 3),
+                                     (250, 1), (9, 2)])
 def test_tensor_core_sweep_batches(nx, nrhs, monkeypatch):
     """The tensor-core sweep (variants 6 and 7: G^T chunks of 32 and 16 rows,
     3xTF32 products; variant 8: FP16 hi/lo products with power-of-two block
-    and right-hand-side scales) in a batched complex64 preconditioner apply, forward and
-    adjoint, against the oracle's M^{-1} x_r and M^{-H} x_r of every vector,
-    beside the CUDA-core sweep (variant 0); block sizes one full row block
-    (128), padded (96, 100, 24, 20), two row blocks (200, 160, 129), batches
-    padded to 8 or 16."""
+    and right-hand-side scales; variant 9: the same products on the factor
+    packed once into FP16 hi/lo tiles) in a batched complex64 preconditioner
+    apply, forward and adjoint, against the oracle's M^{-1} x_r and M^{-H} x_r
+    of every vector, beside the CUDA-core sweep (variant 0); block sizes one
+    full row block (128), padded (96, 100, 24, 20, 9), two row blocks (200,
+    160, 129, 250), batches padded to 8 or 16."""
     p = small_problem(nx, 10, 8, pml=3, seed=nx + nrhs)
     on = mode_n.setup(p, beta_prec=0.25)
     X = np.stack([rand_c(p.shape, seed=100 + r) for r in range(nrhs)])
     ref = [on.apply_prec(X[r]) for r in range(nrhs)]
     refh = [on.apply_prec_adjoint(X[r]) for r in range(nrhs)]
     s = mode_n_solver(p, precision=1, beta_prec=0.25)
-    for var in (0, 6, 7, 8):
+    for var in (0, 6, 7, 8, 9):
         monkeypatch.setenv("HELM3D_FORCE_SWEEP", str(var))
         Y = s.apply_prec_batch(X)
         Yh = s.apply_prec_batch(X, adjoint=True)
