@@ -487,12 +487,17 @@ def run_kernels(args):
     o = helm3d.default_opts(precision=helm3d.PREC_C64, restart=1, tol=TOL, beta_prec=BETA_PREC, max_iter=1,
                             device=0, z_transform=helm3d.ZT_PML_EIGEN)
     s = helm3d.Solver(grid, torch.from_numpy(np.ascontiguousarray(p.s2)).to(dev), o)
+    def one():
+        if args.prec_applies:
+            s.apply_prec_batch(F)   # launched one by one (no graph): profiler captures see each kernel
+        else:
+            s.solve(F, nrhs=BATCH, u=U, allow_not_converged=True)
     for _ in range(args.warmup):
-        s.solve(F, nrhs=BATCH, u=U, allow_not_converged=True)
+        one()
     torch.cuda.synchronize()
     s.profile(True)
     for _ in range(args.steps):
-        s.solve(F, nrhs=BATCH, u=U, allow_not_converged=True)
+        one()
     prof = s.profile_read()
     s.close()
     N = p.nx * p.ny * p.nz
@@ -504,7 +509,8 @@ def run_kernels(args):
     }
     peaks, peak_kind = read_peaks()
     peak = float(peaks["hbm_gbs"])
-    out = {"mode": "kernels", "workload": f"{p.nx}x{p.ny}x{p.nz}, {BATCH} sources, c64 preconditioner, PML eigenbasis",
+    out = {"mode": "kernels" + (" (preconditioner applies)" if args.prec_applies else ""),
+           "workload": f"{p.nx}x{p.ny}x{p.nz}, {BATCH} sources, c64 preconditioner, PML eigenbasis",
            "steps": args.steps, "peak_gbs": peak, "peak_source": peak_kind, "kernels": {}}
     for k, (ms, n) in prof.items():
         d = {"ms_total": round(ms, 4), "launches": int(n)}
@@ -875,6 +881,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernels", action="store_true",
                     help="per-kernel microbench: batched FGMRES(1) iterations instead of full solves")
+    ap.add_argument("--prec-applies", action="store_true",
+                    help="--kernels: batched preconditioner applies (z-transforms and sweep) instead")
     ap.add_argument("--workload", default="headline", choices=["headline", "c3", "c4", "c5", "n200"],
                     help="c3: 160^3 mixed precision, FGMRES(30); c4: 96^3 x 16 sources + 8 uneven grids as one "
                          "group; c5: 200^3 misfit gradient with finite-difference check; n200: 200^3 batched "

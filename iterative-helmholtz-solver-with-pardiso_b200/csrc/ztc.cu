@@ -19,16 +19,17 @@
 //     kZcDepth chunks ahead into registers (the loads stay in flight), splits
 //     them into tf32 hi/lo and stores them into the stage (one 16-byte store
 //     per pair of j), then arrives on the stage's a_full barrier;
-//   * warp 12 (producer): one bulk copy per chunk of B (hi and lo, already in
+//   * warp 16 (producer): one bulk copy per chunk of B (hi and lo, already in
 //     the tensor-core layout in global memory, prepared once per grid; the
 //     same for every tile, so it comes from L2);
-//   * warp 13 (MMA): 3 x (KC / 8) MMAs per chunk into the tile's TMEM
+//   * warp 17 (MMA): 3 x (KC / 8) MMAs per chunk into the tile's TMEM
 //     accumulator, committed to the stage's empty barrier (which gates its
 //     refill); after the tile's last chunk a commit to the accumulator's
 //     full barrier;
-//   * warps 8-11 (epilogue): warp w reads TMEM lanes 32 (w % 4) + [0, 32)
-//     (tcgen05.ld 32x32b) and writes the outputs of those positions, then
-//     frees the accumulator.
+//   * warps 8-15 (epilogue): warps w and w + 4 read TMEM lanes 32 (w % 4) +
+//     [0, 32) (tcgen05.ld 32x32b), each half the columns, 64 columns per
+//     wait; the accumulator is freed as soon as its last load has landed,
+//     and the outputs of those positions are stored after that
 // Two accumulators (2 N <= 512 TMEM columns, nz <= 128) let the epilogue of
 // one tile run under the MMAs of the next; above that one accumulator.
 // Shared-memory operands use the no-swizzle K-major canonical layout: 8 rows x
@@ -52,10 +53,10 @@ namespace h3d {
 
 constexpr int kZcM = 128;                    // tile positions (MMA M)
 constexpr int kZcConvWarps = 8;              // warps 0-7
-constexpr int kZcEpiWarps = 4;               // warps 8-11
-constexpr int kZcProducerWarp = 12;
-constexpr int kZcMmaWarp = 13;
-constexpr int kZcThreads = 14 * 32;
+constexpr int kZcEpiWarps = 8;               // warps 8-15
+constexpr int kZcProducerWarp = 16;
+constexpr int kZcMmaWarp = 17;
+constexpr int kZcThreads = 18 * 32;
 constexpr int kZcDepth = 4;                  // input chunks in flight per converter thread
 constexpr int kZcMaxStages = 8;
 constexpr uint32_t kZcStageBudget = 200u * 1024u;
@@ -208,14 +209,14 @@ __global__ void __launch_bounds__(kZcThreads, 1) ztc_kernel(ZtcArgs a) {
         // ------------------------------------------------------ converters
         const int p = tid & (kZcM - 1), half = tid >> 7;
         In buf[kZcDepth][2 * JP];
-        double bs[kZcDepth];
+        float bs[kZcDepth];   // the chunk's input scale, in FP32
         ZtcCursor<FWD> lc;   // loads: kZcDepth chunks ahead of the conversions
         lc.start(a, p);
 #pragma unroll
         for (int d = 0; d < kZcDepth; d++) {
             if (d < total) {
                 ztc_load<FWD, JP>(a, lc.src, lc.c * (KC / 2), half, buf[d]);
-                bs[d] = lc.src.s;
+                bs[d] = (float)lc.src.s;
                 lc.next(a, p);
             }
         }
@@ -233,12 +234,16 @@ __global__ void __launch_bounds__(kZcThreads, 1) ztc_kernel(ZtcArgs a) {
 #pragma unroll
                         for (int t = 0; t < JP; t++) {
                             const In x0 = buf[d][2 * t], x1 = buf[d][2 * t + 1];
-                            const double s = bs[d];
+                            // in FP32: the input rounded once to FP32 (the
+                            // planes' own precision), then hi + lo with lo
+                            // left in FP32 (the tensor core reads its tf32
+                            // part): 22 significant bits, as the FP64 split
+                            const float s = bs[d];
                             float4 hi, lo;
-                            tf32_split(s * (double)x0.x, hi.x, lo.x);
-                            tf32_split(s * (double)x0.y, hi.y, lo.y);
-                            tf32_split(s * (double)x1.x, hi.z, lo.z);
-                            tf32_split(s * (double)x1.y, hi.w, lo.w);
+                            tf32_split_fast((float)x0.x * s, hi.x, lo.x);
+                            tf32_split_fast((float)x0.y * s, hi.y, lo.y);
+                            tf32_split_fast((float)x1.x * s, hi.z, lo.z);
+                            tf32_split_fast((float)x1.y * s, hi.w, lo.w);
                             const uint32_t off = canon_off(p, 4 * (half + 2 * t), KC);
                             *reinterpret_cast<float4 *>(Ahi + off) = hi;
                             *reinterpret_cast<float4 *>(Alo + off) = lo;
@@ -250,7 +255,7 @@ __global__ void __launch_bounds__(kZcThreads, 1) ztc_kernel(ZtcArgs a) {
                     sp.next(S);
                     if (g + kZcDepth < total) {
                         ztc_load<FWD, JP>(a, lc.src, lc.c * (KC / 2), half, buf[d]);
-                        bs[d] = lc.src.s;
+                        bs[d] = (float)lc.src.s;
                         lc.next(a, p);
                     }
                 }
@@ -336,7 +341,10 @@ __global__ void __launch_bounds__(kZcThreads, 1) ztc_kernel(ZtcArgs a) {
     } else {
         // -------------------------------------------------------- epilogue
         const int q = warp & 3;   // TMEM lanes 32 q + [0, 32) (a warp reads its own quarter)
+        const int eh = (warp - kZcConvWarps) >> 2;   // which half of the 16-column groups
         const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
+        const int G = N / 16, gsplit = (G + 1) / 2;
+        const int g_lo = eh == 0 ? 0 : gsplit, g_hi = eh == 0 ? gsplit : G;
         RingPos ap;
         for (int i = 0; i < my_tiles && !dead; i++) {
             const int tile = blockIdx.x + i * gridDim.x;
@@ -359,28 +367,41 @@ __global__ void __launch_bounds__(kZcThreads, 1) ztc_kernel(ZtcArgs a) {
                 }
             }
             const uint32_t tacc = trow + (uint32_t)(ap.slot * N);
-            for (int cc = 0; cc < N / 16; cc += 2) {
-                // two 16-column loads in flight, one wait
-                float v[32];
-                tmem_ld16_nowait(tacc + (uint32_t)(cc * 16), v);
-                const bool two = cc + 1 < N / 16;
-                if (two) tmem_ld16_nowait(tacc + (uint32_t)((cc + 1) * 16), v + 16);
-                tmem_wait_ld(v);
+            if (g_lo >= g_hi) {
+                // no columns for this warp (N = 16): only the release
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_local(&acc_empty[ap.slot]);
+            }
+            for (int g0 = g_lo; g0 < g_hi; g0 += 4) {
+                // up to four 16-column loads in flight, one wait
+                const int ng = g_hi - g0 < 4 ? g_hi - g0 : 4;
+                float v[2][32];
+                tmem_ld16_nowait(tacc + (uint32_t)(g0 * 16), v[0]);
+                if (ng > 1) tmem_ld16_nowait(tacc + (uint32_t)((g0 + 1) * 16), v[0] + 16);
+                if (ng > 2) tmem_ld16_nowait(tacc + (uint32_t)((g0 + 2) * 16), v[1]);
+                if (ng > 3) tmem_ld16_nowait(tacc + (uint32_t)((g0 + 3) * 16), v[1] + 16);
+                tmem_wait_ld(v[0]);
+                tmem_wait_ld(v[1]);
+                if (g0 + 4 >= g_hi) {
+                    // the accumulator's last columns of this warp are in registers
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive_local(&acc_empty[ap.slot]);
+                }
                 if (!ve) continue;
 #pragma unroll
-                for (int t = 0; t < 16; t++) {
-                    const int k = cc * 8 + t;
-                    if (k >= a.nz || (t >= 8 && !two)) break;
+                for (int t = 0; t < 32; t++) {
+                    const int k = g0 * 8 + t;
+                    if (k >= a.nz || t >= 8 * ng) break;
+                    const float re = v[t >> 4][(2 * t) & 31], im = v[t >> 4][(2 * t + 1) & 31];
                     if (FWD) {
-                        reinterpret_cast<float2 *>(a.planes)[oidx0 + (long)k * ostep] = make_float2(v[2 * t], v[2 * t + 1]);
+                        reinterpret_cast<float2 *>(a.planes)[oidx0 + (long)k * ostep] = make_float2(re, im);
                     } else {
-                        a.vec.p[oidx0 + (long)k * ostep] = make_double2((double)v[2 * t], (double)v[2 * t + 1]);
+                        a.vec.p[oidx0 + (long)k * ostep] = make_double2((double)re, (double)im);
                     }
                 }
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive_local(&acc_empty[ap.slot]);
             ap.next(a.nacc);
         }
     }

@@ -201,13 +201,14 @@ def test_batched_zpml_eigen(prec):
         assert np.linalg.norm(on.apply_a(U[i]) - F[i]) / np.linalg.norm(F[i]) < 2e-10
 
 
-@pytest.mark.parametrize("nz", [17, 48, 130])
-def test_zpml_eigen_tensor_core_transforms(nz, monkeypatch):
+@pytest.mark.parametrize("nz,pml", [(17, 4), (48, 4), (130, 4), (200, 4), (8, 2)])
+def test_zpml_eigen_tensor_core_transforms(nz, pml, monkeypatch):
     """The complex64 eigenbasis transforms run on the tensor cores (3xTF32);
     they agree with the FP64 transforms to FP32 accuracy and take the same
-    FGMRES iterations.  nz = 130 exercises the two-part (N > 256) MMA."""
+    FGMRES iterations.  nz = 130 and 200 exercise the two-part (N > 256) MMA
+    and the single accumulator, nz = 8 one 16-column group (N = 16)."""
     import helm3d
-    p = small_problem(24, 20, nz, pml=4, seed=nz + 3)
+    p = small_problem(24, 20, nz, pml=pml, seed=nz + 3)
     v = rand_c(p.shape, seed=2)
     ref = mode_n.setup(p, beta_prec=0.25, z_transform="eigen").apply_prec(v)
     out, its = {}, {}
