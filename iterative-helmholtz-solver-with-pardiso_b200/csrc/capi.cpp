@@ -205,6 +205,12 @@ int helm3d_create(const helm3d_grid *grid, const double *s2, const helm3d_opts *
     c->opts = *opts;
     c->device = opts->device;
     c->c64 = opts->precision == HELM3D_PREC_C64;
+    // Z_j = M^{-1} V_j is the complex64 preconditioner's output: kept in
+    // complex64 (HELM3D_Z64=0 in the environment keeps it in complex128)
+    {
+        const char *zenv = std::getenv("HELM3D_Z64");
+        c->z64 = c->c64 && opts->mode == HELM3D_MODE_N && !(zenv && zenv[0] == '0');
+    }
     c->plane = (long)grid->nx * grid->ny;
     c->N = c->plane * grid->nz;
     if (cudaSetDevice(c->device) != cudaSuccess) {

@@ -178,7 +178,8 @@ __global__ void __launch_bounds__(kFftThreads) fftz_inverse_kernel(FftK fp, cons
             const double2 a = wr[idx], d = dl[idx];
             t = make_double2(s * a.x - (d.x * t.x - d.y * t.y), s * a.y - (d.x * t.y + d.y * t.x));
         }
-        yr[idx] = t;
+        if (y.c64) reinterpret_cast<float2 *>(y.p)[r * y.stride + idx] = cvt<float2, double2>(t);
+        else yr[idx] = t;
     }
 }
 

@@ -42,10 +42,13 @@ struct Dev {
     size_t smem_optin = 227 * 1024;
 };
 
-// A batch of R complex128 vectors: vector r at p + r * stride.
+// A batch of R complex128 vectors: vector r at p + r * stride.  With c64
+// the vectors are complex64 (p points to float2 data, stride counted in
+// float2): only where a kernel says it takes them (FGMRES's Z basis).
 struct VecBatch {
     double2 *p;
     long stride;
+    bool c64 = false;
 };
 // Per-vector real scales: scale of vector r at p[r * stride] (p may be null: 1).
 struct ScaleBatch {
@@ -355,6 +358,7 @@ struct helm3d_ctx {
     double2 *d_zWH64 = nullptr, *d_zWiH64 = nullptr;   // W^H, Wi^H (adjoint z-transforms)
     // tensor-core forms of Wi, W, W^H, Wi^H (complex64 eigenbasis path)
     bool ztc = false;
+    bool z64 = false;              // mode N, complex64 preconditioner: FGMRES's Z_j = M^{-1} V_j kept in complex64
     float *d_ztc[4] = {nullptr, nullptr, nullptr, nullptr};
     void *d_dxy = nullptr;         // [2][ny][nx] alpha_x alpha_y and conj(1 / (alpha_x alpha_y)), P precision
     double2 *d_cmx64 = nullptr, *d_cpx64 = nullptr, *d_cmy64 = nullptr, *d_cpy64 = nullptr;

@@ -308,8 +308,9 @@ __global__ void __launch_bounds__(kRedThreads) update2_kernel(double2 *__restric
     if (threadIdx.x == 0) partials[(long)r * gridDim.x * cap + (long)blockIdx.x * cap] = nrm[0];
 }
 
-// x += sum_i y[i] zs[i] Z_i  (i < *nzv_dev when given, else nzv)
-__global__ void __launch_bounds__(kRedThreads) combine_kernel(const double2 *__restrict__ Z, long ldz, long sZ,
+// x += sum_i y[i] zs[i] Z_i  (i < *nzv_dev when given, else nzv); Z complex128 or complex64
+template <typename TZ>
+__global__ void __launch_bounds__(kRedThreads) combine_kernel(const TZ *__restrict__ Z, long ldz, long sZ,
                                                               const double *__restrict__ zs, long sZs, int nzv,
                                                               const double2 *__restrict__ y, long sY,
                                                               double2 *__restrict__ x, long sX, long N,
@@ -326,7 +327,7 @@ __global__ void __launch_bounds__(kRedThreads) combine_kernel(const double2 *__r
     const long stride = (long)gridDim.x * blockDim.x;
     for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += stride) {
         double2 acc = x[l];
-        for (int i = 0; i < nzv; i++) acc = cfma(sc[i], Z[i * ldz + l], acc);
+        for (int i = 0; i < nzv; i++) acc = cfma(sc[i], cvt<double2, TZ>(Z[i * ldz + l]), acc);
         x[l] = acc;
     }
 }
@@ -468,8 +469,14 @@ int launch_update2(const VecBatch &V, long ldv, int j, const double2 *coef, long
 
 int launch_combine(const VecBatch &Z, long ldz, const ScaleBatch &zs, int nzv, const double2 *y, long sY,
                    const VecBatch &x, long N, int R, cudaStream_t s, const int *nzv_dev) {
-    combine_kernel<<<dim3(grid_for(N, R), R), kRedThreads, sizeof(double2) * (nzv > 0 ? nzv : 1), s>>>(
-        Z.p, ldz, Z.stride, zs.p, zs.stride, nzv, y, sY, x.p, x.stride, N, nzv_dev);
+    const dim3 grid(grid_for(N, R), R);
+    const size_t sm = sizeof(double2) * (nzv > 0 ? nzv : 1);
+    if (Z.c64)
+        combine_kernel<float2><<<grid, kRedThreads, sm, s>>>(reinterpret_cast<const float2 *>(Z.p), ldz, Z.stride,
+                                                             zs.p, zs.stride, nzv, y, sY, x.p, x.stride, N, nzv_dev);
+    else
+        combine_kernel<double2><<<grid, kRedThreads, sm, s>>>(Z.p, ldz, Z.stride, zs.p, zs.stride, nzv, y, sY, x.p,
+                                                              x.stride, N, nzv_dev);
     return ok() ? HELM3D_OK : HELM3D_ERR_CUDA;
 }
 

@@ -133,7 +133,9 @@ int ensure_krylov(helm3d_ctx *c, int m, int R) {
     for (int v = 0; v < kReduceVariants; v++) red_max = std::max(red_max, reduce_blocks(v));
     int rc;
     if ((rc = get((void **)&c->d_V, vb * (m + 1) * R, "Krylov basis V")) ||
-        (c->opts.mode == HELM3D_MODE_N && (rc = get((void **)&c->d_Z, vb * m * R, "Krylov basis Z"))) ||
+        (c->opts.mode == HELM3D_MODE_N &&
+         (rc = get((void **)&c->d_Z, (c->z64 ? sizeof(float2) : sizeof(double2)) * (size_t)c->N * m * R,
+                   "Krylov basis Z"))) ||
         (rc = get((void **)&c->d_vs, sizeof(double) * (m + 2) * R, "basis scales")) ||
         (rc = get((void **)&c->d_h, sizeof(double2) * scalars_per_rhs(m) * R, "Krylov scalars")) ||
         (rc = get((void **)&c->d_partials, sizeof(double2) * c->red_cap * red_max * R, "partials")) ||
@@ -386,6 +388,13 @@ static void givens(zc a, zc b, zc &cs, zc &sn) {
 // Gram-Schmidt with the conditional second pass.
 static bool lowsync(const helm3d_ctx *c) { return c->opts.mode == HELM3D_MODE_N && c->gs_lowsync; }
 
+// The Z basis from vector offset off (in elements), leading dimension ld:
+// complex64 when the context keeps it so (z64), else complex128.
+static VecBatch zbasis(const helm3d_ctx *c, long off, long ld) {
+    if (c->z64) return VecBatch{reinterpret_cast<double2 *>(reinterpret_cast<float2 *>(c->d_Z) + off), ld, true};
+    return VecBatch{c->d_Z + off, ld};
+}
+
 // ------------------------------------------------ restart cycle as a graph
 // One Arnoldi step j of a batch of B, kernels only: the operator and
 // preconditioner applications, classical Gram-Schmidt with its norms, the
@@ -396,13 +405,13 @@ static int arnoldi_step(helm3d_ctx *c, int m, int B, int j, bool adjoint, const 
     const long N = c->N;
     const long ldV = (long)(m + 1) * N, ldZ = (long)m * N;
     const int M2 = m + 2, SH = scalars_per_rhs(m);
-    double2 *V = c->d_V, *Z = c->d_Z, *Hd = c->d_h;
+    double2 *V = c->d_V, *Hd = c->d_h;
     double2 *d_h1 = Hd, *d_h2 = Hd + M2, *d_nrm = Hd + 2 * M2;
     const Reduce red = reducer(c);
     const VecBatch Vall{V, ldV}, Vj{V + (size_t)j * N, ldV}, w{V + (size_t)(j + 1) * N, ldV};
     const ScaleBatch vsb{c->d_vs, M2}, vsj{c->d_vs + j, M2};
     if (c->opts.mode == HELM3D_MODE_N) {
-        const VecBatch zj{Z + (size_t)j * N, ldZ};
+        const VecBatch zj = zbasis(c, (long)j * N, ldZ);
         if (adjoint) {
             RC(apply_prec_adjoint(c, Vj, 1.0, vsj, zj, B));
             RC(apply_op_adjoint(c, zj, 1.0, kNoScale, w, B));
@@ -458,7 +467,7 @@ static int cycle_tail(helm3d_ctx *c, int m, int B, const ArnState &a) {
     RC(timed(c, HELM3D_K_KRYLOV, 1, [&] { return launch_backsub(a, c->stream); }));
     return timed(c, HELM3D_K_KRYLOV, 1, [&] {
         return c->opts.mode == HELM3D_MODE_N
-                   ? launch_combine(VecBatch{c->d_Z, ldZ}, N, kNoScale, m, d_y, SH, VecBatch{c->d_Uw, N}, N, B,
+                   ? launch_combine(zbasis(c, 0, ldZ), N, kNoScale, m, d_y, SH, VecBatch{c->d_Uw, N}, N, B,
                                     c->stream, a.flags + 2)
                    : launch_combine(VecBatch{c->d_V, ldV}, N, ScaleBatch{c->d_vs, M2}, m, d_y, SH,
                                     VecBatch{c->d_Uw, N}, N, B, c->stream, a.flags + 2);
@@ -576,9 +585,10 @@ int tune_solve(helm3d_ctx *c, int R, bool adjoint) {
         return launch_sweep(c->c64, t, c->stream);
     });
     if (c->opts.mode == HELM3D_MODE_N) {
-        // the stencil from V_0 into V_1 of every right-hand side
-        std::snprintf(shape, sizeof(shape), "%d|%d|%d|%d", g.nx, g.ny, g.nz, R);
-        StencilArgs a0 = stencil_args(c, VecBatch{c->d_V, ldV}, 1.0, kNoScale, VecBatch{c->d_V + N, ldV},
+        // the stencil from Z_0 (its FGMRES input: complex64 when the
+        // context keeps Z so) into V_1 of every right-hand side
+        std::snprintf(shape, sizeof(shape), "%d|%d|%d|%d|%d", g.nx, g.ny, g.nz, R, c->z64 ? 64 : 128);
+        StencilArgs a0 = stencil_args(c, zbasis(c, 0, (long)m * N), 1.0, kNoScale, VecBatch{c->d_V + N, ldV},
                                       VecBatch{nullptr, 0}, R);
         c->tv_stencil = tune_pick(c, "STENCIL", shape, kStencilVariants, [&](int v) {
             StencilArgs t = a0;
@@ -923,7 +933,7 @@ struct FgmresRun {
 int FgmresRun::run_host_cycle() {
     const helm3d_opts &o = c->opts;
     const double tol = o.tol;
-    double2 *V = c->d_V, *Z = c->d_Z, *Uw = c->d_Uw, *Hd = c->d_h;
+    double2 *V = c->d_V, *Uw = c->d_Uw, *Hd = c->d_h;
     double2 *d_h1 = Hd, *d_h2 = Hd + M2, *d_nrm = Hd + 2 * M2, *d_y = Hd + 3 * M2;
     const Reduce red = reducer(c);
     const VecBatch Vall{V, ldV};
@@ -932,7 +942,7 @@ int FgmresRun::run_host_cycle() {
         const VecBatch Vj{V + (size_t)j * N, ldV}, w{V + (size_t)(j + 1) * N, ldV};
         const ScaleBatch vsj{c->d_vs + j, M2};
         if (flexible) {
-            const VecBatch zj{Z + (size_t)j * N, ldZ};
+            const VecBatch zj = zbasis(c, (long)j * N, ldZ);
             if (adjoint) {
                 // A^H M^{-H} = (M^{-1} A)^H: the adjoint of the forward
                 // preconditioned operator, with the same singular values
@@ -1032,7 +1042,7 @@ int FgmresRun::run_host_cycle() {
                                            sizeof(double2) * kmax, B, cudaMemcpyHostToDevice, c->stream),
                       "y"));
         RC(timed(c, HELM3D_K_KRYLOV, 1, [&] {
-            return flexible ? launch_combine(VecBatch{Z, ldZ}, N, kNoScale, kmax, d_y, SH, VecBatch{Uw, N}, N, B,
+            return flexible ? launch_combine(zbasis(c, 0, ldZ), N, kNoScale, kmax, d_y, SH, VecBatch{Uw, N}, N, B,
                                              c->stream)
                             : launch_combine(Vall, N, vsb, kmax, d_y, SH, VecBatch{Uw, N}, N, B, c->stream);
         }));

@@ -397,6 +397,8 @@ __global__ void __launch_bounds__(kZcThreads, 1) ztc_kernel(ZtcArgs a) {
                     const float re = v[t >> 4][(2 * t) & 31], im = v[t >> 4][(2 * t + 1) & 31];
                     if (FWD) {
                         reinterpret_cast<float2 *>(a.planes)[oidx0 + (long)k * ostep] = make_float2(re, im);
+                    } else if (a.vec.c64) {
+                        reinterpret_cast<float2 *>(a.vec.p)[oidx0 + (long)k * ostep] = make_float2(re, im);
                     } else {
                         a.vec.p[oidx0 + (long)k * ostep] = make_double2((double)re, (double)im);
                     }

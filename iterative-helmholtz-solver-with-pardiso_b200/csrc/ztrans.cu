@@ -68,6 +68,7 @@ __global__ void __launch_bounds__(kZtCols *kZtWarps) ztrans_kernel(PlaneLayout L
             const int k = k0 + q;
             if (k >= nz) break;
             if (FWD) planes[zt_plane_index(L, r, k, w)] = cvt<Cx, double2>(acc[q]);
+            else if (vec.c64) reinterpret_cast<float2 *>(vec.p)[r * vec.stride + (long)k * plane + w] = cvt<float2, double2>(acc[q]);
             else v_r[(long)k * plane + w] = acc[q];
         }
     }
