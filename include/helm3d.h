@@ -93,6 +93,12 @@ typedef struct helm3d_opts {
     int device;          /* CUDA device ordinal */
     int verbose;
     int z_transform;     /* helm3d_z_transform (mode N; mode R always uses the FFT) */
+    double kz_skip_ratio; /* > 0: the reference's SAVE_MEM (Source/FGMRES.cpp:197-206):
+                           * mode k with kww >= ratio * k2 is not factored (kww its kz^2,
+                           * -Re of its shift; k2 = omega^2 s2_l0 when s2_l0 > 0, else
+                           * omega^2 times the largest s0^2 of the 2D medium); mode R sets
+                           * its solution to zero as the reference does, mode N solves it
+                           * by the diagonal of its 2D operator.  0 (default): off */
 } helm3d_opts;
 
 typedef struct helm3d_stats {

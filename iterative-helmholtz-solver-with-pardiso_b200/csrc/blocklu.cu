@@ -53,6 +53,7 @@ template <typename R> struct FactorK {
     const cplx<R> *cmx, *cpx, *cmy, *cpy, *base2d;
     const cplx<R> *kz2;  // complex shift of mode kz
     int *status;
+    const int *kzslot;   // >= 0: a skipped mode (nothing to do), or null
 };
 
 template <typename R> __device__ __forceinline__ R cabs1(cplx<R> a) { return fabs(a.x) + fabs(a.y); }
@@ -138,6 +139,7 @@ __global__ void __launch_bounds__(NW * 32, MB) factor_kernel(FactorK<R> a) {
 
     const uint32_t rank = (C > 1) ? cluster_ctarank() : 0u;
     const int kz = blockIdx.x / C;
+    if (a.kzslot && a.kzslot[kz] >= 0) return;   // a skipped mode (kz_skip_ratio): not factored / swept
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n = a.n, ny = a.ny;
     const int col0 = (int)rank * NPC + warp * CB;
@@ -393,6 +395,7 @@ static int launch_cfg(const FactorArgs &fa, cudaStream_t st) {
     k.cpy = (const cplx<R> *)fa.cpy;
     k.base2d = (const cplx<R> *)fa.base2d;
     k.kz2 = (const cplx<R> *)fa.kz2;
+    k.kzslot = fa.kzslot;
     k.status = fa.status;
     constexpr size_t smem = factor_smem_bytes<R, NP, NP / C>();
     auto kern = factor_kernel<R, NP, NW, CB, C, MB>;

@@ -560,7 +560,7 @@ int helm3d_destroy(helm3d_ctx *c) {
     if (!c) return HELM3D_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void *bufs[] = {c->d_Gt, c->d_gscale, c->d_gpack, c->d_tw, c->d_cmx, c->d_cpx, c->d_cmy, c->d_cpy, c->d_base2d, c->d_kz2, c->d_zW, c->d_zWi, c->d_zW64, c->d_zWi64, c->d_zWH64, c->d_zWiH64, c->d_dxy,
+    void *bufs[] = {c->d_Gt, c->d_gscale, c->d_gpack, c->d_kzslot, c->d_kzlist, c->d_kzinv, c->d_tw, c->d_cmx, c->d_cpx, c->d_cmy, c->d_cpy, c->d_base2d, c->d_kz2, c->d_zW, c->d_zWi, c->d_zW64, c->d_zWi64, c->d_zWH64, c->d_zWiH64, c->d_dxy,
                     c->d_cmx64, c->d_cpx64, c->d_cmy64, c->d_cpy64, c->d_cmz64, c->d_cpz64, c->d_s2, c->d_dl,
                     c->d_planes, c->d_status, c->d_V, c->d_Z, c->d_vs, c->d_h, c->d_partials, c->d_f, c->d_u,
                     c->d_r, c->d_t, c->d_t2, c->d_bic, c->d_Fw, c->d_Uw};

@@ -59,6 +59,7 @@ struct FactorTcK {
     float2 *Gt;
     const float2 *cmx, *cpx, *cmy, *cpy, *base2d, *kz2;
     int *status;
+    const int *kzslot;   // >= 0: a skipped mode (nothing to do), or null
 };
 
 struct FtSmem {
@@ -104,6 +105,7 @@ __global__ void __launch_bounds__(kFtThreads, 1) factor_tc_kernel(FactorTcK a) {
     FtSmem sm = ft_carve(smem_raw);
     const int n = a.n, ny = a.ny;
     const int kz = blockIdx.x;
+    if (a.kzslot && a.kzslot[kz] >= 0) return;   // a skipped mode (kz_skip_ratio): not factored / swept
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int npan = (n + kFtB - 1) / kFtB;
     const int ncol = ((n + 7) / 8) * 8;          // complex columns the GEMM covers (N = 2 ncol, a multiple of 16)
@@ -416,6 +418,7 @@ int launch_factor_tc(const FactorArgs &fa, cudaStream_t st) {
     k.base2d = (const float2 *)fa.base2d;
     k.kz2 = (const float2 *)fa.kz2;
     k.status = fa.status;
+    k.kzslot = fa.kzslot;
     if (!smem_limit_max(factor_tc_kernel, kFtSmemBytes))
         return HELM3D_ERR_CUDA;
     factor_tc_kernel<<<dim3((unsigned)fa.nz), kFtThreads, kFtSmemBytes, st>>>(k);

@@ -82,6 +82,7 @@ struct F2K {
     float2 *Gt;
     const float2 *cmx, *cpx, *cmy, *cpy, *base2d, *kz2;
     int *status;
+    const int *kzslot;   // >= 0: a skipped mode (nothing to do, in both CTAs), or null
 };
 
 struct F2Smem {
@@ -167,6 +168,7 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
     const int n = a.n, ny = a.ny;
     const uint32_t rank = cluster_ctarank(), peer = rank ^ 1u;
     const int kz = blockIdx.x >> 1;
+    if (a.kzslot && a.kzslot[kz] >= 0) return;   // a skipped mode (kz_skip_ratio): not factored / swept
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n0 = (n + 1) >> 1;
     const int nr = rank == 0 ? n0 : n - n0;       // rows of this CTA
@@ -608,6 +610,7 @@ int launch_factor_tc2(const FactorArgs &fa, cudaStream_t st) {
     k.base2d = (const float2 *)fa.base2d;
     k.kz2 = (const float2 *)fa.kz2;
     k.status = fa.status;
+    k.kzslot = fa.kzslot;
     if (!smem_limit_max(factor_tc2_kernel, kF2SmemBytes)) return HELM3D_ERR_CUDA;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(2 * fa.nz), 1, 1);

@@ -99,6 +99,7 @@ struct FactorArgs {
     const void *base2d;       // cplx<P>[ny][n]: omega^2 s0^2 (1 + i beta)
     const void *kz2;          // cplx<P>[nz]: complex shift of mode k (-kz^2 or lambda_k)
     int *status;              // device flag: bit 0 = zero pivot
+    const int *kzslot = nullptr;   // [nz]: >= 0 for a skipped mode (not factored), or null
 };
 // variant: one of the factor_variants(c64, n) launch shapes (0: the default)
 int launch_factor(bool c64, const FactorArgs &a, cudaStream_t s, int variant = 0);
@@ -129,8 +130,22 @@ struct SweepArgs {
     const float *gscale = nullptr;   // [nz][ny] power-of-two scales of the blocks (launch_gscale)
     int tc_pack = 0;          // the tensor-core sweep on the packed factor (sweep_tcp.cu)
     const void *gpack = nullptr;     // the packed factor (launch_gpack), or null
+    // skipped modes (kz_skip_ratio): kzslot[kz] >= 0 marks one (the sweep
+    // kernels leave it), kzlist[slot] = kz, kzinv[slot] its inverse diagonal
+    const int *kzslot = nullptr, *kzlist = nullptr;
+    int nskip = 0;
+    const void *kzinv = nullptr;
 };
 int launch_sweep(bool c64, const SweepArgs &a, cudaStream_t s);
+// Skipped modes (opts.kz_skip_ratio, the reference's SAVE_MEM): kzinv[slot][j][i]
+// = 1 / (the diagonal of mode kzlist[slot]'s 2D operator: -(cmx+cpx)[i]
+// -(cmy+cpy)[j] + base2d[j][i] + shift[kz]), or 0 with zero (mode R: the
+// reference sets those modes' solution to zero); launch_kzskip_apply scales
+// those modes' planes by it (by its conjugate for the adjoint).
+int launch_kzinv(bool c64, const int *kzlist, int nskip, int nx, int ny, const void *cmx, const void *cpx,
+                 const void *cmy, const void *cpy, const void *base2d, const void *shift, bool zero, void *kzinv,
+                 cudaStream_t s);
+int launch_kzskip_apply(bool c64, const SweepArgs &a, cudaStream_t s);
 // the sweep's launch variants the autotuner times: stage and ring sizes of
 // the CUDA-core kernels (0-5), the tensor-core kernel's chunk (6, 7), the
 // tensor-core kernel with FP16 products (8), the tensor-core kernel on the
@@ -359,6 +374,13 @@ struct helm3d_ctx {
     // tensor-core forms of Wi, W, W^H, Wi^H (complex64 eigenbasis path)
     bool ztc = false;
     bool z64 = false;              // mode N, complex64 preconditioner: FGMRES's Z_j = M^{-1} V_j kept in complex64
+    // skipped modes (opts.kz_skip_ratio): per kz the slot or -1, the slots' kz,
+    // the slots' inverse diagonals (cplx<P> [nskip][ny][nx])
+    std::vector<int> kzslot_h;
+    int nskip = 0;
+    int *d_kzslot = nullptr, *d_kzlist = nullptr;
+    void *d_kzinv = nullptr;
+    size_t kzinv_bytes = 0;
     float *d_ztc[4] = {nullptr, nullptr, nullptr, nullptr};
     void *d_dxy = nullptr;         // [2][ny][nx] alpha_x alpha_y and conj(1 / (alpha_x alpha_y)), P precision
     double2 *d_cmx64 = nullptr, *d_cpx64 = nullptr, *d_cmy64 = nullptr, *d_cpy64 = nullptr;

@@ -98,6 +98,12 @@ extern "C" int helm3d_apply_prec_noalloc(helm3d_ctx *c, const double *x, double 
     s.R = 1;
     s.dxy = nullptr;
     s.status = c->d_status;
+    if (c->nskip > 0) {
+        s.kzslot = c->d_kzslot;
+        s.kzlist = c->d_kzlist;
+        s.nskip = c->nskip;
+        s.kzinv = c->d_kzinv;
+    }
     rc = launch_sweep(c->c64, s, c->stream);
     if (rc) return set_error(c, rc, "apply_prec_noalloc: sweep launch");
     rc = c->ztc    ? launch_ztc_inverse(scratch, L, yb, c->d_ztc[1], c->d_status, c->stream)

@@ -496,6 +496,75 @@ int ctx_setup_medium(helm3d_ctx *c, const double *s2, bool s2_on_device) {
     return upload_c(c, &c->d_base2d, c->base2d, "base2d");
 }
 
+// The modes skipped by opts.kz_skip_ratio (the reference's SAVE_MEM rule,
+// Source/FGMRES.cpp:197-206: kww >= ratio * k2): kww = -Re of the mode's
+// shift (kz^2, or -Re lambda_k), k2 = omega^2 s2_l0 when s2_l0 > 0 (mode R
+// HOMO: the reference's kk = omega / c_z), else the largest omega^2 s0^2 of
+// the 2D medium (Re base2d).  Their slots, list and inverse diagonals (zero in
+// mode R) go to the device; the factor and sweep kernels leave those modes.
+static int setup_kz_skip(helm3d_ctx *c) {
+    const helm3d_opts &o = c->opts;
+    const helm3d_grid &g = c->grid;
+    const int nz = g.nz;
+    c->nskip = 0;
+    c->kzslot_h.assign(nz, -1);
+    if (!(o.kz_skip_ratio > 0)) return HELM3D_OK;
+    int rc;
+    double k2 = 0.0;
+    if (o.s2_l0 > 0) {
+        k2 = g.omega * g.omega * o.s2_l0;
+    } else {
+        const size_t esz = c->c64 ? 8 : 16;
+        std::vector<unsigned char> b(esz * (size_t)c->plane);
+        if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "base2d")) ||
+            (rc = cuda_check(c, cudaMemcpy(b.data(), c->d_base2d, b.size(), cudaMemcpyDeviceToHost), "base2d")))
+            return rc;
+        for (long l = 0; l < c->plane; l++) {
+            double re;
+            if (c->c64) {
+                float f;
+                std::memcpy(&f, b.data() + 8 * l, 4);
+                re = f;
+            } else {
+                std::memcpy(&re, b.data() + 16 * l, 8);
+            }
+            k2 = std::max(k2, re);
+        }
+    }
+    std::vector<int> list;
+    for (int k = 0; k < nz; k++)
+        if (-c->zshift[k].real() >= o.kz_skip_ratio * k2) {
+            c->kzslot_h[k] = (int)list.size();
+            list.push_back(k);
+        }
+    c->nskip = (int)list.size();
+    if (c->nskip == 0) return HELM3D_OK;
+    const size_t esz = c->c64 ? 8 : 16;
+    const size_t inv_bytes = esz * (size_t)c->plane * c->nskip;
+    if (inv_bytes > c->kzinv_bytes) {
+        if (c->d_kzinv) {
+            cudaFree(c->d_kzinv);
+            c->bytes -= c->kzinv_bytes;
+            c->d_kzinv = nullptr;
+        }
+        if ((rc = dalloc(c, &c->d_kzinv, inv_bytes, "skipped modes' diagonals"))) return rc;
+        c->kzinv_bytes = inv_bytes;
+    }
+    if ((rc = dalloc(c, (void **)&c->d_kzslot, sizeof(int) * nz, "skipped modes")) ||
+        (rc = dalloc(c, (void **)&c->d_kzlist, sizeof(int) * nz, "skipped modes")) ||
+        (rc = cuda_check(c, cudaMemcpy(c->d_kzslot, c->kzslot_h.data(), sizeof(int) * nz, cudaMemcpyHostToDevice),
+                         "skipped modes")) ||
+        (rc = cuda_check(c, cudaMemcpy(c->d_kzlist, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice),
+                         "skipped modes")))
+        return rc;
+    rc = launch_kzinv(c->c64, c->d_kzlist, c->nskip, g.nx, g.ny, c->d_cmx, c->d_cpx, c->d_cmy, c->d_cpy,
+                      c->d_base2d, c->d_kz2, o.mode == HELM3D_MODE_R, c->d_kzinv, c->stream);
+    if (rc) return set_error(c, rc, "skipped modes' diagonals launch failed");
+    if (o.verbose) std::printf("helm3d: %d of %d kz modes skipped (ratio %g, k2 %g)\n", c->nskip, nz,
+                               o.kz_skip_ratio, k2);
+    return HELM3D_OK;
+}
+
 int ctx_factor(helm3d_ctx *c) {
     if (!factor_supported(c->c64, c->grid.nx))
         return set_error(c, HELM3D_ERR_ARG, "nx beyond the supported block size of the factor");
@@ -513,6 +582,8 @@ int ctx_factor(helm3d_ctx *c) {
     a.base2d = c->d_base2d;
     a.kz2 = c->d_kz2;
     a.status = c->d_status;
+    if ((rc = setup_kz_skip(c))) return rc;
+    a.kzslot = c->nskip > 0 ? c->d_kzslot : nullptr;
     const int nv = factor_variants(c->c64, a.n);
     if (nv > 1) {
         // the launch shapes of this block size, timed once per process; the

@@ -198,6 +198,12 @@ static SweepArgs sweep_args(helm3d_ctx *c, int R, bool adjoint) {
     s.status = c->d_status;
     s.gscale = c->d_gscale;
     s.gpack = c->d_gpack;
+    if (c->nskip > 0) {
+        s.kzslot = c->d_kzslot;
+        s.kzlist = c->d_kzlist;
+        s.nskip = c->nskip;
+        s.kzinv = c->d_kzinv;
+    }
     sweep_variant(c->tv_sweep[adjoint ? 1 : 0], s);
     return s;
 }

@@ -46,6 +46,7 @@ template <typename R> struct SweepK {
     uint32_t wait_limit;  // polls of a producer/consumer wait before it gives up (status bit 2)
     int expire_test;      // HELM3D_TEST_EXPIRE_WAIT: the consumers first wait on a barrier that
                           // nothing arrives on, so that the wait expires (tests of the status path)
+    const int *kzslot;    // >= 0: a skipped mode (launch_kzskip_apply handles it), or null
 };
 
 // Polls of a bounded wait.  Waits between the producer and the consumers use
@@ -107,6 +108,7 @@ __global__ void __launch_bounds__((kSweepConsumerWarps + 1) * 32, 1) sweep_kerne
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int n = a.n, ny = a.ny, ldg = a.ldg, Rn = a.nrhs;
     const int kz = blockIdx.x;
+    if (a.kzslot && a.kzslot[kz] >= 0) return;   // a skipped mode (kz_skip_ratio): not factored / swept
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Cx *ring = reinterpret_cast<Cx *>(smem_raw);
     Cx *vbuf = reinterpret_cast<Cx *>(smem_raw + (size_t)a.nstage * a.stage_bytes);  // [2][n][RR]
@@ -261,6 +263,7 @@ __global__ void __launch_bounds__((CW + 1) * 32, 1) sweep_tiled_kernel(SweepK<fl
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int n = a.n, ny = a.ny, ldg = a.ldg, Rn = a.nrhs;
     const int kz = blockIdx.x;
+    if (a.kzslot && a.kzslot[kz] >= 0) return;   // a skipped mode (kz_skip_ratio): not factored / swept
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Cx *ring = reinterpret_cast<Cx *>(smem_raw);
     Cx *vbuf = reinterpret_cast<Cx *>(smem_raw + (size_t)a.nstage * a.stage_bytes);  // [2][n][RR]
@@ -425,6 +428,7 @@ template <int RR, bool ADJ> static int sweep_tiled_rr(const SweepArgs &sa, cudaS
     k.planes = (Cx *)sa.planes;
     k.dxy = (const Cx *)sa.dxy;
     k.status = sa.status;
+    k.kzslot = sa.kzslot;
     k.expire_test = 0;
     k.wait_limit = wait_limit_polls(kSweepWaitLimit);
     // groups: the largest power of two GM with tiles <= threads per group
@@ -482,6 +486,7 @@ template <typename R, int G, int RR, bool ADJ> static int sweep_impl(const Sweep
     k.planes = (Cx *)sa.planes;
     k.dxy = (const Cx *)sa.dxy;
     k.status = sa.status;
+    k.kzslot = sa.kzslot;
     k.wait_limit = wait_limit_polls(kSweepWaitLimit);
     {
         const char *e = std::getenv("HELM3D_TEST_EXPIRE_WAIT");
@@ -537,7 +542,15 @@ void sweep_variant(int v, SweepArgs &a) {
     a.tc_pack = kTcPack[v];
 }
 
+static int launch_sweep_kernels(bool c64, const SweepArgs &sa, cudaStream_t s);
+
 int launch_sweep(bool c64, const SweepArgs &sa, cudaStream_t s) {
+    const int rc = launch_sweep_kernels(c64, sa, s);
+    if (rc || sa.nskip <= 0) return rc;
+    return launch_kzskip_apply(c64, sa, s);   // the skipped modes, which the sweep kernels left
+}
+
+static int launch_sweep_kernels(bool c64, const SweepArgs &sa, cudaStream_t s) {
     if (sa.n < 1 || sa.n > kSweepMaxN || sa.R < 1 || sa.R > kMaxBatch) return HELM3D_ERR_ARG;
     // the tensor-core kernel where it applies (complex64, n <= 256, shared memory fits)
     if (c64 && sa.tc_mc && sweep_tc_supported(sa)) return launch_sweep_tc(sa, sa.tc_mc, s);

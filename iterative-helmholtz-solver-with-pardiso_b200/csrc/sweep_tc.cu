@@ -79,6 +79,7 @@ struct SweepTcK {
     float2 *planes;
     const float2 *dxy;   // adjoint scaling table (see sweep.cu), or null
     int *status;
+    const int *kzslot;   // >= 0: a skipped mode (launch_kzskip_apply handles it), or null
 };
 
 __device__ __forceinline__ void tc_epilogue_barrier() {
@@ -118,6 +119,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_kernel(SweepTcK a) {
     const int n = a.n, ny = a.ny, ldg = a.ldg, Rn = a.nrhs, npad = a.npad, cpl = a.cpl;
     const int Kp = 2 * npad;
     const int kz = blockIdx.x;
+    if (a.kzslot && a.kzslot[kz] >= 0) return;   // a skipped mode (kz_skip_ratio): not factored / swept
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nsteps = 2 * ny - 1;
     const long nseq = (long)nsteps * cpl;
@@ -666,6 +668,7 @@ static int sweep_tc_impl(const SweepArgs &sa, const TcShape &sh, cudaStream_t st
     k.planes = (float2 *)sa.planes;
     k.dxy = (const float2 *)sa.dxy;
     k.status = sa.status;
+    k.kzslot = sa.kzslot;
     k.stage_bytes = sh.stage_bytes;
     k.nstage = sh.nstage;
     auto kern = sweep_tc_kernel<RR, MC, MB, ADJ, F16>;

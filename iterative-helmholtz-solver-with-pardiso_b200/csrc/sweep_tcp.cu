@@ -64,6 +64,7 @@ struct SweepTpK {
     float2 *planes;
     const float2 *dxy;      // adjoint scaling table (see sweep.cu), or null
     int *status;
+    const int *kzslot;      // >= 0: a skipped mode (launch_kzskip_apply handles it), or null
 };
 
 __device__ __forceinline__ void tp_epilogue_barrier() {
@@ -91,6 +92,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) sweep_tcp_kernel(SweepTpK a) {
     const int n = a.n, ny = a.ny, Rn = a.nrhs, npad = a.npad, cpl = a.cpl;
     const int Kp = 2 * npad;
     const int kz = blockIdx.x;
+    if (a.kzslot && a.kzslot[kz] >= 0) return;   // a skipped mode (kz_skip_ratio): not factored / swept
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nsteps = 2 * ny - 1;
     const long nseq = (long)nsteps * cpl;
@@ -535,6 +537,7 @@ template <int RR, int MB, bool ADJ> static int sweep_tcp_impl(const SweepArgs &s
     k.planes = (float2 *)sa.planes;
     k.dxy = (const float2 *)sa.dxy;
     k.status = sa.status;
+    k.kzslot = sa.kzslot;
     auto kern = sweep_tcp_kernel<RR, MB, ADJ>;
     if (!smem_limit_max(kern, sh.smem)) return HELM3D_ERR_CUDA;
     kern<<<dim3((unsigned)sa.nz), kTpThreads, sh.smem, st>>>(k);

@@ -44,7 +44,7 @@ class Opts(ctypes.Structure):
                 ("beta_prec", ctypes.c_double), ("beta_phys", ctypes.c_double), ("s2_l0", ctypes.c_double),
                 ("quirk_q1", ctypes.c_int), ("restart", ctypes.c_int), ("max_iter", ctypes.c_int),
                 ("tol", ctypes.c_double), ("stop_phys", ctypes.c_int), ("device", ctypes.c_int),
-                ("verbose", ctypes.c_int), ("z_transform", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("z_transform", ctypes.c_int), ("kz_skip_ratio", ctypes.c_double)]
 
 
 class Stats(ctypes.Structure):

@@ -76,6 +76,8 @@ class ModeN:
     lus: list
     zW: np.ndarray | None = None
     zWi: np.ndarray | None = None
+    skip: np.ndarray | None = None     # modes solved by the diagonal of their 2D operator
+    diag: np.ndarray | None = None     # (nz, ny, nx) that diagonal
 
     @property
     def shape(self):
@@ -137,7 +139,10 @@ class ModeN:
             vh = np.fft.fft(v.reshape(self.shape), axis=0)
         out = np.empty_like(vh)
         for k in range(self.shape[0]):
-            out[k] = self.lus[k].solve(vh[k].ravel()).reshape(vh[k].shape)
+            if self.skip is not None and self.skip[k]:
+                out[k] = vh[k] / self.diag[k]
+            else:
+                out[k] = self.lus[k].solve(vh[k].ravel()).reshape(vh[k].shape)
         if self.zW is not None:
             return np.tensordot(self.zW, out, axes=(1, 0))
         return np.fft.ifft(out, axis=0)
@@ -151,7 +156,10 @@ class ModeN:
             vh = np.fft.fft(v.reshape(self.shape), axis=0)
         out = np.empty_like(vh)
         for k in range(self.shape[0]):
-            out[k] = self.lus[k].solve(vh[k].ravel(), trans="H").reshape(vh[k].shape)
+            if self.skip is not None and self.skip[k]:
+                out[k] = vh[k] / np.conj(self.diag[k])
+            else:
+                out[k] = self.lus[k].solve(vh[k].ravel(), trans="H").reshape(vh[k].shape)
         if self.zW is not None:
             return np.tensordot(self.zWi.conj().T, out, axes=(1, 0))
         return np.fft.ifft(out, axis=0)
@@ -182,7 +190,12 @@ def zpml_eigen(cm: np.ndarray, cp: np.ndarray):
 
 
 def setup(prob: Problem, beta_prec: float = 0.5, kz_symbol: str = "discrete", factor: bool = True,
-          z_transform: str = "fft") -> ModeN:
+          z_transform: str = "fft", kz_skip_ratio: float = 0.0) -> ModeN:
+    """kz_skip_ratio > 0: the reference's SAVE_MEM idea (Source/FGMRES.cpp:
+    197-206) for the 7-point operator: a mode whose kz^2 (FFT) or -Re lambda_k
+    (eigenbasis) is at least ratio * k2, k2 = omega^2 max_(x,y) s0^2, is not
+    factored; its 2D system is solved by its diagonal instead of being set to
+    zero (zeroing stalls FGMRES on this operator)."""
     ax = Axis(n=prob.nx, h=prob.h, pml_pts=prob.pml)
     ay = Axis(n=prob.ny, h=prob.h, pml_pts=prob.pml)
     az = Axis(n=prob.nz, h=prob.h, pml_pts=prob.pml)
@@ -197,11 +210,18 @@ def setup(prob: Problem, beta_prec: float = 0.5, kz_symbol: str = "discrete", fa
         shifts = base[None, :, :] + lam[:, None, None]
     else:
         shifts = base[None, :, :] - kz2[:, None, None]
+    skip = diag = None
+    if kz_skip_ratio > 0:
+        kww = -lam.real if z_transform == "eigen" else kz2
+        skip = kww >= kz_skip_ratio * (prob.omega ** 2) * s0.max()
+        cmx, cpx = coef["x"]
+        cmy, cpy = coef["y"]
+        diag = -(cmx + cpx)[None, None, :] - (cmy + cpy)[None, :, None] + shifts
     lus = []
     if factor:
         for k in range(prob.nz):
-            lus.append(spla.splu(assemble_2d(g, shifts[k])))
-    return ModeN(prob, g, beta_prec, coef, kz2, shifts, lus, zW, zWi)
+            lus.append(None if skip is not None and skip[k] else spla.splu(assemble_2d(g, shifts[k])))
+    return ModeN(prob, g, beta_prec, coef, kz2, shifts, lus, zW, zWi, skip, diag)
 
 
 @dataclass

@@ -182,6 +182,7 @@ class ModeR:
     shifts: np.ndarray      # (nz, ny, nx) complex diagonal shift per kz
     mats: list
     lus: list
+    skip: np.ndarray | None = None   # SAVE_MEM: modes neither factored nor solved
 
     @property
     def shape(self):
@@ -191,9 +192,11 @@ class ModeR:
     def l0_solve(self, f: np.ndarray) -> np.ndarray:
         fh = np.fft.fft(f.reshape(self.shape), axis=0)
         out = np.empty_like(fh)
-        n2 = self.g.size2d
         for k in range(self.g.z.n):
-            out[k] = self.lus[k].solve(fh[k].ravel()).reshape(fh[k].shape)
+            if self.skip is not None and self.skip[k]:
+                out[k] = 0.0      # D2csr[k]->solve == 0: x_sol_prd = 0 (functions.cpp:6020-6024)
+            else:
+                out[k] = self.lus[k].solve(fh[k].ravel()).reshape(fh[k].shape)
         return np.fft.ifft(out, axis=0)
 
     def l0_apply(self, u: np.ndarray) -> np.ndarray:
@@ -215,9 +218,17 @@ class ModeR:
         return self.l0_apply(u) - self.dl * u
 
 
+def kz_skip_reference(kz2: np.ndarray, omega: float, ratio: float) -> np.ndarray:
+    """The reference's SAVE_MEM rule (Source/FGMRES.cpp:197-206): mode k is
+    neither factored nor solved when kww >= ratio * k2, kww its kz table
+    value and k2 = kk^2, kk = omega / c_z (definitions.h)."""
+    return kz2 >= ratio * (omega / C_Z) ** 2
+
+
 def setup(g: Grid3D, beta: float = 0.5, media: str = "homo", quirk_q1: bool = True,
-          kz2: np.ndarray | None = None, factor: bool = True) -> ModeR:
-    """Media, dL, per-kz 2D matrices and their factorizations."""
+          kz2: np.ndarray | None = None, factor: bool = True, kz_skip_ratio: float = 0.0) -> ModeR:
+    """Media, dL, per-kz 2D matrices and their factorizations (kz_skip_ratio
+    > 0: the reference's SAVE_MEM build with that ratio, 5 at nu = 4 Hz)."""
     c3d = sound_speed_3d(g, media)
     c2d = sound_speed_2d(g, c3d, quirk_q1=quirk_q1)
     dl = delta_l(g, c3d, c2d, beta)
@@ -229,12 +240,13 @@ def setup(g: Grid3D, beta: float = 0.5, media: str = "homo", quirk_q1: bool = Tr
     else:
         base = (w / c2d) ** 2 * complex(1.0, beta)
     shifts = base[None, :, :] - kz2[:, None, None]
+    skip = kz_skip_reference(kz2, w, kz_skip_ratio) if kz_skip_ratio > 0 else None
     mats, lus = [], []
     for k in range(g.z.n):
         A = assemble_2d(g, shifts[k])
         mats.append(A)
-        lus.append(spla.splu(A) if factor else None)
-    return ModeR(g, beta, dl, c3d, c2d, shifts, mats, lus)
+        lus.append(spla.splu(A) if factor and (skip is None or not skip[k]) else None)
+    return ModeR(g, beta, dl, c3d, c2d, shifts, mats, lus, skip)
 
 
 def point_source_rhs(g: Grid3D) -> np.ndarray:

@@ -127,3 +127,25 @@ def test_inverse_traversal_identity():
     lhs = st.apply_a(st.l0_solve(v))
     rhs = st.apply_k(v)
     assert np.linalg.norm(lhs - rhs) <= 1e-11 * np.linalg.norm(rhs)
+
+
+def test_fgmres_savemem_matches_reference():
+    """The reference built with SAVE_MEM (Source/FGMRES.cpp:197-206: modes
+    with kww >= 5 k2 neither factored nor solved, their solution set to
+    zero): the oracle's skip rule picks the same modes, and its FGMRES gives
+    the same residual history and solution (every 2nd point per axis)."""
+    z = np.load(os.path.join(GOLDEN, "ref_fgmres_savemem_n50p4s4.npz"))
+    n, pml, spg, beta, niter, rest = z["params"]
+    g = grid.reference_grid(int(n), int(pml), int(spg))
+    st = mode_r.setup(g, beta=float(beta), media="homo", kz_skip_ratio=5.0)
+    assert np.flatnonzero(st.skip).tolist() == z["skipped"].tolist()
+    f = mode_r.point_source_rhs(g)
+    log = mode_r.fgmres_reference(st, f, m=int(niter), rest=int(rest), arnoldi="reference")
+    conv = z["conv"]
+    assert len(log.rows) == conv.shape[0]
+    for row, ref in zip(log.rows, conv):
+        assert row[1] == pytest.approx(ref[1], rel=1e-5)
+        assert row[2] == pytest.approx(ref[2], rel=1e-5)
+    sub = log.u[::2, ::2, ::2]
+    err = np.linalg.norm(sub - z["x_sol_sub"]) / np.linalg.norm(z["x_sol_sub"])
+    assert err < 1e-11
