@@ -285,6 +285,8 @@ def roofline_table(p, prof, its_per_source, nsrc, peaks):
 # dram__bytes_write.sum of one captured launch), per (family, grid, sources)
 TRAFFIC = {
     ("sweep", 128, 16): 5.273e9,
+    # the 200 x 200 x 32 capture of the packed sweep (4.825 GB) scaled by the kz chains, 200 / 32
+    ("sweep", 200, 16): 30.16e9,
 }
 
 
