@@ -82,7 +82,10 @@ typedef struct helm3d_opts {
     int mode;            /* helm3d_mode */
     int precision;       /* helm3d_precision */
     int kz_symbol;       /* helm3d_kz_symbol */
-    double beta_prec;    /* complex shift of the preconditioner; mode R: beta_eq */
+    double beta_prec;    /* complex shift of the preconditioner; mode R: beta_eq.  The FFT-z
+                          * preconditioner needs damping (0.25); with HELM3D_ZT_PML_EIGEN a small
+                          * shift (0.01) converges in far fewer iterations (measured at 128^3-200^3:
+                          * 7-8 instead of 22-33) */
     double beta_phys;    /* mode N: physical damping in A */
     double s2_l0;        /* mode R: > 0 -> L0 uses this constant s^2 (HOMO, q3) */
     int quirk_q1;        /* mode R: c0 by the reference's running-sum mean (q1) */
