@@ -88,7 +88,7 @@ struct F2K {
 struct F2Smem {
     float *Bhi, *Blo;   // [2 kF2MaxN rows][2 kF2B] canonical K-major each
     float2 *Y;          // [kF2B][kF2MaxN]: the panel's pivot rows
-    float2 *PF;         // [kF2MaxN][kF2B]: the panel's entries of every row
+    float2 *PF;         // [kF2MaxN][kF2PFld]: the panel's entries of every row
     float2 *wrow;       // [2][kF2RowWarps][kF2B]: each warp's candidate row, by step parity
     uint32_t *wkey;     // [2][kF2RowWarps]
     int *rho, *kap;     // [2][kF2Tab] each: the frame, double-buffered by line
@@ -98,7 +98,10 @@ struct F2Smem {
 };
 
 constexpr size_t kF2BBytes = sizeof(float) * 2 * kF2MaxN * 2 * kF2B;
-constexpr size_t kF2SmemBytes = 2 * kF2BBytes + 2 * sizeof(float2) * kF2B * kF2MaxN +
+// row stride of PF: 18 complex (144 bytes) instead of 16, so that a warp's
+// row-per-thread accesses (16-byte and 8-byte) fall on distinct banks
+constexpr int kF2PFld = kF2B + 2;
+constexpr size_t kF2SmemBytes = 2 * kF2BBytes + sizeof(float2) * (kF2B + kF2PFld) * kF2MaxN +
                                 sizeof(float2) * 2 * kF2RowWarps * kF2B + sizeof(uint32_t) * 2 * kF2RowWarps +
                                 sizeof(int) * 7 * kF2Tab + 6 * sizeof(uint64_t) + 16 + 1024 + 16;
 
@@ -109,7 +112,7 @@ __device__ __forceinline__ F2Smem f2_carve(unsigned char *raw) {
     s.Blo = s.Bhi + 2 * kF2MaxN * 2 * kF2B;
     s.Y = reinterpret_cast<float2 *>(s.Blo + 2 * kF2MaxN * 2 * kF2B);
     s.PF = s.Y + kF2B * kF2MaxN;
-    s.wrow = s.PF + kF2MaxN * kF2B;
+    s.wrow = s.PF + kF2MaxN * kF2PFld;
     s.wkey = reinterpret_cast<uint32_t *>(s.wrow + 2 * kF2RowWarps * kF2B);
     s.rho = reinterpret_cast<int *>(s.wkey + 2 * kF2RowWarps);
     s.kap = s.rho + 2 * kF2Tab;
@@ -311,8 +314,8 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                     tmem_ld32_nowait(trow + (uint32_t)(2 * k0), f);
                     tmem_wait_ld(f);
                     if (valid) {
-                        float4 *dst = reinterpret_cast<float4 *>(sm.PF + (size_t)g * kF2B);
-                        const uint32_t rdst = pf_peer + (uint32_t)(g * kF2B * sizeof(float2));
+                        float4 *dst = reinterpret_cast<float4 *>(sm.PF + (size_t)g * kF2PFld);
+                        const uint32_t rdst = pf_peer + (uint32_t)(g * kF2PFld * sizeof(float2));
 #pragma unroll
                         for (int e = 0; e < kF2B / 2; e++) {
                             const float4 q4 = make_float4(f[4 * e], f[4 * e + 1], f[4 * e + 2], f[4 * e + 3]);
@@ -328,8 +331,8 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                 ph_pan ^= 1u;
                 float2 P0[kF2B], P1[kF2B];
                 {
-                    const float4 *s0 = reinterpret_cast<const float4 *>(sm.PF + (size_t)t * kF2B);
-                    const float4 *s1 = reinterpret_cast<const float4 *>(sm.PF + (size_t)(has1 ? g1 : t) * kF2B);
+                    const float4 *s0 = reinterpret_cast<const float4 *>(sm.PF + (size_t)t * kF2PFld);
+                    const float4 *s1 = reinterpret_cast<const float4 *>(sm.PF + (size_t)(has1 ? g1 : t) * kF2PFld);
 #pragma unroll
                     for (int e = 0; e < kF2B / 2; e++) {
                         const float4 x0 = s0[e], x1 = s1[e];
@@ -417,8 +420,8 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                 // ---- the panel after its steps back into PF, in column order
                 // (P[e] holds column (bl + e) mod 16)
                 {
-                    float2 *d0 = sm.PF + (size_t)t * kF2B;
-                    float2 *d1 = sm.PF + (size_t)(has1 ? g1 : t) * kF2B;
+                    float2 *d0 = sm.PF + (size_t)t * kF2PFld;
+                    float2 *d1 = sm.PF + (size_t)(has1 ? g1 : t) * kF2PFld;
 #pragma unroll
                     for (int e = 0; e < kF2B; e++) d0[(bl + e) & (kF2B - 1)] = P0[e];
                     if (has1) {
@@ -439,7 +442,7 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                 const bool piv = valid && my_step >= k0 && my_step < k0 + bl;
                 {
                     float xh[32], xl[32], f[32];
-                    const float4 *src = reinterpret_cast<const float4 *>(sm.PF + (size_t)(valid ? g : 0) * kF2B);
+                    const float4 *src = reinterpret_cast<const float4 *>(sm.PF + (size_t)(valid ? g : 0) * kF2PFld);
 #pragma unroll
                     for (int e = 0; e < kF2B / 2; e++) {
                         const float4 q4 = src[e];
@@ -477,17 +480,26 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                     const int yr = piv ? my_step - k0 : 0;
                     float2 *yrow = sm.Y + (size_t)yr * kF2MaxN;
                     const uint32_t yrp = y_peer + (uint32_t)(yr * kF2MaxN * sizeof(float2));
+                    // two 32-column loads in flight per wait
+                    const int nc = ncol / 16;
 #pragma unroll 1
-                    for (int c = 0; c < ncol / 16; c++) {
-                        float f[32];
-                        tmem_ld32_nowait(trow + (uint32_t)(32 * c), f);
-                        tmem_wait_ld(f);
+                    for (int c = 0; c < nc; c += 2) {
+                        float f[2][32];
+                        tmem_ld32_nowait(trow + (uint32_t)(32 * c), f[0]);
+                        if (c + 1 < nc) tmem_ld32_nowait(trow + (uint32_t)(32 * (c + 1)), f[1]);
+                        tmem_wait_ld(f[0]);
+                        tmem_wait_ld(f[1]);
                         if (piv) {
 #pragma unroll
-                            for (int e = 0; e < 8; e++) {
-                                const float4 q4 = make_float4(f[4 * e], f[4 * e + 1], f[4 * e + 2], f[4 * e + 3]);
-                                reinterpret_cast<float4 *>(yrow + 16 * c)[e] = q4;
-                                st_cluster_v4f32(yrp + (uint32_t)((16 * c + 2 * e) * sizeof(float2)), q4);
+                            for (int h = 0; h < 2; h++) {
+                                if (c + h >= nc) break;
+#pragma unroll
+                                for (int e = 0; e < 8; e++) {
+                                    const float4 q4 = make_float4(f[h][4 * e], f[h][4 * e + 1], f[h][4 * e + 2],
+                                                                  f[h][4 * e + 3]);
+                                    reinterpret_cast<float4 *>(yrow + 16 * (c + h))[e] = q4;
+                                    st_cluster_v4f32(yrp + (uint32_t)((16 * (c + h) + 2 * e) * sizeof(float2)), q4);
+                                }
                             }
                         }
                     }
