@@ -87,7 +87,7 @@ struct F2K {
 
 struct F2Smem {
     float *Bhi, *Blo;   // [2 kF2MaxN rows][2 kF2B] canonical K-major each
-    float2 *Y;          // [kF2B][kF2MaxN]: the panel's pivot rows
+    float2 *Y;          // [kF2B][kF2Yld]: the panel's pivot rows
     float2 *PF;         // [kF2MaxN][kF2PFld]: the panel's entries of every row
     float2 *wrow;       // [2][kF2RowWarps][kF2B]: each warp's candidate row, by step parity
     uint32_t *wkey;     // [2][kF2RowWarps]
@@ -101,7 +101,10 @@ constexpr size_t kF2BBytes = sizeof(float) * 2 * kF2MaxN * 2 * kF2B;
 // row stride of PF: 18 complex (144 bytes) instead of 16, so that a warp's
 // row-per-thread accesses (16-byte and 8-byte) fall on distinct banks
 constexpr int kF2PFld = kF2B + 2;
-constexpr size_t kF2SmemBytes = 2 * kF2BBytes + sizeof(float2) * (kF2B + kF2PFld) * kF2MaxN +
+// row stride of Y: 226 complex, so that the B build's reads of four pivot
+// rows at the same column fall on distinct banks (16-byte aligned rows)
+constexpr int kF2Yld = kF2MaxN + 2;
+constexpr size_t kF2SmemBytes = 2 * kF2BBytes + sizeof(float2) * (kF2B * kF2Yld + kF2PFld * kF2MaxN) +
                                 sizeof(float2) * 2 * kF2RowWarps * kF2B + sizeof(uint32_t) * 2 * kF2RowWarps +
                                 sizeof(int) * 7 * kF2Tab + 6 * sizeof(uint64_t) + 16 + 1024 + 16;
 
@@ -111,7 +114,7 @@ __device__ __forceinline__ F2Smem f2_carve(unsigned char *raw) {
     s.Bhi = reinterpret_cast<float *>(b);
     s.Blo = s.Bhi + 2 * kF2MaxN * 2 * kF2B;
     s.Y = reinterpret_cast<float2 *>(s.Blo + 2 * kF2MaxN * 2 * kF2B);
-    s.PF = s.Y + kF2B * kF2MaxN;
+    s.PF = s.Y + kF2B * kF2Yld;
     s.wrow = s.PF + kF2MaxN * kF2PFld;
     s.wkey = reinterpret_cast<uint32_t *>(s.wrow + 2 * kF2RowWarps * kF2B);
     s.rho = reinterpret_cast<int *>(s.wkey + 2 * kF2RowWarps);
@@ -478,8 +481,8 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                 // the panel's update, outside the panel) into Y of both CTAs
                 if (__any_sync(0xffffffffu, piv)) {
                     const int yr = piv ? my_step - k0 : 0;
-                    float2 *yrow = sm.Y + (size_t)yr * kF2MaxN;
-                    const uint32_t yrp = y_peer + (uint32_t)(yr * kF2MaxN * sizeof(float2));
+                    float2 *yrow = sm.Y + (size_t)yr * kF2Yld;
+                    const uint32_t yrp = y_peer + (uint32_t)(yr * kF2Yld * sizeof(float2));
                     // two 32-column loads in flight per wait
                     const int nc = ncol / 16;
 #pragma unroll 1
@@ -517,8 +520,8 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                     const int rlo = u & 7, kq = (u >> 3) & 7, rg = u >> 6;
                     const int row = rg * 8 + rlo, j = row >> 1;
                     const int kk0 = 2 * kq;
-                    const float2 y0 = kk0 < bl ? sm.Y[(size_t)kk0 * kF2MaxN + j] : make_float2(0.f, 0.f);
-                    const float2 y1 = kk0 + 1 < bl ? sm.Y[(size_t)(kk0 + 1) * kF2MaxN + j] : make_float2(0.f, 0.f);
+                    const float2 y0 = kk0 < bl ? sm.Y[(size_t)kk0 * kF2Yld + j] : make_float2(0.f, 0.f);
+                    const float2 y1 = kk0 + 1 < bl ? sm.Y[(size_t)(kk0 + 1) * kF2Yld + j] : make_float2(0.f, 0.f);
                     float4 e;
                     if ((row & 1) == 0) e = make_float4(y0.x, -y0.y, y1.x, -y1.y);   // (Re y, -Im y)
                     else e = make_float4(y0.y, y0.x, y1.y, y1.x);                   // (Im y, Re y)
