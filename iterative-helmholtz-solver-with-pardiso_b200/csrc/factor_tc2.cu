@@ -168,6 +168,20 @@ __device__ __forceinline__ uint32_t f2_key(float2 v, bool cand, int g) {
     return (__float_as_uint(av) & 0xFFFFFF00u) | (uint32_t)(255 - g);
 }
 
+// 1 / pv for a nonzero pivot with |pv| in [2^-126, 2^127): pv is scaled by
+// the power of two that brings its larger component into [1, 2) (exact), and
+// 1 / |pv s|^2 (in [1/8, 1]) is the hardware's approximate reciprocal
+// (rcp.approx, relative error within 2^-22); 1 / pv = s^2 conj(pv) / |pv s|^2.
+__device__ __forceinline__ float2 f2_inv(float2 pv) {
+    const float m = fmaxf(fabsf(pv.x), fabsf(pv.y));
+    const float s = __uint_as_float((254u - (__float_as_uint(m) >> 23)) << 23);
+    const float ax = pv.x * s, ay = pv.y * s;
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(ax * ax + ay * ay));
+    const float rd = s * r;
+    return make_float2(ax * rd, -ay * rd);
+}
+
 __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     F2Smem sm = f2_carve(smem_raw);
@@ -349,76 +363,107 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                 // The rows rotate by one column per step, so that the column
                 // of step kk is always P[0] (no register indexed by kk): after
                 // step kk, P[e] holds panel column (kk + 1 + e) mod 16.
+                // A pivot row is left unscaled in its step (its multiplier is
+                // 0, its new column 1) and scaled by its 1 / pv after the
+                // panel: every later step is linear in the row, so this gives
+                // the same rows as scaling it in its step. Each step issues
+                // the next step's warp reduction right after the update of
+                // the next pivot column, before the other columns.
+                float2 sc0 = make_float2(1.f, 0.f), sc1 = sc0;
+                bool piv0 = false, piv1 = false;
+                uint32_t key0 = f2_key(P0[0], !used0, t);
+                uint32_t key1 = f2_key(P1[0], has1 && !used1, g1);
+                uint32_t key = key0 > key1 ? key0 : key1;
+                uint32_t kw = __reduce_max_sync(0xffffffffu, key);
 #pragma unroll 1
                 for (int kk = 0; kk < bl; kk++) {
                     const int k = k0 + kk, buf = k & 1;
-                    const uint32_t key0 = f2_key(P0[0], !used0, t);
-                    const uint32_t key1 = f2_key(P1[0], has1 && !used1, g1);
-                    const uint32_t key = key0 > key1 ? key0 : key1;
-                    const uint32_t kw = __reduce_max_sync(0xffffffffu, key);
                     if (lane == 0) sm.wkey[buf * kF2RowWarps + warp] = kw;
                     if (kw != 0u && key == kw) {
-                        // the winning row in panel column order
-                        float2 *w = sm.wrow + (size_t)(buf * kF2RowWarps + warp) * kF2B;
+                        // the winning row in register order: w[0] the pivot, w[1 + e] = prow[e]
+                        float4 *w = reinterpret_cast<float4 *>(sm.wrow + (size_t)(buf * kF2RowWarps + warp) * kF2B);
+                        if (key0 == kw) {
 #pragma unroll
-                        for (int e = 0; e < kF2B; e++) w[(kk + e) & (kF2B - 1)] = key0 == kw ? P0[e] : P1[e];
+                            for (int e = 0; e < kF2B / 2; e++)
+                                w[e] = make_float4(P0[2 * e].x, P0[2 * e].y, P0[2 * e + 1].x, P0[2 * e + 1].y);
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < kF2B / 2; e++)
+                                w[e] = make_float4(P1[2 * e].x, P1[2 * e].y, P1[2 * e + 1].x, P1[2 * e + 1].y);
+                        }
                     }
                     f2_row_barrier();
-                    uint32_t kmax = sm.wkey[buf * kF2RowWarps];
+                    const uint4 kv = *reinterpret_cast<const uint4 *>(sm.wkey + buf * kF2RowWarps);
+                    uint32_t kmax = kv.x;
                     int wsel = 0;
-#pragma unroll
-                    for (int w2 = 1; w2 < kF2RowWarps; w2++) {
-                        const uint32_t kk2 = sm.wkey[buf * kF2RowWarps + w2];
-                        if (kk2 > kmax) {
-                            kmax = kk2;
-                            wsel = w2;
-                        }
+                    if (kv.y > kmax) {
+                        kmax = kv.y;
+                        wsel = 1;
+                    }
+                    if (kv.z > kmax) {
+                        kmax = kv.z;
+                        wsel = 2;
+                    }
+                    if (kv.w > kmax) {
+                        kmax = kv.w;
+                        wsel = 3;
                     }
                     const int r = kmax != 0u ? 255 - (int)(kmax & 0xFFu) : -1;
                     // the pivot row, rotated like the rows: prow[e] = column (kk + 1 + e) mod 16
-                    const float2 *w = sm.wrow + (size_t)(buf * kF2RowWarps + wsel) * kF2B;
-                    float2 prow[kF2B];
+                    const float4 *w = reinterpret_cast<const float4 *>(sm.wrow + (size_t)(buf * kF2RowWarps + wsel) * kF2B);
+                    float2 prow[kF2B], pv = make_float2(0.f, 0.f);
 #pragma unroll
-                    for (int e = 0; e < kF2B; e++) prow[e] = w[(kk + 1 + e) & (kF2B - 1)];
-                    const float2 pv = w[kk];
+                    for (int e = 0; e < kF2B / 2; e++) {
+                        const float4 q4 = w[e];
+                        if (e == 0) pv = make_float2(q4.x, q4.y);
+                        else prow[2 * e - 1] = make_float2(q4.x, q4.y);
+                        prow[2 * e] = make_float2(q4.z, q4.w);
+                    }
                     float2 pinv = make_float2(0.f, 0.f);
                     if (r < 0 || (pv.x == 0.f && pv.y == 0.f)) {
                         // no finite candidate, or an exactly zero pivot: flagged, the block is invalid
                         if (t == 0 && rank == 0) atomicOr(a.status, 1);
                     } else {
-                        // 1 / pv, scaled against overflow of |pv|^2
-                        const float sc = __frcp_rn(fmaxf(fabsf(pv.x), fabsf(pv.y)));
-                        const float ax = pv.x * sc, ay = pv.y * sc;
-                        const float rd = sc * __frcp_rn(ax * ax + ay * ay);
-                        pinv = make_float2(ax * rd, -ay * rd);
+                        pinv = f2_inv(pv);
                     }
                     if (t == 0) sm.perm[k] = r >= 0 ? r : 0;
-                    // row -= (c / pv) * pivot row, column k becomes -c / pv;
-                    // the pivot row is scaled by 1 / pv, its column k becomes 1 / pv
-                    {
-                        const float2 s0 = cmul(P0[0], pinv), s1 = cmul(P1[0], pinv);
-#pragma unroll
-                        for (int e = 0; e < kF2B - 1; e++) {
-                            P0[e] = cfms(s0, prow[e], P0[e + 1]);
-                            P1[e] = cfms(s1, prow[e], P1[e + 1]);
-                        }
-                        P0[kF2B - 1] = make_float2(-s0.x, -s0.y);
-                        P1[kF2B - 1] = make_float2(-s1.x, -s1.y);
-                    }
-                    if (t == r) {
-#pragma unroll
-                        for (int e = 0; e < kF2B - 1; e++) P0[e] = cmul(prow[e], pinv);
-                        P0[kF2B - 1] = pinv;
-                        used0 = true;
+                    // row -= (c / pv) * pivot row, column k becomes -c / pv
+                    const bool ip0 = t == r, ip1 = g1 == r;
+                    float2 s0 = cmul(P0[0], pinv), s1 = cmul(P1[0], pinv);
+                    if (ip0) {
+                        s0 = make_float2(0.f, 0.f);
+                        sc0 = pinv;
+                        used0 = piv0 = true;
                         sm.stepof[t] = k;
                     }
-                    if (g1 == r) {
-#pragma unroll
-                        for (int e = 0; e < kF2B - 1; e++) P1[e] = cmul(prow[e], pinv);
-                        P1[kF2B - 1] = pinv;
-                        used1 = true;
+                    if (ip1) {
+                        s1 = make_float2(0.f, 0.f);
+                        sc1 = pinv;
+                        used1 = piv1 = true;
                         sm.stepof[g1] = k;
                     }
+                    P0[0] = cfms(s0, prow[0], P0[1]);
+                    P1[0] = cfms(s1, prow[0], P1[1]);
+                    key0 = f2_key(P0[0], !used0, t);
+                    key1 = f2_key(P1[0], has1 && !used1, g1);
+                    key = key0 > key1 ? key0 : key1;
+                    kw = __reduce_max_sync(0xffffffffu, key);
+#pragma unroll
+                    for (int e = 1; e < kF2B - 1; e++) {
+                        P0[e] = cfms(s0, prow[e], P0[e + 1]);
+                        P1[e] = cfms(s1, prow[e], P1[e + 1]);
+                    }
+                    P0[kF2B - 1] = ip0 ? make_float2(1.f, 0.f) : make_float2(-s0.x, -s0.y);
+                    P1[kF2B - 1] = ip1 ? make_float2(1.f, 0.f) : make_float2(-s1.x, -s1.y);
+                }
+                // the panel's pivot rows scaled by their 1 / pv
+                if (piv0) {
+#pragma unroll
+                    for (int e = 0; e < kF2B; e++) P0[e] = cmul(P0[e], sc0);
+                }
+                if (piv1) {
+#pragma unroll
+                    for (int e = 0; e < kF2B; e++) P1[e] = cmul(P1[e], sc1);
                 }
                 // ---- the panel after its steps back into PF, in column order
                 // (P[e] holds column (bl + e) mod 16)
