@@ -558,25 +558,29 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                 f2_row_barrier();
                 wait_cluster(sm.y_bar, ph_y);
                 ph_y ^= 1u;
-                // ---- B = real form of Y (rows 2j + c, K = 2kk + c'), hi and lo,
-                // 16-byte units in address order (row & 7, K quad, 8-row group)
-#pragma unroll 4
-                for (int u = t; u < 2 * ncol * (2 * kF2B / 4); u += kF2RowThreads) {
-                    const int rlo = u & 7, kq = (u >> 3) & 7, rg = u >> 6;
-                    const int row = rg * 8 + rlo, j = row >> 1;
+                // ---- B = real form of Y (rows 2j + c, K = 2kk + c'), hi and lo:
+                // each pair (column j of Y, K quad kq) gives the 16-byte units of
+                // rows 2j, (Re y, -Im y), and 2j + 1, (Im y, Re y), adjacent in
+                // address order (row & 7, K quad, 8-row group); the TF32 split
+                // is odd in its argument, so one split serves both rows
+#pragma unroll 2
+                for (int v = t; v < ncol * (2 * kF2B / 4); v += kF2RowThreads) {
+                    const int jlo = v & 3, kq = (v >> 2) & 7, j = (v >> 5) * 4 + jlo;
                     const int kk0 = 2 * kq;
                     const float2 y0 = kk0 < bl ? sm.Y[(size_t)kk0 * kF2Yld + j] : make_float2(0.f, 0.f);
                     const float2 y1 = kk0 + 1 < bl ? sm.Y[(size_t)(kk0 + 1) * kF2Yld + j] : make_float2(0.f, 0.f);
-                    float4 e;
-                    if ((row & 1) == 0) e = make_float4(y0.x, -y0.y, y1.x, -y1.y);   // (Re y, -Im y)
-                    else e = make_float4(y0.y, y0.x, y1.y, y1.x);                   // (Im y, Re y)
-                    float4 h, l;
-                    tf32_split_fast(e.x, h.x, l.x);
-                    tf32_split_fast(e.y, h.y, l.y);
-                    tf32_split_fast(e.z, h.z, l.z);
-                    tf32_split_fast(e.w, h.w, l.w);
-                    reinterpret_cast<float4 *>(sm.Bhi)[u] = h;
-                    reinterpret_cast<float4 *>(sm.Blo)[u] = l;
+                    float4 h, l;   // split of (Re y0, Im y0, Re y1, Im y1)
+                    tf32_split_fast(y0.x, h.x, l.x);
+                    tf32_split_fast(y0.y, h.y, l.y);
+                    tf32_split_fast(y1.x, h.z, l.z);
+                    tf32_split_fast(y1.y, h.w, l.w);
+                    const int u0 = (v >> 5) * 64 + kq * 8 + 2 * jlo;
+                    float4 *bh = reinterpret_cast<float4 *>(sm.Bhi) + u0;
+                    float4 *bl4 = reinterpret_cast<float4 *>(sm.Blo) + u0;
+                    bh[0] = make_float4(h.x, -h.y, h.z, -h.w);
+                    bh[1] = make_float4(h.y, h.x, h.w, h.z);
+                    bl4[0] = make_float4(l.x, -l.y, l.z, -l.w);
+                    bl4[1] = make_float4(l.y, l.x, l.w, l.z);
                 }
                 fence_proxy_async_smem();
                 __syncwarp();
