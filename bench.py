@@ -13,9 +13,11 @@ lockstep batched FGMRES over the 16 sources, with the preconditioner in
 complex64 and the z-transform in the PML eigenbasis (outer loop, operator
 and Gram-Schmidt in complex128).  `value` is seconds per source-solve (step
 time / 16) with the medium and the sources resident on the device, timed
-with CUDA events on the solver's stream.  `e2e` repeats the headline step
-through the C ABI with pinned host buffers (medium and sources copied in,
-solutions copied out inside the timed region).
+with CUDA events on the solver's stream.  Both call the C ABI's
+helm3d_solve_medium (medium, factor and solve in one call).  `e2e` repeats
+the headline step with pinned host buffers (medium and sources copied in,
+the sources while the medium is factored, solutions copied out, all inside
+the timed region).
 
 Beside the headline, one step each (after one warm-up step) of the same
 workload solved other ways, so that each stated change can be read apart:
@@ -350,8 +352,9 @@ def run_ours(args, rank, world, dist):
         return dist_max(dist, x, dev)
 
     def step(s, nrhs, s2=s2_dev, F=F_dev, U=U_dev):
-        s.set_medium(s2)
-        s.solve(F[:nrhs], nrhs=nrhs, u=U[:nrhs], allow_not_converged=True)
+        # helm3d_solve_medium: set-up, factor and solve in one call (with host
+        # buffers the sources are copied in while the medium is factored)
+        s.solve_medium(s2, F[:nrhs], nrhs=nrhs, u=U[:nrhs], allow_not_converged=True)
 
     def timed_steps(s, nrhs, steps, warmup, s2=s2_dev, F=F_dev, U=U_dev):
         """ms per step (max over ranks), iterations per source of the last

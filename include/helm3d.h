@@ -140,6 +140,16 @@ int helm3d_set_medium(helm3d_ctx *ctx, const double *s2);
  * Source/templates.h:59), which the reference calls once per source. */
 int helm3d_solve(helm3d_ctx *ctx, const double *f, double *u, int nrhs, helm3d_stats *stats);
 
+/* helm3d_set_medium(ctx, s2) then helm3d_solve(ctx, f, u, nrhs, stats) in
+ * one call, as the reference's FGMRES builds the medium, factors and solves
+ * in one call (Source/FGMRES.cpp:72-298 then :300-725).  With host f (pinned
+ * for the overlap) and nrhs in one lockstep batch, the right-hand sides are
+ * copied to the device while the medium is set up and factored.  Returns the
+ * factor's error (and leaves the context refusing solves, as
+ * helm3d_set_medium does) or the solve's status. */
+int helm3d_solve_medium(helm3d_ctx *ctx, const double *s2, const double *f, double *u, int nrhs,
+                        helm3d_stats *stats);
+
 /* Solve n contexts at once: grids of different sizes, each with its own
  * medium, options and factor, on one device.  Context i solves nrhs[i]
  * right-hand sides f[i] -> u[i] (host or device pointers, laid out as for

@@ -294,6 +294,78 @@ int helm3d_solve(helm3d_ctx *c, const double *f, double *u, int nrhs, helm3d_sta
     return solve_common(c, f, u, nrhs, st, 0);
 }
 
+int helm3d_solve_medium(helm3d_ctx *c, const double *s2, const double *f, double *u, int nrhs,
+                        helm3d_stats *st) {
+    if (!c || !s2 || !f || !u || nrhs < 1) return HELM3D_ERR_ARG;
+    cudaSetDevice(c->device);
+    const size_t count = (size_t)nrhs * c->N;
+    // host right-hand sides that fit one lockstep batch go to the staging
+    // buffer on a copy stream while the medium is factored: the staging
+    // buffer and the stream are made first, the copy is issued after the
+    // medium's own upload (so that it does not queue behind the sources)
+    bool pre = !is_device_ptr(f) && batch_size(c, nrhs, true) >= nrhs;
+    if (pre) {
+        int rc = HELM3D_OK;
+        if (!c->copy_stream) {
+            rc = cuda_check(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "copy stream");
+            if (!rc) rc = cuda_check(c, cudaEventCreateWithFlags(&c->ev_copy0, cudaEventDisableTiming), "copy event");
+            if (!rc) rc = cuda_check(c, cudaEventCreateWithFlags(&c->ev_copy, cudaEventDisableTiming), "copy event");
+            if (rc) return rc;
+        }
+        if (c->d_f && c->f_cap < count) {
+            rc = cuda_check(c, cudaStreamSynchronize(c->stream), "staging sync");
+            if (rc) return rc;
+            cudaFree(c->d_f);
+            c->bytes -= sizeof(double2) * c->f_cap;
+            c->d_f = nullptr;
+            c->f_cap = 0;
+        }
+        if (!c->d_f) {
+            rc = cuda_check(c, cudaMalloc((void **)&c->d_f, sizeof(double2) * count), "staging buffer");
+            if (rc) return rc;
+            c->bytes += sizeof(double2) * count;
+            c->f_cap = count;
+        }
+    }
+    int rc = ctx_setup_medium(c, s2, is_device_ptr(s2));
+    if (!rc && pre) {
+        // after the medium's upload and the context's earlier work on the
+        // staging buffer (both on the context's stream)
+        rc = cuda_check(c, cudaEventRecord(c->ev_copy0, c->stream), "copy order");
+        if (!rc) rc = cuda_check(c, cudaStreamWaitEvent(c->copy_stream, c->ev_copy0, 0), "copy order");
+        if (!rc)
+            rc = cuda_check(c, cudaMemcpyAsync(c->d_f, f, sizeof(double2) * count, cudaMemcpyHostToDevice, c->copy_stream),
+                            "copy in");
+        if (!rc) rc = cuda_check(c, cudaEventRecord(c->ev_copy, c->copy_stream), "copy order");
+        if (rc) {
+            cudaStreamSynchronize(c->copy_stream);
+            c->factor_rc = rc;
+            return rc;
+        }
+    } else {
+        pre = false;
+    }
+    if (!rc) rc = ctx_factor(c);
+    c->factor_rc = rc;
+    if (pre) {
+        // the solve reads the copy on the context's stream; a failed factor
+        // still waits for it, so that no copy outlives the call
+        const int rc2 = cuda_check(c, cudaStreamWaitEvent(c->stream, c->ev_copy, 0), "copy order");
+        if (rc) {
+            cudaEventSynchronize(c->ev_copy);
+            return rc;
+        }
+        if (rc2) {
+            cudaEventSynchronize(c->ev_copy);
+            return rc2;
+        }
+    }
+    if (rc) return rc;
+    rc = solve_common(c, pre ? (const double *)c->d_f : f, u, nrhs, st, 0);
+    if (pre) cudaEventSynchronize(c->ev_copy);   // f is not read after the call returns
+    return rc;
+}
+
 int helm3d_solve_group(helm3d_ctx *const *ctxs, int n, const double *const *f, double *const *u, const int *nrhs,
                        helm3d_stats *stats) {
     if (!ctxs || n < 1 || !f || !u || !nrhs) return HELM3D_ERR_ARG;
@@ -578,6 +650,12 @@ int helm3d_destroy(helm3d_ctx *c) {
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
+    if (c->ev_copy0) cudaEventDestroy(c->ev_copy0);
+    if (c->ev_copy) cudaEventDestroy(c->ev_copy);
     delete c;
     return HELM3D_OK;
 }

@@ -340,6 +340,9 @@ struct helm3d_ctx {
     double ms_factor = 0;      // wall time of set-up + factor in helm3d_create
     long long reorth = 0;      // Gram-Schmidt second passes taken
     cudaStream_t own_stream = nullptr;
+    // helm3d_solve_medium: host right-hand sides copied in under the factor
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_copy0 = nullptr, ev_copy = nullptr;
 
     // optional per-kernel-family profiler (helm3d_profile)
     struct ProfEv {

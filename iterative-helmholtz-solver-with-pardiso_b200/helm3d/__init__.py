@@ -60,6 +60,7 @@ _sig = {
     "helm3d_create": (ctypes.c_int, [ctypes.POINTER(Grid), _vp, ctypes.POINTER(Opts), ctypes.POINTER(_vp)]),
     "helm3d_set_medium": (ctypes.c_int, [_vp, _vp]),
     "helm3d_solve": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.POINTER(Stats)]),
+    "helm3d_solve_medium": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.POINTER(Stats)]),
     "helm3d_solve_group": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp),
                                           ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(Stats)]),
     "helm3d_solve_bicgstab": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(Stats)]),
@@ -193,6 +194,22 @@ class Solver:
             self._err(rc, "solve")
         self.last_stats = st
         self.last_history = list(hist[:st.history_len]) if hist is not None else []
+        return u
+
+    def solve_medium(self, s2, f, nrhs: int = 1, u=None, allow_not_converged=False):
+        """A new medium, its factor and the solve in one call
+        (helm3d_solve_medium): host right-hand sides are copied in while
+        the medium is factored."""
+        s2 = s2 if hasattr(s2, "data_ptr") else np.ascontiguousarray(s2, dtype=np.float64)
+        self._s2 = s2
+        f = _c128(f)
+        u = self._out_like(f, nrhs) if u is None else u
+        st = Stats()
+        rc = lib.helm3d_solve_medium(self.h, _ptr(s2), _ptr(f), _ptr(u), nrhs, ctypes.byref(st))
+        if rc != OK and not (allow_not_converged and rc == ERR_NOT_CONVERGED):
+            self._err(rc, "solve_medium")
+        self.last_stats = st
+        self.last_history = []
         return u
 
     def solve_bicgstab(self, f, history: int = 0, allow_not_converged=False):
